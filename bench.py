@@ -1,0 +1,333 @@
+"""Benchmark of the sector-Lanczos hot path on B200.
+
+Workload: 4x4 periodic square lattice, nearest-neighbour t=1, U=8,
+half filling Nup=Ndw=8, D = 12870^2 = 165,636,900. A step is one H x v of that sector in
+FP32 (the bulk precision of the engine), stored form, vectors resident in HBM; inputs are
+larger than L2 (662 MB per vector), so no flush is needed between steps.
+
+    metric : H x v throughput as algorithmic GB/s = (H x v per s) * 2*D*4 B
+             (read v once, write Hv once, FP32), the HBM-roofline figure of the path
+    e2e    : the same metric through the reference-facing dd_sparse_HxV entry (edg_hxv_z):
+             complex(8) host vectors in pinned memory, H2D + H x v + D2H inside the timing
+    extra  : E0 time-to-solution (relative 1e-8) for plain FP64 Lanczos and FP32+refine
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs independent replicas (one per GPU, launched by torchrun): the path has no
+exchange step on one sector per GPU ("replicas only"), so scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LX, LY, U, NUP, NDW = 4, 4, 8.0, 8, 8
+WORKLOAD = "hubbard_4x4_U8_half_filling_sector(8,8)_D165636900"
+METRIC = "hxv_algorithmic_GBps"
+UNIT = "GB/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons with NVML during the timed region."""
+
+    def __init__(self, device_index: int, period: float = 0.02):
+        self.idx, self.period = device_index, period
+        self.samples: list[tuple[int, int, int]] = []
+        self._stop = threading.Event()
+        self._t = None
+        self.ok = False
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            return self
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                clk = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((clk, rs, int(time.time() * 1000)))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        nv = self.nv
+        names = {
+            "gpu_idle": getattr(nv, "nvmlClocksEventReasonGpuIdle", 0x1),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+        }
+        seen = set()
+        for _, rs, _ in self.samples:
+            for k, bit in names.items():
+                if rs & bit and k != "gpu_idle":
+                    seen.add(k)
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(seen), "samples": len(self.samples)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline_sample(target_seconds: float = 12.0):
+    """The oracle's stored-form spMatVec (FP64, OpenMP on all host threads) on config 2,
+    timed on a bounded sample of output rows. Returns (GB/s in the metric's unit, info)."""
+    from ed_lattice_b200.edlat import square_lattice
+    from oracle import oracle as O
+    m = O.Model(square_lattice(LX, LY), uloc=U, xmu=U / 2, hfmode=False)
+    st = O.Stored(m, NUP, NDW)
+    D, ddw = st.dim, st.dimdw
+    v = O.random_vector(7, D)
+    hv = np.zeros(D)
+    rows = max(1, ddw // 256)
+    t0 = time.perf_counter()
+    st.matvec_rows_d(v, hv, 0, rows)
+    t1 = time.perf_counter()
+    per_row = (t1 - t0) / rows
+    rows = int(min(ddw, max(rows, target_seconds / max(per_row, 1e-9))))
+    t0 = time.perf_counter()
+    st.matvec_rows_d(v, hv, 0, rows)
+    dt = time.perf_counter() - t0
+    frac = rows / ddw
+    hxv_per_s = frac / dt
+    return hxv_per_s * 2 * D * 4 / 1e9, {"cores": O.num_threads(), "kind": "port",
+                                        "sample": f"stored spMatVec FP64 restatement, output rows 0..{rows} of "
+                                                  f"{ddw} ({frac:.3%} of one H x v, {dt:.1f} s)"}
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from ed_lattice_b200.edlat import square_lattice
+    from oracle import oracle as O
+    m = O.Model(square_lattice(LX, LY), uloc=U, xmu=U / 2, hfmode=False)
+    st = O.Stored(m, NUP, NDW)
+    D, ddw = st.dim, st.dimdw
+    v = O.random_vector(7, D)
+    hv = np.zeros(D)
+    # one step = a bounded sample of the H x v (output rows), sized so that the whole run
+    # stays within a few minutes; the same rows every step
+    budget = 150.0 / max(1, args.steps + args.warmup)
+    rows = max(1, ddw // 512)
+    t0 = time.perf_counter()
+    st.matvec_rows_d(v, hv, 0, rows)
+    per_row = (time.perf_counter() - t0) / rows
+    rows = int(min(ddw, max(1, budget / max(per_row, 1e-9))))
+    for _ in range(args.warmup):
+        st.matvec_rows_d(v, hv, 0, rows)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st.matvec_rows_d(v, hv, 0, rows)
+    dt = time.perf_counter() - t0
+    hxv_per_s = args.steps * (rows / ddw) / dt
+    val = hxv_per_s * 2 * D * 4 / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": "stored (spMatVec)", "sample_rows_per_step": rows,
+                       "rows_total": ddw},
+            "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                             "sample": f"output rows 0..{rows} of {ddw} per step (FP64 stored-form restatement; "
+                                       "reference Fortran/SciFortran not buildable here)"},
+            "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def e0_time_to_solution(E, L, sector, seed=2024, maxit=600):
+    """Plain FP64 Lanczos vs FP32+refine to relative 1e-8 in E0 (E0 only), against a tightly
+    converged FP64 value."""
+    import torch
+    out = {}
+    e_ref, _, it_ref = E.sp_lanc_eigh(sector, seed=seed, maxit=maxit, tol=1e-13, mode=E.EDG_GS_F64,
+                                      want_vector=False)
+    out["e0_reference_tol1e-13"] = e_ref
+    for name, mode in (("fp64", E.EDG_GS_F64), ("fp32_refine", E.EDG_GS_F32_REFINE)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, _, it = E.sp_lanc_eigh(sector, seed=seed, maxit=maxit, tol=1e-9, mode=mode, want_vector=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"seconds": dt, "hxv_applications": it, "e0": e0, "rel_err": abs(e0 - e_ref) / abs(e_ref)}
+    out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
+    return out
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_env()
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import ed_lattice_b200 as E
+    from ed_lattice_b200 import _edgpu_lib as L
+
+    lib = L.lib()
+    model = E.Model(E.square_lattice(LX, LY), uloc=U, xmu=U / 2, hfmode=False)
+    sector = E.Sector(model, NUP, NDW, E.EDG_FORM_STORED)
+    D = sector.dim
+    stream = torch.cuda.current_stream()
+    L.check(lib.edg_sector_set_stream(sector.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1234 + rank)
+    v = torch.rand(D, device="cuda", dtype=torch.float32, generator=g) * 2 - 1
+    hv = torch.empty_like(v)
+    vp, hp = C.c_void_p(v.data_ptr()), C.c_void_p(hv.data_ptr())
+    for _ in range(max(3, args.warmup)):
+        L.check(lib.edg_hxv_dev_f32(sector.handle, vp, hp), "hxv")
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record()
+        for k in range(args.steps):
+            ev[k][0].record()
+            L.check(lib.edg_hxv_dev_f32(sector.handle, vp, hp), "hxv")
+            ev[k][1].record()
+        t_end.record()
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    per_launch = [a.elapsed_time(b) for a, b in ev]
+    t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    alg_bytes = 2 * D * 4
+    value = ws * args.steps * alg_bytes / (total_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    avg_launch_ms = float(np.mean(per_launch))
+    achieved = alg_bytes / (avg_launch_ms * 1e-3) / 1e9
+
+    # e2e through the reference-facing dd_sparse_HxV (complex(8) host vectors, pinned)
+    e2e = None
+    if not args.no_e2e:
+        zin = torch.empty(2 * D, dtype=torch.float64).pin_memory()
+        zout = torch.empty(2 * D, dtype=torch.float64).pin_memory()
+        zin.copy_(torch.rand(2 * D, dtype=torch.float64, generator=torch.Generator().manual_seed(5)) * 2 - 1)
+        zi = C.cast(C.c_void_p(zin.data_ptr()), L._pd)
+        zo = C.cast(C.c_void_p(zout.data_ptr()), L._pd)
+        L.check(lib.edg_hxv_z(sector.handle, D, zi, zo), "hxv_z")  # warm: staging buffers
+        ksteps = max(3, min(args.steps, 10))
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ksteps):
+            L.check(lib.edg_hxv_z(sector.handle, D, zi, zo), "hxv_z")
+        torch.cuda.synchronize()
+        dt = torch.tensor([time.perf_counter() - t0], device="cuda", dtype=torch.float64)
+        if ws > 1:
+            dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+        e2e = {"value": round(ws * ksteps * alg_bytes / float(dt.item()) / 1e9, 4), "unit": UNIT,
+               "h2d_bytes_per_step": 16 * D, "d2h_bytes_per_step": 16 * D, "steps": ksteps,
+               "entry": "edg_hxv_z (dd_sparse_HxV drop-in, complex(8) host vectors, FP64 H x v)"}
+        del zin, zout
+
+    extra = {}
+    if rank == 0 and not args.no_e0 and ws == 1:
+        del v, hv
+        torch.cuda.empty_cache()
+        extra["e0_time_to_1e-8"] = e0_time_to_solution(E, L, sector)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        val, info = cpu_baseline_sample()
+        cpu = {"value": round(val, 4), "unit": UNIT, **info}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lattice": "4x4 periodic square", "t": 1.0, "U": U, "nup": NUP,
+                       "ndw": NDW, "dim": D, "form": "stored", "vector_bytes": D * 4,
+                       "l2_policy": "inputs larger than L2 (662 MB per vector), no flush",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "hbm", "kernel": "hxv_f32 (k_dw_slab + k_up_rows, one H x v)",
+                         "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_launch_ms,
+                         "traffic": None},
+            "clocks": clk.summary(),
+            "gpu_launches": 2 * args.steps,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            **extra,
+        }
+        print(json.dumps(line), flush=True)
+    sector.delete()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-e0", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,327 @@
+// basis.cu -- sector Fock basis, index maps and hop tables built on the device.
+//
+// Replaces build_sector (src/SECTOR.f90:69-115), the binary_search rank lookup
+// (src/AUX_FUNX.f90:163-180) and the table construction of ed_buildh
+// (src/DIAG/HAMILTONIAN_STORED_HxV.f90:21-126 with stored/H_local.f90, H_up.f90, H_dw.f90).
+//
+// Basis: the reference scans 0..2^Ns-1 and keeps popcount==N in ascending order. The same
+// list is produced here without the 2^Ns scan: rank r -> bitstring by combinatorial
+// unranking at the start of each thread's chunk, then Gosper's next-permutation step.
+// Rank of a bitstring with set bits p_1<...<p_N is sum_i C(p_i, i) (the combinatorial number
+// system), which equals its position in ascending order, i.e. binary_search's result - 1.
+//
+// Hop tables: gather form over target rows. For a target configuration t and a directed
+// bond (a,b) with a occupied and b empty in t, the source is s = t - 2^a + 2^b and
+// <t|H_sigma|s> = h(a,b) * (-1)^{popcount of t strictly between a and b}, which is the
+// product sg1*sg2 of c(b) then cdg(a) in the reference (src/AUX_FUNX.f90:76-102).
+// h(a,b) = Hij(a,b) for the direct form (direct/HxV_up.f90:24) and conjg(Hij(a,b)) for the
+// stored form (stored/H_up.f90:20); both are real on the device.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace edg {
+
+namespace {
+thread_local char g_err[512] = "";
+}
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+const char* get_error() { return g_err; }
+
+// HBM admission: keep this many bytes free for the CUDA context, cuBLAS-free driver
+// state and other users of the device.
+static const size_t kReserveBytes = size_t(1) << 30;
+
+int dev_alloc(void** p, size_t bytes, const char* what) {
+  *p = nullptr;
+  if (bytes == 0) return EDG_OK;
+  size_t freeb = 0, totalb = 0;
+  cudaError_t e = cudaMemGetInfo(&freeb, &totalb);
+  if (e != cudaSuccess) {
+    set_error("cudaMemGetInfo: %s", cudaGetErrorString(e));
+    return EDG_ERR_CUDA;
+  }
+  if (bytes + kReserveBytes > freeb) {
+    set_error("HBM admission refused for %s: %zu bytes requested, %zu free", what, bytes, freeb);
+    return EDG_ERR_NOMEM;
+  }
+  e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_error("cudaMalloc(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
+    *p = nullptr;
+    return EDG_ERR_NOMEM;
+  }
+  return EDG_OK;
+}
+
+void dev_free(void* p) {
+  if (p) cudaFree(p);
+}
+
+uint64_t binom_host(int n, int k) {
+  if (k < 0 || k > n || n < 0) return 0;
+  uint64_t r = 1;
+  for (int i = 1; i <= k; ++i) r = r * uint64_t(n + 1 - i) / uint64_t(i);
+  return r;
+}
+
+namespace {
+
+struct EnergyParams {
+  double eps[kMaxSites];  // Hdiag(io) - shift
+};
+
+__device__ __forceinline__ uint32_t binom_dev(const uint32_t* C, int n, int k) { return C[n * kBinomN + k]; }
+
+__device__ __forceinline__ uint32_t rank_of(uint32_t s, const uint32_t* C) {
+  uint32_t r = 0;
+  int i = 1;
+  while (s) {
+    int p = __ffs(s) - 1;
+    r += binom_dev(C, p, i);
+    ++i;
+    s &= s - 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t unrank(uint64_t r, int k, int ns, const uint32_t* C) {
+  uint32_t s = 0;
+  for (int i = k; i >= 1; --i) {
+    int p = i - 1;
+    while (p + 1 < ns && binom_dev(C, p + 1, i) <= r) ++p;
+    s |= 1u << p;
+    r -= binom_dev(C, p, i);
+  }
+  return s;
+}
+
+__device__ __forceinline__ uint32_t gosper_next(uint32_t s) {
+  uint32_t c = s & (0u - s);
+  uint32_t r = s + c;
+  return (((r ^ s) >> 2) / c) | r;
+}
+
+constexpr int kEnumChunk = 64;
+
+__global__ void k_enum_map(uint32_t* map, int64_t dim, int k, int ns, const uint32_t* C) {
+  int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  int64_t start = t * kEnumChunk;
+  if (start >= dim) return;
+  int64_t cnt = dim - start < kEnumChunk ? dim - start : kEnumChunk;
+  uint32_t s = unrank(uint64_t(start), k, ns, C);
+  for (int64_t j = 0; j < cnt; ++j) {
+    map[start + j] = s;
+    if (j + 1 < cnt) s = gosper_next(s);
+  }
+}
+
+__global__ void k_local_energy(const uint32_t* map, int64_t dim, EnergyParams ep, double* e64, float* e32) {
+  int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= dim) return;
+  uint32_t s = map[r];
+  double e = 0.0;
+  while (s) {
+    int p = __ffs(s) - 1;
+    e += ep.eps[p];
+    s &= s - 1;
+  }
+  e64[r] = e;
+  e32[r] = float(e);
+}
+
+
+__global__ void k_hop_count(const uint32_t* map, int64_t dim, const int32_t* bonds, int nb, uint32_t* cnt) {
+  int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= dim) return;
+  uint32_t t = map[r];
+  uint32_t c = 0;
+  for (int k = 0; k < nb; ++k) {
+    int a = bonds[2 * k], b = bonds[2 * k + 1];
+    c += ((t >> a) & 1u) & (((t >> b) & 1u) ^ 1u);
+  }
+  cnt[r] = c;
+}
+
+__device__ __forceinline__ int between_parity(uint32_t t, int a, int b) {
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  uint32_t mask = ((hi >= 32 ? 0u : (1u << hi)) - 1u) & ~((2u << lo) - 1u);
+  return __popc(t & mask) & 1;
+}
+
+__global__ void k_hop_fill(const uint32_t* map, int64_t dim, const int32_t* bonds, const double* bh, int nb,
+                           const uint32_t* C, const uint32_t* off, uint32_t* src, double* v64, float* v32) {
+  int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= dim) return;
+  uint32_t t = map[r];
+  uint32_t o = off[r];
+  uint32_t n = 0;
+  for (int k = 0; k < nb; ++k) {
+    int a = bonds[2 * k], b = bonds[2 * k + 1];
+    if (((t >> a) & 1u) && !((t >> b) & 1u)) {
+      uint32_t s = (t & ~(1u << a)) | (1u << b);
+      double v = between_parity(t, a, b) ? -bh[k] : bh[k];
+      uint32_t j = rank_of(s, C);
+      // insertion into the row, ascending source rank (the reference's summation order)
+      uint32_t pos = n;
+      while (pos > 0 && src[o + pos - 1] > j) {
+        src[o + pos] = src[o + pos - 1];
+        v64[o + pos] = v64[o + pos - 1];
+        --pos;
+      }
+      src[o + pos] = j;
+      v64[o + pos] = v;
+      ++n;
+    }
+  }
+  for (uint32_t q = 0; q < n; ++q) v32[o + q] = float(v64[o + q]);
+}
+
+int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
+  const int ns = s->model.ns;
+  B.nel = nel;
+  B.dim = int64_t(binom_host(ns, nel));
+  cudaStream_t st = s->stream;
+  EDG_CHECK(B.map.alloc(B.dim, "basis map"));
+  {
+    int64_t nthr = (B.dim + kEnumChunk - 1) / kEnumChunk;
+    int blocks = int((nthr + 255) / 256);
+    k_enum_map<<<blocks, 256, 0, st>>>(B.map.p, B.dim, nel, ns, s->binom.p);
+    EDG_CUDA(cudaGetLastError());
+  }
+  // local energies: Hdiag(io) = Re Hij(spin,io,io); the xmu / Hartree shift is applied
+  // always in the stored form (stored/H_local.f90:62-89) and only for ed_filling==0 in the
+  // direct form (direct/HxV_local.f90:63-92).
+  const edg_model_s& m = s->model;
+  const int sp = (m.nspin == 2) ? spin - 1 : 0;
+  bool apply_shift = (s->form == EDG_FORM_STORED) || (m.ed_filling == 0);
+  double shift = 0.0;
+  if (apply_shift) {
+    shift = m.xmu;
+    if (m.hfmode && m.uloc != 0.0) shift += 0.5 * m.uloc;
+  }
+  EnergyParams ep{};
+  for (int io = 0; io < ns; ++io) ep.eps[io] = m.hre[sp][io * ns + io] - shift;
+  EDG_CHECK(B.e64.alloc(B.dim, "local energies"));
+  EDG_CHECK(B.e32.alloc(B.dim, "local energies"));
+  {
+    int blocks = int((B.dim + 255) / 256);
+    k_local_energy<<<blocks, 256, 0, st>>>(B.map.p, B.dim, ep, B.e64.p, B.e32.p);
+    EDG_CUDA(cudaGetLastError());
+  }
+  // directed bond list (a created, b annihilated): Hij(a,b) != 0, a != b
+  BondList& bl = s->bonds[spin - 1];
+  bl = BondList();
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b < ns; ++b) {
+      if (a == b) continue;
+      double h = m.hre[sp][a * ns + b];
+      double hi = m.him[sp].empty() ? 0.0 : m.him[sp][a * ns + b];
+      if (h == 0.0 && hi == 0.0) continue;
+      bl.a.push_back(a);
+      bl.b.push_back(b);
+      bl.h.push_back(h);  // real part; the imaginary part is rejected at model level
+    }
+  bl.nb = int(bl.a.size());
+  // Order bonds by d = 2^b - 2^a: the source of a hop is target + d, so this order yields
+  // every row's sources in ascending rank (the reference's summation order) for free.
+  std::vector<int> ord(bl.nb);
+  for (int k = 0; k < bl.nb; ++k) ord[k] = k;
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) {
+    const int64_t dx = (int64_t(1) << bl.b[x]) - (int64_t(1) << bl.a[x]);
+    const int64_t dy = (int64_t(1) << bl.b[y]) - (int64_t(1) << bl.a[y]);
+    return dx < dy;
+  });
+  BondList sorted;
+  for (int k : ord) { sorted.a.push_back(bl.a[k]); sorted.b.push_back(bl.b[k]); sorted.h.push_back(bl.h[k]); }
+  sorted.nb = bl.nb;
+  bl = sorted;
+  return EDG_OK;
+}
+
+int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
+  cudaStream_t st = s->stream;
+  const BondList& bl = s->bonds[spin - 1];
+  const int nb = bl.nb;
+  DevBuf<int32_t> bonds;
+  DevBuf<double> bh;
+  std::vector<int32_t> hb(2 * nb + 2);
+  for (int k = 0; k < nb; ++k) { hb[2 * k] = bl.a[k]; hb[2 * k + 1] = bl.b[k]; }
+  EDG_CHECK(bonds.alloc(hb.size(), "bond list"));
+  EDG_CHECK(bh.alloc(nb + 1, "bond values"));
+  EDG_CUDA(cudaMemcpyAsync(bonds.p, hb.data(), hb.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  if (nb) EDG_CUDA(cudaMemcpyAsync(bh.p, bl.h.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+  EDG_CHECK(B.off.alloc(B.dim + 1, "hop offsets"));
+  DevBuf<uint32_t> cnt;
+  EDG_CHECK(cnt.alloc(B.dim, "hop counts"));
+  int blocks = int((B.dim + 255) / 256);
+  k_hop_count<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, nb, cnt.p);
+  EDG_CUDA(cudaGetLastError());
+  EDG_CUDA(cudaMemsetAsync(B.off.p, 0, sizeof(uint32_t), st));
+  size_t tmp_bytes = 0;
+  EDG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, cnt.p, B.off.p + 1, B.dim, st));
+  DevBuf<unsigned char> tmp;
+  EDG_CHECK(tmp.alloc(tmp_bytes + 1, "scan scratch"));
+  EDG_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, cnt.p, B.off.p + 1, B.dim, st));
+  uint32_t nnz = 0;
+  EDG_CUDA(cudaMemcpyAsync(&nnz, B.off.p + B.dim, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  B.nnz = nnz;
+  EDG_CHECK(B.src.alloc(nnz + 1, "hop sources"));
+  EDG_CHECK(B.val64.alloc(nnz + 1, "hop values"));
+  EDG_CHECK(B.val32.alloc(nnz + 1, "hop values"));
+  k_hop_fill<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, bh.p, nb, s->binom.p, B.off.p, B.src.p, B.val64.p,
+                                     B.val32.p);
+  EDG_CUDA(cudaGetLastError());
+  EDG_CUDA(cudaStreamSynchronize(st));
+  return EDG_OK;
+}
+
+}  // namespace
+
+int sector_build(edg_sector_s* s) {
+  // exact binomial table C(n,k), n,k < kBinomN
+  std::vector<uint32_t> C(kBinomN * kBinomN, 0);
+  for (int n = 0; n < kBinomN; ++n)
+    for (int k = 0; k < kBinomN; ++k) C[n * kBinomN + k] = uint32_t(binom_host(n, k));
+  EDG_CHECK(s->binom.alloc(C.size(), "binomial table"));
+  EDG_CUDA(cudaMemcpyAsync(s->binom.p, C.data(), C.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
+  EDG_CHECK(build_spin(s, 1, s->up, s->nup));
+  EDG_CHECK(build_spin(s, 2, s->dw, s->ndw));
+  s->dim = s->up.dim * s->dw.dim;
+  s->U = s->model.uloc;
+  if (s->form == EDG_FORM_STORED) {
+    EDG_CHECK(build_tables(s, 1, s->up));
+    EDG_CHECK(build_tables(s, 2, s->dw));
+  } else {
+    // direct form: bond lists only (both spins packed: [spin][k] -> a,b ; values)
+    std::vector<int32_t> hb;
+    std::vector<double> hv;
+    for (int sp = 0; sp < 2; ++sp) {
+      const BondList& bl = s->bonds[sp];
+      for (int k = 0; k < bl.nb; ++k) { hb.push_back(bl.a[k]); hb.push_back(bl.b[k]); hv.push_back(bl.h[k]); }
+    }
+    EDG_CHECK(s->bond_dev.alloc(hb.size() + 2, "bond list"));
+    EDG_CHECK(s->bondh_dev.alloc(hv.size() + 1, "bond values"));
+    if (!hb.empty()) {
+      EDG_CUDA(cudaMemcpyAsync(s->bond_dev.p, hb.data(), hb.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
+      EDG_CUDA(cudaMemcpyAsync(s->bondh_dev.p, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    }
+  }
+  EDG_CUDA(cudaStreamSynchronize(s->stream));
+  return EDG_OK;
+}
+
+}  // namespace edg

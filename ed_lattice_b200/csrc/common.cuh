@@ -1,0 +1,162 @@
+// common.cuh -- internal types of the sector-Lanczos engine (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/edgpu.h"
+
+namespace edg {
+
+constexpr int kMaxSites = 30;       // bitstrings fit int32 like the reference's `integer` maps
+constexpr int kBinomN = kMaxSites + 2;
+
+// Thread-local last-error text for edg_last_error().
+void set_error(const char* fmt, ...);
+const char* get_error();
+
+#define EDG_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      ::edg::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+      return EDG_ERR_CUDA;                                                              \
+    }                                                                                   \
+  } while (0)
+
+#define EDG_CHECK(expr)          \
+  do {                           \
+    int s_ = (expr);             \
+    if (s_ != EDG_OK) return s_; \
+  } while (0)
+
+// Device allocation with HBM admission: refuse when the request would leave less than
+// `reserve` bytes free, instead of letting cudaMalloc fail half-way through a pipeline.
+int dev_alloc(void** p, size_t bytes, const char* what);
+void dev_free(void* p);
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  int alloc(size_t count, const char* what) {
+    if (n >= count && p) return EDG_OK;
+    reset();
+    if (count == 0) return EDG_OK;
+    int s = dev_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), what);
+    if (s == EDG_OK) n = count;
+    return s;
+  }
+  void reset() {
+    if (p) dev_free(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// One spin species of a sector: basis maps, local energies and the gather hop table.
+struct SpinBasis {
+  int nel = 0;                  // Nup or Ndw
+  int64_t dim = 0;              // C(Ns, nel)
+  DevBuf<uint32_t> map;         // ascending bitstrings [dim]
+  DevBuf<double> e64;           // local one-body energy of each configuration [dim]
+  DevBuf<float> e32;
+  // Gather hop table over target rows: row r lists (source rank, value) with
+  // <r|H_sigma|src> = value, sources ascending. FORM_DIRECT keeps no table.
+  DevBuf<uint32_t> off;         // [dim+1]
+  DevBuf<uint32_t> src;         // [nnz]
+  DevBuf<double> val64;         // [nnz]
+  DevBuf<float> val32;
+  int64_t nnz = 0;
+};
+
+// Directed bond list for one spin: Hij(a,b) != 0, a != b, value = matrix element used when
+// an electron moves from b to a (direct form Hij(a,b), stored form conjg(Hij(a,b))).
+struct BondList {
+  int nb = 0;
+  std::vector<int> a, b;
+  std::vector<double> h;
+};
+
+}  // namespace edg
+
+struct edg_model_s {
+  int ns = 0, nspin = 1;
+  std::vector<double> hre[2], him[2];  // [spin-1][io*ns+jo]
+  bool complex_hij = false;
+  double uloc = 0, xmu = 0;
+  int hfmode = 0, ed_filling = 0;
+};
+
+struct edg_sector_s {
+  edg_model_s model;     // private copy: a sector outlives nothing it depends on
+  int nup = 0, ndw = 0, form = EDG_FORM_STORED;
+  int device = 0;
+  int64_t dim = 0;
+  edg::SpinBasis up, dw;
+  edg::BondList bonds[2];
+  edg::DevBuf<uint32_t> binom;    // C(n,k) table [kBinomN*kBinomN], exact integers
+  edg::DevBuf<int32_t> bond_dev;  // device bond list for the direct form: [spin][a,b] packed
+  edg::DevBuf<double> bondh_dev;
+  double U = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  // work space of the Lanczos drivers (grown on demand, freed with the sector)
+  edg::DevBuf<double> w64[4];
+  edg::DevBuf<float> w32[4];
+  edg::DevBuf<double> red;        // reduction partials + device scalars
+  edg::DevBuf<double> state;      // FP64 eigenvector kept on the device (ground_state_keep)
+  edg::DevBuf<double> zstage;     // interleaved complex staging of the dd_sparse_HxV entry
+  edg::DevBuf<float> basis32;     // FP32 Lanczos basis for Ritz vectors
+  size_t basis32_cols = 0;
+  bool has_state = false;
+};
+
+namespace edg {
+
+// ---- basis.cu
+int sector_build(edg_sector_s* s);
+uint64_t binom_host(int n, int k);
+
+// ---- hxv.cu
+template <typename T>
+int hxv_apply(edg_sector_s* s, const T* v, T* hv);
+
+// ---- vecops.cu
+constexpr int kRedBlocks = 592;  // 148 SMs x 4: fixed reduction grid (deterministic sums)
+constexpr int kRedThreads = 256;
+template <typename T>
+int dot_dev(cudaStream_t st, const T* x, const T* y, int64_t n, double* partial, double* out);
+template <typename T>
+int lanczos_step_a(cudaStream_t st, T* w, const T* vprev, const T* v, const double* bprev, int64_t n,
+                   double* partial, double* aout);
+template <typename T>
+int lanczos_step_b(cudaStream_t st, T* w, const T* v, const double* a, int64_t n, double* partial,
+                   double* bout);
+template <typename T>
+int scale_into(cudaStream_t st, T* dst, const T* src, const double* b, int64_t n);
+template <typename TD, typename TS>
+int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale);
+template <typename TD>
+int axpy_accum_dev(cudaStream_t st, double* dst, const TD* x, double coef, int64_t n);
+int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed);
+uint64_t splitmix64(uint64_t x);
+
+// ---- lanczos.cu
+int tridiag_dev(edg_sector_s* s, const double* dv0, int nlanc, double threshold, int precision,
+                double* alanc, double* blanc, double* norm2, int* nsteps);
+int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
+                 double* e0, int* niter);
+
+// ---- tridiag_host.cpp
+int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull);
+
+}  // namespace edg

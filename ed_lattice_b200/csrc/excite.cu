@@ -1,0 +1,295 @@
+// excite.cu -- excitation operators and static observables on device vectors.
+//
+//  c^+ / c   : apply_op_CDG / apply_op_C (src/SECTOR.f90:217-268) over a whole vector as in
+//              lanc_build_gf_electrons_diag (src/GF/GF_ELECTRONS.f90:241-245,267-271). In the
+//              spin-factorised layout they are a signed permutation along one index: along iup
+//              (within rows) for spin up, of whole rows for spin down.
+//  S^z / N   : apply_op_Sz / apply_op_N (src/SECTOR.f90:271-341), diagonal scalings, with an
+//              optional real site-weight vector for momentum combinations (cos(q.r)).
+//  J         : the current of lanc_ed_build_oc (src/OC/OC_ELECTRONS.f90:139-205).
+//  observables: lanc_observables (src/OBSERVABLES.f90:127-152), per-site moments of |psi|^2.
+#include "common.cuh"
+
+namespace edg {
+namespace {
+
+__device__ __forceinline__ uint32_t rank_c(uint32_t s, const uint32_t* C) {
+  uint32_t r = 0;
+  int i = 1;
+  while (s) {
+    int p = __ffs(s) - 1;
+    r += C[p * kBinomN + i];
+    ++i;
+    s &= s - 1;
+  }
+  return r;
+}
+
+// For every target configuration (rank jr in the destination basis of one spin): source
+// rank in the origin basis (or -1) and the fermionic sign of c^+/c at `pos` (0-based).
+__global__ void k_cop_table(const uint32_t* mapJ, int64_t dimJ, int pos, int op, const uint32_t* C, int64_t* srcI,
+                            double* sgn) {
+  int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (j >= dimJ) return;
+  const uint32_t t = mapJ[j];
+  const uint32_t bit = 1u << pos;
+  uint32_t s;
+  if (op > 0) {  // t = cdg(pos) s : t has pos set, s has it clear
+    if (!(t & bit)) { srcI[j] = -1; sgn[j] = 0.0; return; }
+    s = t & ~bit;
+  } else {  // t = c(pos) s : t has pos clear, s has it set
+    if (t & bit) { srcI[j] = -1; sgn[j] = 0.0; return; }
+    s = t | bit;
+  }
+  srcI[j] = int64_t(rank_c(s, C));
+  sgn[j] = (__popc(s & (bit - 1u)) & 1) ? -1.0 : 1.0;  // bits below pos (src/AUX_FUNX.f90:84-86)
+}
+
+// spin up: out[jdw][jup] (+)= coef * sgn[jup] * in[jdw][src[jup]]
+__global__ void k_cop_up(const double* __restrict__ in, double* __restrict__ out, int64_t dupI, int64_t dupJ,
+                         int64_t ddw, const int64_t* __restrict__ src, const double* __restrict__ sg, double coef,
+                         int accumulate) {
+  for (int64_t row = blockIdx.x; row < ddw; row += gridDim.x) {
+    const double* ir = in + row * dupI;
+    double* orow = out + row * dupJ;
+    for (int64_t j = threadIdx.x; j < dupJ; j += blockDim.x) {
+      const int64_t sidx = src[j];
+      const double v = sidx >= 0 ? coef * sg[j] * ir[sidx] : 0.0;
+      if (accumulate) orow[j] += v; else orow[j] = v;
+    }
+  }
+}
+
+// spin down: out[jdw][:] (+)= coef * sgn[jdw] * in[src[jdw]][:]
+__global__ void k_cop_dw(const double* __restrict__ in, double* __restrict__ out, int64_t dup, int64_t ddwJ,
+                         const int64_t* __restrict__ src, const double* __restrict__ sg, double coef, int accumulate) {
+  for (int64_t row = blockIdx.x; row < ddwJ; row += gridDim.x) {
+    const int64_t sidx = src[row];
+    const double f = sidx >= 0 ? coef * sg[row] : 0.0;
+    const double* ir = in + (sidx >= 0 ? sidx : 0) * dup;
+    double* orow = out + row * dup;
+    for (int64_t j = threadIdx.x; j < dup; j += blockDim.x) {
+      const double v = sidx >= 0 ? f * ir[j] : 0.0;
+      if (accumulate) orow[j] += v; else orow[j] = v;
+    }
+  }
+}
+
+// per-configuration site sums f[r] = sum_i w_i n_i(map[r])
+__global__ void k_site_sum(const uint32_t* map, int64_t dim, const double* w, int ns, double* f) {
+  int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (r >= dim) return;
+  uint32_t s = map[r];
+  double acc = 0.0;
+  for (int i = 0; i < ns; ++i)
+    if ((s >> i) & 1u) acc += w[i];
+  f[r] = acc;
+}
+
+// out = (kind 0: (fu - fd)/2 ; kind 1: fu + fd) * in
+__global__ void k_diagop(const double* __restrict__ in, double* __restrict__ out, int64_t dup, int64_t ddw,
+                         const double* __restrict__ fu, const double* __restrict__ fd, int kind) {
+  for (int64_t row = blockIdx.x; row < ddw; row += gridDim.x) {
+    const double d = fd[row];
+    for (int64_t j = threadIdx.x; j < dup; j += blockDim.x) {
+      const double f = kind == 0 ? (fu[j] - d) / 2.0 : fu[j] + d;
+      out[row * dup + j] = f * in[row * dup + j];
+    }
+  }
+}
+
+// Signed hop operator sum_k coef_k T(a_k <- b_k) of one spin, gather form (J of the OC builder).
+struct HopOp {
+  int nb;
+  int a[2 * kMaxSites];
+  int b[2 * kMaxSites];
+  double c[2 * kMaxSites];
+};
+
+__device__ __forceinline__ int parity_between(uint32_t t, int a, int b) {
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  uint32_t mask = ((1u << hi) - 1u) & ~((2u << lo) - 1u);
+  return __popc(t & mask) & 1;
+}
+
+__global__ void k_hopop(const double* __restrict__ in, double* __restrict__ out, int64_t dup, int64_t ddw,
+                        const uint32_t* mup, const uint32_t* mdw, const uint32_t* C, HopOp hu, HopOp hd) {
+  const int64_t n = dup * ddw;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t idw = e / dup, iup = e - idw * dup;
+    const uint32_t tu = mup[iup], td = mdw[idw];
+    double acc = 0.0;
+    for (int k = 0; k < hu.nb; ++k) {
+      const int a = hu.a[k], b = hu.b[k];
+      if (((tu >> a) & 1u) && !((tu >> b) & 1u)) {
+        const uint32_t s = (tu & ~(1u << a)) | (1u << b);
+        const double sg = parity_between(tu, a, b) ? -1.0 : 1.0;
+        acc += hu.c[k] * sg * in[idw * dup + rank_c(s, C)];
+      }
+    }
+    for (int k = 0; k < hd.nb; ++k) {
+      const int a = hd.a[k], b = hd.b[k];
+      if (((td >> a) & 1u) && !((td >> b) & 1u)) {
+        const uint32_t s = (td & ~(1u << a)) | (1u << b);
+        const double sg = parity_between(td, a, b) ? -1.0 : 1.0;
+        acc += hd.c[k] * sg * in[int64_t(rank_c(s, C)) * dup + iup];
+      }
+    }
+    out[e] = acc;
+  }
+}
+
+// Observables: one CTA per row idw; per-site sums of |psi|^2 weighted by the up bits, then
+// combined with the down bits of the row. out layout per block: [5][kMaxSites].
+__global__ void __launch_bounds__(256) k_obs_rows(const double* __restrict__ psi, int64_t dup, int64_t ddw,
+                                                  const uint32_t* mup, const uint32_t* mdw, int ns,
+                                                  double* __restrict__ partial) {
+  __shared__ double sq[8][kMaxSites + 1];
+  __shared__ double blk[3][kMaxSites];
+  double acc_up[kMaxSites];
+  double acc_tot = 0.0;
+  for (int i = threadIdx.x; i < 3 * kMaxSites; i += blockDim.x) (&blk[0][0])[i] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t row = blockIdx.x; row < ddw; row += gridDim.x) {
+#pragma unroll
+    for (int i = 0; i < kMaxSites; ++i) acc_up[i] = 0.0;
+    acc_tot = 0.0;
+    for (int64_t j = threadIdx.x; j < dup; j += blockDim.x) {
+      const double p = psi[row * dup + j];
+      const double w = p * p;
+      const uint32_t u = mup[j];
+      acc_tot += w;
+#pragma unroll
+      for (int i = 0; i < kMaxSites; ++i) acc_up[i] += ((u >> i) & 1u) ? w : 0.0;
+    }
+    // block reduce (kMaxSites + 1 values)
+#pragma unroll
+    for (int i = 0; i <= kMaxSites; ++i) {
+      double v = i < kMaxSites ? acc_up[i] : acc_tot;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) sq[wid][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t d = mdw[row];
+      double tot = 0.0;
+      for (int w8 = 0; w8 < 8; ++w8) tot += sq[w8][kMaxSites];
+      for (int i = 0; i < ns; ++i) {
+        double qu = 0.0;
+        for (int w8 = 0; w8 < 8; ++w8) qu += sq[w8][i];
+        const double nd = double((d >> i) & 1u);
+        blk[0][i] += qu;
+        blk[1][i] += nd * tot;
+        blk[2][i] += nd * qu;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double* o = partial + int64_t(blockIdx.x) * 3 * kMaxSites;
+    for (int i = 0; i < kMaxSites; ++i) {
+      o[i] = blk[0][i];
+      o[kMaxSites + i] = blk[1][i];
+      o[2 * kMaxSites + i] = blk[2][i];
+    }
+  }
+}
+
+int grid_rows(int64_t rows) { return int(rows < 148 * 8 ? (rows < 1 ? 1 : rows) : 148 * 8); }
+
+}  // namespace
+
+int apply_cop(const edg_sector_s* from, const edg_sector_s* to, int op, int site, int spin, double coef,
+              int accumulate, const double* din, double* dout, cudaStream_t st) {
+  const int pos = site - 1;
+  const SpinBasis& BJ = spin == 1 ? to->up : to->dw;
+  DevBuf<int64_t> src;
+  DevBuf<double> sg;
+  EDG_CHECK(src.alloc(BJ.dim, "c-op table"));
+  EDG_CHECK(sg.alloc(BJ.dim, "c-op table"));
+  k_cop_table<<<int((BJ.dim + 255) / 256), 256, 0, st>>>(BJ.map.p, BJ.dim, pos, op, to->binom.p, src.p, sg.p);
+  EDG_CUDA(cudaGetLastError());
+  if (spin == 1) {
+    k_cop_up<<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, from->up.dim, to->up.dim, to->dw.dim, src.p, sg.p,
+                                                    coef, accumulate);
+  } else {
+    k_cop_dw<<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, to->up.dim, to->dw.dim, src.p, sg.p, coef,
+                                                    accumulate);
+  }
+  EDG_CUDA(cudaGetLastError());
+  EDG_CUDA(cudaStreamSynchronize(st));  // tables are freed on return
+  return EDG_OK;
+}
+
+int apply_diagop(const edg_sector_s* s, int kind, const double* wsite, const double* din, double* dout,
+                 cudaStream_t st) {
+  const int ns = s->model.ns;
+  DevBuf<double> w, fu, fd;
+  EDG_CHECK(w.alloc(ns, "site weights"));
+  EDG_CHECK(fu.alloc(s->up.dim, "site sums"));
+  EDG_CHECK(fd.alloc(s->dw.dim, "site sums"));
+  EDG_CUDA(cudaMemcpyAsync(w.p, wsite, ns * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_site_sum<<<int((s->up.dim + 255) / 256), 256, 0, st>>>(s->up.map.p, s->up.dim, w.p, ns, fu.p);
+  k_site_sum<<<int((s->dw.dim + 255) / 256), 256, 0, st>>>(s->dw.map.p, s->dw.dim, w.p, ns, fd.p);
+  k_diagop<<<grid_rows(s->dw.dim), 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, fu.p, fd.p, kind);
+  EDG_CUDA(cudaGetLastError());
+  EDG_CUDA(cudaStreamSynchronize(st));
+  return EDG_OK;
+}
+
+// J along the site chain 1-2-...-Ns-1 (Norb=1): for each isite, jsite=isite+1 (periodic),
+// + Hij(isite,jsite) c^+_isite c_jsite - conjg(Hij(jsite,isite)) c^+_jsite c_isite, per spin,
+// skipped where Hij is zero (src/OC/OC_ELECTRONS.f90:153-198). Returns r with J|psi> = i r.
+int apply_current(const edg_sector_s* s, const double* din, double* dout, cudaStream_t st) {
+  const edg_model_s& m = s->model;
+  const int ns = m.ns;
+  HopOp h[2];
+  for (int sp = 0; sp < 2; ++sp) {
+    const int idx = (m.nspin == 2) ? sp : 0;
+    h[sp].nb = 0;
+    for (int isite = 0; isite < ns; ++isite) {
+      const int jsite = (isite + 1 == ns) ? 0 : isite + 1;
+      const double t1 = m.hre[idx][isite * ns + jsite];  // Hij(io=isite, jo=jsite)
+      if (t1 != 0.0) { h[sp].a[h[sp].nb] = isite; h[sp].b[h[sp].nb] = jsite; h[sp].c[h[sp].nb] = t1; ++h[sp].nb; }
+      const double t2 = m.hre[idx][jsite * ns + isite];  // Hij(io=jsite, jo=isite)
+      if (t2 != 0.0) { h[sp].a[h[sp].nb] = jsite; h[sp].b[h[sp].nb] = isite; h[sp].c[h[sp].nb] = -t2; ++h[sp].nb; }
+    }
+  }
+  const int64_t n = s->dim;
+  int g = int((n + 255) / 256);
+  if (g > 148 * 8) g = 148 * 8;
+  k_hopop<<<g, 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, s->binom.p, h[0], h[1]);
+  EDG_CUDA(cudaGetLastError());
+  EDG_CUDA(cudaStreamSynchronize(st));
+  return EDG_OK;
+}
+
+int observables(const edg_sector_s* s, const double* psi, double weight, double* dens, double* dens_up,
+                double* dens_dw, double* docc, double* magz, cudaStream_t st) {
+  const int ns = s->model.ns;
+  const int g = grid_rows(s->dw.dim);
+  DevBuf<double> part;
+  EDG_CHECK(part.alloc(size_t(g) * 3 * kMaxSites, "observable partials"));
+  k_obs_rows<<<g, 256, 0, st>>>(psi, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, ns, part.p);
+  EDG_CUDA(cudaGetLastError());
+  std::vector<double> h(size_t(g) * 3 * kMaxSites);
+  EDG_CUDA(cudaMemcpyAsync(h.data(), part.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < ns; ++i) {
+    double u = 0, d = 0, dd = 0;
+    for (int b = 0; b < g; ++b) {
+      u += h[size_t(b) * 3 * kMaxSites + i];
+      d += h[size_t(b) * 3 * kMaxSites + kMaxSites + i];
+      dd += h[size_t(b) * 3 * kMaxSites + 2 * kMaxSites + i];
+    }
+    if (dens_up) dens_up[i] += weight * u;
+    if (dens_dw) dens_dw[i] += weight * d;
+    if (dens) dens[i] += weight * (u + d);
+    if (docc) docc[i] += weight * dd;
+    if (magz) magz[i] += weight * (u - d);
+  }
+  return EDG_OK;
+}
+
+}  // namespace edg

@@ -1,0 +1,228 @@
+// hxv.cu -- the spin-factorised Hubbard H x v on the device.
+//
+// Hv = diag o v + (I (x) H_up) v + (H_dw (x) I) v, with v laid out as the reference's
+// i = iup + idw*DimUp: a row-major DimDw x DimUp matrix V whose rows are contiguous in iup.
+//  * diag(iup,idw) = Eup[iup] + Edw[idw] + U*popcount(mup & mdw)  (src/DIAG/direct/
+//    HxV_local.f90:15-95 and stored/H_local.f90:15-89, one orbital),
+//  * H_up acts inside each row: a gather along iup (direct/HxV_up.f90, spMatVec :193-207),
+//  * H_dw combines whole rows: row idw' += h * row jdw, coalesced along iup
+//    (direct/HxV_dw.f90, spMatVec :178-191).
+// Summation order per output element follows the reference form being replaced:
+//  STORED (spMatVec, src/DIAG/HAMILTONIAN_STORED_HxV.f90:159-220): diag, DW, UP;
+//  DIRECT (directMatVec, src/DIAG/HAMILTONIAN_DIRECT_HxV.f90:19-59): diag, UP, DW;
+// inside each spin part sources are added in ascending rank, as the reference's loops do.
+#include "common.cuh"
+
+namespace edg {
+namespace {
+
+template <typename T>
+struct HxvArgs {
+  const T* __restrict__ v;
+  T* __restrict__ hv;
+  int64_t dimup, dimdw;
+  const uint32_t* __restrict__ off_up;
+  const uint32_t* __restrict__ src_up;
+  const T* __restrict__ val_up;
+  const uint32_t* __restrict__ off_dw;
+  const uint32_t* __restrict__ src_dw;
+  const T* __restrict__ val_dw;
+  const T* __restrict__ e_up;
+  const T* __restrict__ e_dw;
+  const uint32_t* __restrict__ map_up;
+  const uint32_t* __restrict__ map_dw;
+  T U;
+};
+
+template <typename T>
+__device__ __forceinline__ T fmaT(T a, T b, T c);
+template <>
+__device__ __forceinline__ float fmaT<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <>
+__device__ __forceinline__ double fmaT<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Row pass: one CTA per row idw (grid-stride), threads along iup. H_up gathers hit L1/L2
+// (a row is DimUp*sizeof(T) bytes). FIRST: hv = diag*v + up-part; else hv += up-part.
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(256) k_up_rows(HxvArgs<T> a) {
+  for (int64_t idw = blockIdx.x; idw < a.dimdw; idw += gridDim.x) {
+    const T* __restrict__ vrow = a.v + idw * a.dimup;
+    T* __restrict__ hrow = a.hv + idw * a.dimup;
+    const uint32_t mdw = a.map_dw[idw];
+    const T edw = a.e_dw[idw];
+    for (int64_t iup = threadIdx.x; iup < a.dimup; iup += blockDim.x) {
+      T acc;
+      if (FIRST) {
+        const T d = a.e_up[iup] + edw + a.U * T(__popc(a.map_up[iup] & mdw));
+        acc = d * vrow[iup];
+      } else {
+        acc = hrow[iup];
+      }
+      const uint32_t k0 = a.off_up[iup], k1 = a.off_up[iup + 1];
+      for (uint32_t k = k0; k < k1; ++k) acc = fmaT<T>(a.val_up[k], __ldg(vrow + a.src_up[k]), acc);
+      hrow[iup] = acc;
+    }
+  }
+}
+
+// Column-slab pass: a tile is 32 consecutive iup x 8 rows; tiles are visited slab-major so
+// that the slab of V being combined (DimDw rows x 32 columns) stays resident in L2 while
+// every row of it is read ~(hops per row) times. FIRST: hv = diag*v + dw-part.
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(256) k_dw_slab(HxvArgs<T> a, int64_t nrb, int64_t ntiles) {
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t slab = tile / nrb, rb = tile - slab * nrb;
+    const int64_t iup = slab * 32 + threadIdx.x;
+    const int64_t idw = rb * 8 + threadIdx.y;
+    if (iup >= a.dimup || idw >= a.dimdw) continue;
+    const int64_t e = idw * a.dimup + iup;
+    T acc;
+    if (FIRST) {
+      const T d = a.e_up[iup] + a.e_dw[idw] + a.U * T(__popc(a.map_up[iup] & a.map_dw[idw]));
+      acc = d * a.v[e];
+    } else {
+      acc = a.hv[e];
+    }
+    const uint32_t k0 = a.off_dw[idw], k1 = a.off_dw[idw + 1];
+    for (uint32_t k = k0; k < k1; ++k) acc = fmaT<T>(a.val_dw[k], a.v[int64_t(a.src_dw[k]) * a.dimup + iup], acc);
+    a.hv[e] = acc;
+  }
+}
+
+// ---------------------------------------------------------------- direct (on-the-fly) form
+// No tables: each thread derives its hops from the bitstrings, as directMatVec does, with
+// ranks from the combinatorial number system instead of binary_search. Bonds arrive
+// sorted by 2^b - 2^a so that sources come out in ascending rank.
+struct DirectArgsHdr {
+  int nb_up, nb_dw;
+  const int32_t* bonds;   // [nb_up + nb_dw][2]
+  const double* bh;       // [nb_up + nb_dw]
+  const uint32_t* C;      // binomial table
+};
+
+__device__ __forceinline__ uint32_t rank_of_d(uint32_t s, const uint32_t* C) {
+  uint32_t r = 0;
+  int i = 1;
+  while (s) {
+    int p = __ffs(s) - 1;
+    r += C[p * kBinomN + i];
+    ++i;
+    s &= s - 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ int between_parity_d(uint32_t t, int a, int b) {
+  int lo = a < b ? a : b, hi = a < b ? b : a;
+  uint32_t mask = ((1u << hi) - 1u) & ~((2u << lo) - 1u);
+  return __popc(t & mask) & 1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_direct(HxvArgs<T> a, DirectArgsHdr d) {
+  extern __shared__ unsigned char smem_raw[];
+  int32_t* sb = reinterpret_cast<int32_t*>(smem_raw);
+  const int nb = d.nb_up + d.nb_dw;
+  T* sh = reinterpret_cast<T*>(smem_raw + ((2 * nb * sizeof(int32_t) + 15) / 16) * 16);
+  __shared__ uint32_t sC[kBinomN * kBinomN];
+  for (int k = threadIdx.x; k < 2 * nb; k += blockDim.x) sb[k] = d.bonds[k];
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) sh[k] = T(d.bh[k]);
+  for (int k = threadIdx.x; k < kBinomN * kBinomN; k += blockDim.x) sC[k] = d.C[k];
+  __syncthreads();
+  const int64_t n = a.dimup * a.dimdw;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t idw = e / a.dimup, iup = e - idw * a.dimup;
+    const uint32_t mup = a.map_up[iup], mdw = a.map_dw[idw];
+    T acc = (a.e_up[iup] + a.e_dw[idw] + a.U * T(__popc(mup & mdw))) * a.v[e];
+    for (int k = 0; k < d.nb_up; ++k) {
+      const int ba = sb[2 * k], bb = sb[2 * k + 1];
+      if (((mup >> ba) & 1u) && !((mup >> bb) & 1u)) {
+        const uint32_t s = (mup & ~(1u << ba)) | (1u << bb);
+        const T h = between_parity_d(mup, ba, bb) ? -sh[k] : sh[k];
+        acc = fmaT<T>(h, a.v[idw * a.dimup + rank_of_d(s, sC)], acc);
+      }
+    }
+    for (int k = d.nb_up; k < nb; ++k) {
+      const int ba = sb[2 * k], bb = sb[2 * k + 1];
+      if (((mdw >> ba) & 1u) && !((mdw >> bb) & 1u)) {
+        const uint32_t s = (mdw & ~(1u << ba)) | (1u << bb);
+        const T h = between_parity_d(mdw, ba, bb) ? -sh[k] : sh[k];
+        acc = fmaT<T>(h, a.v[int64_t(rank_of_d(s, sC)) * a.dimup + iup], acc);
+      }
+    }
+    a.hv[e] = acc;
+  }
+}
+
+template <typename T>
+const T* pick(const DevBuf<double>& d, const DevBuf<float>& f);
+template <>
+const double* pick<double>(const DevBuf<double>& d, const DevBuf<float>&) { return d.p; }
+template <>
+const float* pick<float>(const DevBuf<double>&, const DevBuf<float>& f) { return f.p; }
+
+int sm_count() {
+  static int cached = 0;
+  if (!cached) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
+    if (cached <= 0) cached = 148;
+  }
+  return cached;
+}
+
+}  // namespace
+
+template <typename T>
+int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
+  HxvArgs<T> a;
+  a.v = v;
+  a.hv = hv;
+  a.dimup = s->up.dim;
+  a.dimdw = s->dw.dim;
+  a.off_up = s->up.off.p;
+  a.src_up = s->up.src.p;
+  a.val_up = pick<T>(s->up.val64, s->up.val32);
+  a.off_dw = s->dw.off.p;
+  a.src_dw = s->dw.src.p;
+  a.val_dw = pick<T>(s->dw.val64, s->dw.val32);
+  a.e_up = pick<T>(s->up.e64, s->up.e32);
+  a.e_dw = pick<T>(s->dw.e64, s->dw.e32);
+  a.map_up = s->up.map.p;
+  a.map_dw = s->dw.map.p;
+  a.U = T(s->U);
+  const int sms = sm_count();
+  cudaStream_t st = s->stream;
+  if (s->form == EDG_FORM_STORED) {
+    const int64_t nslab = (a.dimup + 31) / 32, nrb = (a.dimdw + 7) / 8;
+    const int64_t ntiles = nslab * nrb;
+    const int g1 = int(ntiles < int64_t(sms) * 8 ? ntiles : int64_t(sms) * 8);
+    k_dw_slab<T, true><<<g1, dim3(32, 8), 0, st>>>(a, nrb, ntiles);
+    EDG_CUDA(cudaGetLastError());
+    const int g2 = int(a.dimdw < int64_t(sms) * 8 ? a.dimdw : int64_t(sms) * 8);
+    k_up_rows<T, false><<<g2, 256, 0, st>>>(a);
+    EDG_CUDA(cudaGetLastError());
+  } else {
+    DirectArgsHdr d;
+    d.nb_up = s->bonds[0].nb;
+    d.nb_dw = s->bonds[1].nb;
+    d.bonds = s->bond_dev.p;
+    d.bh = s->bondh_dev.p;
+    d.C = s->binom.p;
+    const int nb = d.nb_up + d.nb_dw;
+    size_t smem = ((2 * nb * sizeof(int32_t) + 15) / 16) * 16 + nb * sizeof(T) + 16;
+    const int64_t n = a.dimup * a.dimdw;
+    const int64_t want = (n + 255) / 256;
+    const int g = int(want < int64_t(sms) * 8 ? want : int64_t(sms) * 8);
+    if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(k_direct<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_direct<T><<<g, 256, smem, st>>>(a, d);
+    EDG_CUDA(cudaGetLastError());
+  }
+  return EDG_OK;
+}
+
+template int hxv_apply<float>(edg_sector_s*, const float*, float*);
+template int hxv_apply<double>(edg_sector_s*, const double*, double*);
+
+}  // namespace edg

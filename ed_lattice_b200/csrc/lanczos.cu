@@ -1,0 +1,294 @@
+// lanczos.cu -- device Lanczos drivers.
+//
+// tridiag_dev : tridiag_Hv_sector (src/DIAG/HAMILTONIAN.f90:242-275) + sp_lanc_tridiag.
+// ground_state: the ground-state solve of ed_diag_d with lanc_method="lanczos"
+//               (src/DIAG/DIAG.f90:206-218, sp_lanc_eigh), in two modes:
+//   EDG_GS_F64        plain FP64 Lanczos; the eigenvector is rebuilt by a second pass of
+//                     the (bit-reproducible) recurrence;
+//   EDG_GS_F32_REFINE FP32 vectors with FP64 scalars until the lowest Ritz value settles at
+//                     FP32 resolution, FP32 Ritz vector accumulated in FP64 from the stored
+//                     FP32 basis, then restarted FP64 Lanczos from it to the requested tol.
+// The sector's work buffers hold v_j, v_{j-1}, w; scalars a_j, b_{j+1} are written by the
+// reduction kernels into device arrays and copied to the host once per step (16 bytes)
+// for the convergence test.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace edg {
+namespace {
+
+struct Scalars {
+  double* partial;  // [kRedBlocks]
+  double* a;        // [cap]
+  double* b;        // [cap+1], b[0] = 0
+  int cap;
+};
+
+int scalars(edg_sector_s* s, int cap, Scalars* sc) {
+  const size_t need = size_t(kRedBlocks) + 2 * size_t(cap) + 8;
+  EDG_CHECK(s->red.alloc(need, "reduction scratch"));
+  sc->partial = s->red.p;
+  sc->a = s->red.p + kRedBlocks;
+  sc->b = sc->a + cap + 1;
+  sc->cap = cap;
+  EDG_CUDA(cudaMemsetAsync(s->red.p, 0, need * sizeof(double), s->stream));
+  return EDG_OK;
+}
+
+template <typename T>
+DevBuf<T>* work(edg_sector_s* s);
+template <>
+DevBuf<double>* work<double>(edg_sector_s* s) { return s->w64; }
+template <>
+DevBuf<float>* work<float>(edg_sector_s* s) { return s->w32; }
+
+// One recurrence step j on (V=v_j, P=v_{j-1}, W): W = H V; a_j; b_{j+1}.
+template <typename T>
+int step(edg_sector_s* s, const Scalars& sc, int j, const T* V, const T* P, T* W) {
+  const int64_t n = s->dim;
+  EDG_CHECK(hxv_apply<T>(s, V, W));
+  EDG_CHECK(lanczos_step_a<T>(s->stream, W, P, V, sc.b + j, n, sc.partial, sc.a + j));
+  EDG_CHECK(lanczos_step_b<T>(s->stream, W, V, sc.a + j, n, sc.partial, sc.b + j + 1));
+  return EDG_OK;
+}
+
+int fetch_ab(edg_sector_s* s, const Scalars& sc, int j, double* a, double* b) {
+  double h[2];
+  EDG_CUDA(cudaMemcpyAsync(&h[0], sc.a + j, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EDG_CUDA(cudaMemcpyAsync(&h[1], sc.b + j + 1, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EDG_CUDA(cudaStreamSynchronize(s->stream));
+  *a = h[0];
+  *b = h[1];
+  return EDG_OK;
+}
+
+// Tridiagonalisation in precision T from the FP64 device start vector dv0.
+template <typename T>
+int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, double* alanc, double* blanc,
+              double* norm2, int* nsteps) {
+  const int64_t n = s->dim;
+  cudaStream_t st = s->stream;
+  Scalars sc;
+  EDG_CHECK(scalars(s, nlanc + 1, &sc));
+  for (int j = 0; j < nlanc; ++j) { alanc[j] = 0.0; blanc[j] = 0.0; }
+  *nsteps = 0;
+  EDG_CHECK(dot_dev<double>(st, dv0, dv0, n, sc.partial, sc.b + nlanc + 1));
+  double n2 = 0.0;
+  EDG_CUDA(cudaMemcpyAsync(&n2, sc.b + nlanc + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  *norm2 = n2;
+  if (n2 == 0.0 || nlanc <= 0) return EDG_OK;
+  DevBuf<T>* wb = work<T>(s);
+  for (int k = 0; k < 3; ++k) EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
+  T* V = wb[0].p;
+  T* P = wb[1].p;
+  T* W = wb[2].p;
+  EDG_CHECK((convert_dev<T, double>(st, V, dv0, n, 1.0 / std::sqrt(n2))));
+  EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), st));
+  EDG_CUDA(cudaMemsetAsync(sc.b, 0, sizeof(double), st));
+  for (int j = 0; j < nlanc; ++j) {
+    EDG_CHECK(step<T>(s, sc, j, V, P, W));
+    double a, b;
+    EDG_CHECK(fetch_ab(s, sc, j, &a, &b));
+    alanc[j] = a;
+    *nsteps = j + 1;
+    if (j + 1 < nlanc) blanc[j + 1] = b;
+    if (!(b >= threshold)) {  // also stops on NaN
+      if (j + 1 < nlanc) blanc[j + 1] = 0.0;
+      break;
+    }
+    if (j + 1 == nlanc) break;
+    EDG_CHECK(scale_into<T>(st, P, W, sc.b + j + 1, n));
+    T* t = P;
+    P = V;
+    V = t;
+  }
+  return EDG_OK;
+}
+
+double lowest_ritz(const std::vector<double>& a, const std::vector<double>& b) {
+  const int m = int(a.size());
+  std::vector<double> w(m);
+  tridiag_eigh_host(m, a.data(), b.data(), w.data(), nullptr, nullptr);
+  return w[0];
+}
+
+// Plain Lanczos in precision T from the normalised FP64 device vector dv0 until the lowest
+// Ritz value settles (|dE| <= tol*|E|), b underflows, or maxit. Optionally stores the basis
+// (FP32 only) so the Ritz vector needs no second pass. Returns a, b (b[0] = 0).
+template <typename T>
+int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vector<double>* A,
+           std::vector<double>* B, float* basis, int basis_cols, double* e0) {
+  const int64_t n = s->dim;
+  cudaStream_t st = s->stream;
+  Scalars sc;
+  EDG_CHECK(scalars(s, maxit + 1, &sc));
+  DevBuf<T>* wb = work<T>(s);
+  for (int k = 0; k < 3; ++k) EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
+  T* V = wb[0].p;
+  T* P = wb[1].p;
+  T* W = wb[2].p;
+  EDG_CHECK((convert_dev<T, double>(st, V, dv0, n, 1.0)));
+  EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), st));
+  A->clear();
+  B->assign(1, 0.0);
+  double eold = 0.0;
+  for (int j = 0; j < maxit; ++j) {
+    if (basis && j < basis_cols) EDG_CHECK((convert_dev<float, T>(st, basis + size_t(j) * n, V, n, 1.0)));
+    EDG_CHECK(step<T>(s, sc, j, V, P, W));
+    double a, b;
+    EDG_CHECK(fetch_ab(s, sc, j, &a, &b));
+    if (!std::isfinite(a) || !std::isfinite(b)) {
+      set_error("Lanczos produced a non-finite coefficient at step %d", j);
+      return EDG_ERR_NOCONV;
+    }
+    A->push_back(a);
+    const double e = lowest_ritz(*A, *B);
+    const bool conv = (j > 0 && std::fabs(e - eold) <= tol * std::fabs(e)) || b < 1e-14;
+    eold = e;
+    B->push_back(b);
+    *e0 = e;
+    if (conv || j + 1 == maxit) break;
+    EDG_CHECK(scale_into<T>(st, P, W, sc.b + j + 1, n));
+    T* t = P;
+    P = V;
+    V = t;
+  }
+  return EDG_OK;
+}
+
+// Ritz vector x = sum_j z_j v_j (FP64, device) for the lowest Ritz value of (A, B):
+// from the stored FP32 basis when present, else by replaying the recurrence from dv0.
+template <typename T>
+int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A, const std::vector<double>& B,
+                const float* basis, int basis_cols, double* x) {
+  const int64_t n = s->dim;
+  cudaStream_t st = s->stream;
+  const int m = int(A.size());
+  std::vector<double> w(m), Z(size_t(m) * m);
+  EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), w.data(), nullptr, Z.data()));
+  EDG_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
+  if (basis && basis_cols >= m) {
+    for (int j = 0; j < m; ++j) EDG_CHECK(axpy_accum_dev<float>(st, x, basis + size_t(j) * n, Z[j], n));
+  } else {
+    Scalars sc;
+    EDG_CHECK(scalars(s, m + 1, &sc));
+    DevBuf<T>* wb = work<T>(s);
+    T* V = wb[0].p;
+    T* P = wb[1].p;
+    T* W = wb[2].p;
+    EDG_CHECK((convert_dev<T, double>(st, V, dv0, n, 1.0)));
+    EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), st));
+    for (int j = 0; j < m; ++j) {
+      EDG_CHECK(axpy_accum_dev<T>(st, x, V, Z[j], n));
+      if (j + 1 == m) break;
+      EDG_CHECK(step<T>(s, sc, j, V, P, W));
+      EDG_CHECK(scale_into<T>(st, P, W, sc.b + j + 1, n));
+      T* t = P;
+      P = V;
+      V = t;
+    }
+  }
+  // normalise
+  Scalars sc2;
+  EDG_CHECK(scalars(s, 2, &sc2));
+  EDG_CHECK(dot_dev<double>(st, x, x, n, sc2.partial, sc2.a));
+  double nn = 0.0;
+  EDG_CUDA(cudaMemcpyAsync(&nn, sc2.a, sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  if (!(nn > 0.0)) {
+    set_error("Ritz vector vanished");
+    return EDG_ERR_NOCONV;
+  }
+  EDG_CHECK((convert_dev<double, double>(st, x, x, n, 1.0 / std::sqrt(nn))));
+  return EDG_OK;
+}
+
+// normalise dv (FP64, device) in place
+int normalise(edg_sector_s* s, double* dv) {
+  Scalars sc;
+  EDG_CHECK(scalars(s, 2, &sc));
+  EDG_CHECK(dot_dev<double>(s->stream, dv, dv, s->dim, sc.partial, sc.a));
+  double nn = 0.0;
+  EDG_CUDA(cudaMemcpyAsync(&nn, sc.a, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EDG_CUDA(cudaStreamSynchronize(s->stream));
+  if (!(nn > 0.0)) {
+    set_error("start vector has zero norm");
+    return EDG_ERR_ARG;
+  }
+  return convert_dev<double, double>(s->stream, dv, dv, s->dim, 1.0 / std::sqrt(nn));
+}
+
+}  // namespace
+
+int tridiag_dev(edg_sector_s* s, const double* dv0, int nlanc, double threshold, int precision, double* alanc,
+                double* blanc, double* norm2, int* nsteps) {
+  if (precision == EDG_PREC_F32) return tridiag_t<float>(s, dv0, nlanc, threshold, alanc, blanc, norm2, nsteps);
+  return tridiag_t<double>(s, dv0, nlanc, threshold, alanc, blanc, norm2, nsteps);
+}
+
+int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
+                 double* e0, int* niter) {
+  const int64_t n = s->dim;
+  cudaStream_t st = s->stream;
+  if (maxit <= 0) maxit = 1;
+  if (maxit > n) maxit = int(n);
+  EDG_CHECK(s->state.alloc(n, "eigenvector"));
+  EDG_CHECK(s->w64[3].alloc(n, "start vector"));
+  double* x0 = s->w64[3].p;
+  if (v0_host) {
+    EDG_CUDA(cudaMemcpyAsync(x0, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  } else {
+    EDG_CHECK(random_dev(st, x0, n, seed));
+  }
+  EDG_CHECK(normalise(s, x0));
+  std::vector<double> A, B;
+  *niter = 0;
+  s->has_state = false;
+  const bool want_vec = !(mode & EDG_GS_E0_ONLY);
+  mode &= 0xff;
+  if (mode == EDG_GS_F64) {
+    EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, e0));
+    *niter += int(A.size());
+    if (want_vec) {
+      EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, s->state.p));
+      *niter += int(A.size()) - 1;
+    }
+  } else {
+    // phase 1: FP32 vectors; keep as many basis vectors as HBM admits (2 vectors of slack)
+    size_t freeb = 0, totb = 0;
+    EDG_CUDA(cudaMemGetInfo(&freeb, &totb));
+    const size_t vecb = size_t(n) * sizeof(float);
+    const size_t slack = (size_t(3) << 30) + 6 * vecb;
+    int cols = 0;
+    if (freeb > slack) cols = int(std::min<size_t>((freeb - slack) / 2 / vecb, size_t(maxit)));
+    if (s->basis32_cols < size_t(cols)) {
+      s->basis32.reset();
+      if (cols > 0 && s->basis32.alloc(size_t(cols) * n, "FP32 Lanczos basis") != EDG_OK) cols = 0;
+      s->basis32_cols = cols > 0 ? cols : 0;
+    } else {
+      cols = int(s->basis32_cols);
+    }
+    const double tol32 = tol > 2e-7 ? tol : 2e-7;
+    double e32 = 0.0;
+    EDG_CHECK(gs_run<float>(s, x0, maxit, tol32, &A, &B, s->basis32.p, cols, &e32));
+    *niter += int(A.size());
+    EDG_CHECK(ritz_vector<float>(s, x0, A, B, s->basis32.p, cols, s->state.p));
+    if (cols < int(A.size())) *niter += int(A.size()) - 1;
+    // phase 2: restarted FP64 Lanczos from the FP32 Ritz vector
+    EDG_CUDA(cudaMemcpyAsync(x0, s->state.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, e0));
+    *niter += int(A.size());
+    if (want_vec) {
+      EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, s->state.p));
+      *niter += int(A.size()) - 1;
+    }
+  }
+  EDG_CUDA(cudaStreamSynchronize(st));
+  s->has_state = want_vec;
+  return EDG_OK;
+}
+
+}  // namespace edg

@@ -1,0 +1,191 @@
+// vecops.cu -- the fused vector passes of the Lanczos recurrence.
+//
+// The recurrence of sp_lanc_tridiag / sp_lanc_eigh (called from src/DIAG/HAMILTONIAN.f90:268
+// and src/DIAG/DIAG.f90:216) split into three HBM passes around H x v:
+//   step A : w <- Hv - b_j v_{j-1};        a_j = <v_j|w>            (reads 3 vectors, writes 1)
+//   step B : w <- w - a_j v_j;             b_{j+1}^2 = <w|w>        (reads 2, writes 1)
+//   scale  : v_{j+1} <- w / b_{j+1}                                   (reads 1, writes 1)
+// Element arithmetic is FP64 (FP32 vectors are widened on load and rounded once on store);
+// dot products accumulate in FP64 over a fixed grid of kRedBlocks blocks followed by a
+// one-block pass in fixed order, so results are bit-reproducible run to run.
+// Scalars (a, b) live in device memory and are read by the next kernel: no host round trip
+// is needed between the passes.
+#include "common.cuh"
+
+namespace edg {
+namespace {
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    r = lane < kRedThreads / 32 ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ x, const T* __restrict__ y, int64_t n,
+                                                     double* __restrict__ partial) {
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    s = __fma_rn(double(x[i]), double(y[i]), s);
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// out = sum(partial) (do_sqrt: sqrt of the sum)
+__global__ void __launch_bounds__(kRedThreads) k_finish(const double* __restrict__ partial, int nblk,
+                                                        double* __restrict__ out, int do_sqrt) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += blockDim.x) s += partial[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[0] = do_sqrt ? sqrt(s) : s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_step_a(T* __restrict__ w, const T* __restrict__ vprev,
+                                                        const T* __restrict__ v, const double* __restrict__ bprev,
+                                                        int64_t n, double* __restrict__ partial) {
+  const double b = *bprev;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const T wt = T(double(w[i]) - b * double(vprev[i]));
+    w[i] = wt;
+    s = __fma_rn(double(v[i]), double(wt), s);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_step_b(T* __restrict__ w, const T* __restrict__ v,
+                                                        const double* __restrict__ a, int64_t n,
+                                                        double* __restrict__ partial) {
+  const double al = *a;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const T wt = T(double(w[i]) - al * double(v[i]));
+    w[i] = wt;
+    s = __fma_rn(double(wt), double(wt), s);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <typename T>
+__global__ void k_scale_into(T* __restrict__ dst, const T* __restrict__ src, const double* __restrict__ b, int64_t n) {
+  const double bb = *b;
+  const double inv = bb != 0.0 ? 1.0 / bb : 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    dst[i] = T(double(src[i]) * inv);
+}
+
+template <typename TD, typename TS>
+__global__ void k_convert(TD* __restrict__ dst, const TS* __restrict__ src, int64_t n, double scale) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    dst[i] = TD(double(src[i]) * scale);
+}
+
+template <typename TS>
+__global__ void k_axpy_accum(double* __restrict__ dst, const TS* __restrict__ x, double coef, int64_t n) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    dst[i] = __fma_rn(coef, double(x[i]), dst[i]);
+}
+
+__device__ __host__ __forceinline__ uint64_t splitmix64_d(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+__global__ void k_random(double* __restrict__ dst, int64_t n, uint64_t seed) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const uint64_t z = splitmix64_d(seed + uint64_t(i));
+    dst[i] = double(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+  }
+}
+
+inline int grid_for(int64_t n) {
+  int64_t g = (n + 255) / 256;
+  return int(g < 148 * 16 ? (g < 1 ? 1 : g) : 148 * 16);
+}
+
+}  // namespace
+
+uint64_t splitmix64(uint64_t x) { return splitmix64_d(x); }
+
+template <typename T>
+int dot_dev(cudaStream_t st, const T* x, const T* y, int64_t n, double* partial, double* out) {
+  k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n, partial);
+  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, out, 0);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int lanczos_step_a(cudaStream_t st, T* w, const T* vprev, const T* v, const double* bprev, int64_t n, double* partial,
+                   double* aout) {
+  k_step_a<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, vprev, v, bprev, n, partial);
+  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, aout, 0);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int lanczos_step_b(cudaStream_t st, T* w, const T* v, const double* a, int64_t n, double* partial, double* bout) {
+  k_step_b<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, v, a, n, partial);
+  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, bout, 1);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int scale_into(cudaStream_t st, T* dst, const T* src, const double* b, int64_t n) {
+  k_scale_into<T><<<grid_for(n), 256, 0, st>>>(dst, src, b, n);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename TD, typename TS>
+int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale) {
+  k_convert<TD, TS><<<grid_for(n), 256, 0, st>>>(dst, src, n, scale);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename TS>
+int axpy_accum_dev(cudaStream_t st, double* dst, const TS* x, double coef, int64_t n) {
+  k_axpy_accum<TS><<<grid_for(n), 256, 0, st>>>(dst, x, coef, n);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed) {
+  k_random<<<grid_for(n), 256, 0, st>>>(dst, n, seed);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+#define EDG_INST(T)                                                                                        \
+  template int dot_dev<T>(cudaStream_t, const T*, const T*, int64_t, double*, double*);                   \
+  template int lanczos_step_a<T>(cudaStream_t, T*, const T*, const T*, const double*, int64_t, double*,   \
+                                 double*);                                                                 \
+  template int lanczos_step_b<T>(cudaStream_t, T*, const T*, const double*, int64_t, double*, double*);   \
+  template int scale_into<T>(cudaStream_t, T*, const T*, const double*, int64_t);                         \
+  template int axpy_accum_dev<T>(cudaStream_t, double*, const T*, double, int64_t);
+EDG_INST(float)
+EDG_INST(double)
+#undef EDG_INST
+template int convert_dev<float, double>(cudaStream_t, float*, const double*, int64_t, double);
+template int convert_dev<double, float>(cudaStream_t, double*, const float*, int64_t, double);
+template int convert_dev<double, double>(cudaStream_t, double*, const double*, int64_t, double);
+template int convert_dev<float, float>(cudaStream_t, float*, const float*, int64_t, double);
+
+}  // namespace edg

@@ -1,0 +1,200 @@
+/*
+ * edgpu.h -- C ABI of the B200 sector-Lanczos engine (libedgpu.so).
+ *
+ * The engine replaces the hot path of EDlattice (aamaricci/ED_Lattice): the sector Fock
+ * basis, the H x v product and the Lanczos tridiagonalisation behind the GF/CHI/OC
+ * builders. Every entry point below names the reference interface it stands in for
+ * (paths relative to the EDlattice project root).
+ *
+ * Conventions
+ *  - Plain C types only; host pointers unless the name says _dev.
+ *  - Every call returns an int status: EDG_OK (0) or a negative EDG_ERR_* code. No call
+ *    aborts the process; edg_last_error() gives a one-line message for the calling thread.
+ *  - Vector layout is the reference's: element i (0-based) = iup + idw*DimUp with iup the
+ *    up-spin basis rank (fastest) and idw the down-spin rank (src/SECTOR.f90:443-480).
+ *  - Sites and spins are 1-based where the reference's arguments are (site io, ispin).
+ *  - Sizes are int64_t: sectors above 2^31 states are supported (the reference's are int32).
+ *  - One sector handle is used by one host thread at a time; separate handles are
+ *    independent (the reference keeps one active sector in module globals,
+ *    src/DIAG/HAMILTONIAN_COMMON.f90:13-40).
+ */
+#ifndef EDGPU_H
+#define EDGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  EDG_OK = 0,
+  EDG_ERR_ARG = -1,          /* invalid argument (replaces the reference's `stop` on bad input) */
+  EDG_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  EDG_ERR_NOMEM = -3,        /* HBM admission refused or allocation failed */
+  EDG_ERR_UNSUPPORTED = -4,  /* model feature outside the engine (e.g. complex Hij on device) */
+  EDG_ERR_STATE = -5,        /* handle in the wrong state */
+  EDG_ERR_NOCONV = -6,       /* eigen-solver did not converge */
+  EDG_ERR_NODEVICE = -8      /* no CUDA device visible */
+};
+
+/* H x v forms: the reference's ed_sparse_H switch (src/INPUT_VARS.f90:151,
+ * src/DIAG/HAMILTONIAN.f90:148-160). STORED = spMatVec over tables built once per sector;
+ * DIRECT = directMatVec, matrix elements generated on the fly. */
+enum { EDG_FORM_STORED = 0, EDG_FORM_DIRECT = 1 };
+
+/* Precision of the device Lanczos vectors. Scalars (alpha, beta, dots) are always FP64. */
+enum { EDG_PREC_F64 = 0, EDG_PREC_F32 = 1 };
+
+/* Ground-state modes: plain FP64 Lanczos, or FP32 Lanczos + restarted FP64 refinement.
+ * OR with EDG_GS_E0_ONLY to skip building the final eigenvector (time-to-E0 runs). */
+enum { EDG_GS_F64 = 0, EDG_GS_F32_REFINE = 1, EDG_GS_E0_ONLY = 0x100 };
+
+typedef struct edg_model_s edg_model;
+typedef struct edg_sector_s edg_sector;
+
+const char* edg_last_error(void);
+int edg_device_count(int* n);
+
+/* ------------------------------------------------------------------ model
+ * Replaces Hij_init/Hij_add_link/Hij_build/Hij_get (src/GRAPH_MATRIX.f90:79-344) plus the
+ * hot-path input keys ULOC, XMU, HFMODE, ED_FILLING (src/INPUT_VARS.f90:106-166).
+ * hij_re/hij_im: Hij(1,io,jo) row-major [io*ns+jo], Norb=1; hijdw_*: Hij(2,:,:) when
+ * nspin==2 (NULL otherwise). hij_im/hijdw_im may be NULL (real Hij). The Hermiticity check
+ * of Hij_build (tolerance 1e-6, src/GRAPH_MATRIX.f90:325) returns EDG_ERR_ARG. */
+int edg_model_create(int ns, int nspin, const double* hij_re, const double* hij_im,
+                     const double* hijdw_re, const double* hijdw_im, double uloc, double xmu,
+                     int hfmode, int ed_filling, edg_model** out);
+int edg_model_destroy(edg_model* m);
+
+/* ------------------------------------------------------------------ sector numbering
+ * get_Sector / get_Nup / get_Ndw (src/SECTOR.f90:370-424) and binomial
+ * (src/SETUP.f90:336-358). */
+int edg_get_sector(int ns, int nup, int ndw);
+int edg_get_nup(int ns, int isector);
+int edg_get_ndw(int ns, int isector);
+int64_t edg_binomial(int n, int k);
+
+/* ------------------------------------------------------------------ sector lifecycle
+ * build_Hv_sector(isector) / delete_Hv_sector() / vecDim_Hv_sector(isector)
+ * (src/DIAG/HAMILTONIAN.f90:53-239) with build_sector (src/SECTOR.f90:69-115) done on the
+ * device: Gosper enumeration of the Nup/Ndw bitstrings, combinatorial-rank index maps and,
+ * for EDG_FORM_STORED, the per-spin hop tables of ed_buildh
+ * (src/DIAG/HAMILTONIAN_STORED_HxV.f90:21-126). */
+int edg_sector_create(const edg_model* m, int nup, int ndw, int form, edg_sector** out);
+int edg_sector_destroy(edg_sector* s);
+int edg_sector_dims(const edg_sector* s, int64_t* dim, int64_t* dimup, int64_t* dimdw);
+/* Copy the device-built maps Hsector%H(1)%map / H(2)%map (bitstrings, ascending). */
+int edg_sector_get_maps(const edg_sector* s, int32_t* map_up, int32_t* map_dw);
+/* Copy one spin's hop table (spin 1 = spH0ups(1), 2 = spH0dws(1)) as CSR over target rows:
+ * rowptr[dim+1], cols[nnz] (source ranks, ascending per row), vals[nnz] (real part). Pass
+ * NULL arrays to get *nnz only. */
+int edg_sector_get_hops(const edg_sector* s, int spin, int64_t* rowptr, int32_t* cols,
+                        double* vals, int64_t* nnz);
+/* Run this sector's work on a caller-owned stream (cudaStream_t passed as void*). */
+int edg_sector_set_stream(edg_sector* s, void* stream);
+
+/* ------------------------------------------------------------------ H x v
+ * dd_sparse_HxV(Nloc,v,Hv) (src/VARS_GLOBAL.f90:102-108), the callback that
+ * spHtimesV_p points to (spMatVec / directMatVec). Host complex(8) vectors, interleaved
+ * (re,im); Hv is overwritten. Real Hij only on the device: H acts on the real and the
+ * imaginary parts separately. nloc must equal the sector dimension (the reference stops
+ * with "Nloc != dim(isector)", src/DIAG/HAMILTONIAN_DIRECT_HxV.f90:33). */
+int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv);
+/* Same on real host vectors. */
+int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv);
+/* Device-resident forms (vectors in HBM, reference layout); stream-ordered, no sync. */
+int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv);
+int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv);
+
+/* ------------------------------------------------------------------ Lanczos
+ * tridiag_Hv_sector(isector,vvinit,alanc,blanc,norm2) (src/DIAG/HAMILTONIAN.f90:242-275)
+ * with the recurrence of sp_lanc_tridiag: norm2=<v|v>, v/=sqrt(norm2), then nlanc steps;
+ * alanc[j]=a_{j+1}, blanc[0]=0, blanc[j]=b_{j+1} (the reference's blanc(1) unused
+ * convention, src/GF/GF_ELECTRONS.f90:445-447). Stops early when b < threshold; the rest
+ * stays zero; *nsteps = steps taken. vvinit is a host real vector of the sector dimension.
+ * precision: EDG_PREC_F64 or EDG_PREC_F32 (FP32 vectors, FP64 scalars). */
+int edg_tridiag_d(edg_sector* s, const double* vvinit, int nlanc, double threshold, int precision,
+                  double* alanc, double* blanc, double* norm2, int* nsteps);
+/* Same from a device vector (not modified). */
+int edg_tridiag_dev_f64(edg_sector* s, const double* dvinit, int nlanc, double threshold,
+                        int precision, double* alanc, double* blanc, double* norm2, int* nsteps);
+
+/* Ground state: the contract of sp_lanc_eigh(Hv_p,E,v,Nitermax,threshold) as called from
+ * ed_diag_d (src/DIAG/DIAG.f90:212-217). v0: host start vector or NULL for the seeded
+ * uniform[-1,1) start vector of edg_random_vector. Stops when the lowest Ritz value changes
+ * by <= tol*|E0| between steps (or b underflows, or maxit). mode: EDG_GS_F64 or
+ * EDG_GS_F32_REFINE. evec (host, may be NULL) receives the normalised eigenvector.
+ * *niter = total H x v applications. */
+int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, double tol, int mode,
+                     double* e0, double* evec, int* niter);
+/* Device variant: the eigenvector stays on the device in the sector's state buffer; copy
+ * with edg_state_get or use in the excitation builders below. */
+int edg_ground_state_keep(edg_sector* s, const double* v0, uint64_t seed, int maxit, double tol,
+                          int mode, double* e0, int* niter);
+int edg_state_get(const edg_sector* s, double* evec);
+int edg_state_set(edg_sector* s, const double* evec);
+
+/* Seeded start vector used by the engine and the tests: splitmix64 counter stream,
+ * x_i = ((splitmix64(seed + i) >> 11) * 2^-53) * 2 - 1. */
+int edg_random_vector(uint64_t seed, int64_t n, double* out);
+
+/* ------------------------------------------------------------------ excitations
+ * apply_op_CDG / apply_op_C over a whole vector, as in lanc_build_gf_electrons_diag
+ * (src/GF/GF_ELECTRONS.f90:241-245,267-271; src/SECTOR.f90:217-268): out = coef*op|in>
+ * (overwrite) or out += coef*op|in> (accumulate=1, the (c_i + c_j) vectors of _mix,
+ * :343-353). op=+1 creates, -1 annihilates; site, spin 1-based. from/to must be the
+ * sectors (Nup,Ndw) and (Nup+op,Ndw) or (Nup,Ndw+op). Device FP64 vectors. */
+int edg_apply_cop_dev_f64(const edg_sector* from, const edg_sector* to, int op, int site, int spin,
+                          double coef, int accumulate, const double* din, double* dout);
+/* S^z_i / n_i (apply_op_Sz / apply_op_N, src/SECTOR.f90:271-341): kind 0 = Sz, 1 = N;
+ * site2 > 0 adds the second site (lanc_build_spinChi_mix, src/CHI/CHI_SPIN_ELECTRONS.f90:275-279).
+ * Momentum form: when qcos != NULL, out = sum_i qcos[i]*O_i|in> (real combination). */
+int edg_apply_diagop_dev_f64(const edg_sector* s, int kind, int site, int site2, const double* qcos,
+                             const double* din, double* dout);
+/* J|psi> (lanc_ed_build_oc, src/OC/OC_ELECTRONS.f90:139-205): returns the real vector r with
+ * J|psi> = i*r (real Hij). */
+int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* dout);
+
+/* Static observables of one state (lanc_observables, src/OBSERVABLES.f90:127-152): per-site
+ * dens, dens_up, dens_dw, docc, magz of the device state buffer, each scaled by weight. */
+int edg_observables(const edg_sector* s, double weight, double* dens, double* dens_up,
+                    double* dens_dw, double* docc, double* magz);
+
+/* ------------------------------------------------------------------ response functions
+ * One Lanczos chain per excitation, as built by the GF/CHI/OC builders:
+ *  edg_gf_chain: c^+ (op=+1) or c (op=-1) on the state buffer of `from`, tridiagonalised in
+ *  `to`; poles = isign*(theta_j - ei), weights = norm2*Z(1,j)^2 (add_to_lanczos_gf_normal,
+ *  src/GF/GF_ELECTRONS.f90:417-457). site2 > 0 forms (c_site + c_site2).
+ *  poles/weights have room for nlanc entries; *nout = entries written. */
+int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int site2, int spin,
+                 int nlanc, int precision, double ei, double* poles, double* weights, double* norm2,
+                 int* nout);
+/* Spin/charge susceptibility chain (add_to_lanczos_spinChi,
+ * src/CHI/CHI_SPIN_ELECTRONS.f90:305-366): vector O|psi> with O from edg_apply_diagop_dev_f64,
+ * poles theta_j - ei, weights norm2*Z(1,j)^2. */
+int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qcos, int nlanc,
+                  int precision, double ei, double* poles, double* weights, double* norm2, int* nout);
+/* Optical-conductivity chain (add_to_lanczos_oc, src/OC/OC_ELECTRONS.f90:223-263). */
+int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* poles,
+                 double* weights, double* norm2, int* nout);
+
+/* Batched chains: k start vectors in one sector run as block H x V in a single recurrence
+ * (one alpha/beta pair per column). dvinit: k device vectors, column c at dvinit + c*dim.
+ * alanc/blanc/norm2: [k][nlanc] row-major per column; nsteps[k]. */
+int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc, double threshold,
+                          int precision, double* alanc, double* blanc, double* norm2, int* nsteps);
+
+/* Tridiagonal eigenproblem (SF_LINALG eigh(diag,subdiag,Ev) as used at
+ * src/GF/GF_ELECTRONS.f90:447): FP64 implicit QL, eigenvalues ascending; z1 receives the
+ * first component of each eigenvector (may be NULL). d[n], e[n] with e[0] ignored. */
+int edg_tridiag_eigh(int n, const double* d, const double* e, double* w, double* z1);
+/* poles/weights from (a,b,norm2): the loop of add_to_lanczos_gf_normal (:451-456). */
+int edg_poles_weights(int n, const double* alanc, const double* blanc, double norm2, double ei,
+                      int isign, double* poles, double* weights);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EDGPU_H */

@@ -1,0 +1,90 @@
+"""Generate the committed golden fixtures under tests/golden/ from the CPU oracle.
+
+The reference (Fortran + SciFortran) cannot be built or run on this machine and ships no
+fixtures, so these vectors come from oracle/edlat_oracle.cpp, whose own correctness is
+pinned by known answers in tests/test_oracle_known_answers.py. They freeze the oracle's
+outputs (regression) and give the GPU tests fixed expected values that do not depend on
+rebuilding the oracle on the GPU host.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+
+
+def ring(L, t=1.0):
+    H = np.zeros((L, L))
+    for i in range(L):
+        j = (i + 1) % L
+        H[i, j] = H[j, i] = -t
+    return H
+
+
+def square(lx, ly, t=1.0):
+    ns = lx * ly
+    H = np.zeros((ns, ns))
+    for y in range(ly):
+        for x in range(lx):
+            i = x + lx * y
+            for dx, dy in ((1, 0), (0, 1)):
+                j = (x + dx) % lx + lx * ((y + dy) % ly)
+                if i != j:
+                    H[i, j] = H[j, i] = -t
+    return H
+
+
+def config1():
+    """L=8 periodic ring, t=1, U=4, mu=U/2 (HFMODE=F, XMU=2), sector (4,4), FP64,
+    seeded uniform[-1,1) start vector (seed 2024), 100 tridiagonal steps."""
+    m = O.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
+    st = O.Stored(m, 4, 4)
+    v0 = O.random_vector(2024, st.dim)
+    a, b, n2, n = st.tridiag(v0, 100)
+    e0, vec, ga, gb = st.ground_state(v0, maxit=300, tol=1e-15)
+    obs = O.observables(8, 4, 4, vec)
+    hv = st.matvec_d(v0)
+    hvd = O.direct_matvec_d(m, 4, 4, v0)
+    np.savez_compressed(os.path.join(HERE, "config1_ring8.npz"), v0=v0, hv_stored=hv, hv_direct=hvd, alanc=a,
+                        blanc=b, norm2=n2, e0=e0, dens=obs["dens"], docc=obs["docc"],
+                        map_up=O.build_map(8, 4))
+
+
+def disorder3x4():
+    """3x4 periodic square, t=1, U=4, Anderson eps_i ~ uniform[-1,1) quantised to 2^-16
+    (seed 7), XMU=2 HFMODE=F; sector (3,2): maps, hop tables, H x v, E0 and a GF chain."""
+    rng = np.random.default_rng(7)
+    eps = np.round(rng.uniform(-1, 1, 12) * 65536) / 65536
+    H = square(3, 4)
+    H[np.diag_indices(12)] = eps
+    m = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    st = O.Stored(m, 3, 2)
+    v0 = O.random_vector(99, st.dim)
+    hv = st.matvec_d(v0)
+    rp_up, c_up, v_up = O.hop_csr(m, 1, 3)
+    rp_dw, c_dw, v_dw = O.hop_csr(m, 2, 2)
+    e0, vec, _, _ = st.ground_state(v0, maxit=400, tol=1e-15)
+    # c^+_{5,up}|GS> into (4,2), 60 steps
+    x = O.apply_cop(12, 3, 2, +1, 5, 1, vec)
+    stJ = O.Stored(m, 4, 2)
+    a, b, n2, n = stJ.tridiag(x, 60)
+    p, w = O.poles_weights(a[:n], b[:n], n2, e0, +1)
+    np.savez_compressed(os.path.join(HERE, "disorder3x4.npz"), eps=eps, v0=v0, hv=hv, rp_up=rp_up, c_up=c_up,
+                        v_up=v_up, rp_dw=rp_dw, c_dw=c_dw, v_dw=v_dw, e0=e0, gf_poles=p, gf_weights=w, gf_norm2=n2)
+
+
+if __name__ == "__main__":
+    config1()
+    disorder3x4()
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

@@ -1,0 +1,364 @@
+"""GPU parity tests: the CUDA path through the C ABI against the CPU oracle and the
+committed golden fixtures. Integer work (basis maps, hop tables) is compared bit-exactly;
+FP64 results within the tolerances stated in each test; FP32 within FP32 round-off."""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+import pytest
+
+import ed_lattice_b200 as E
+from ed_lattice_b200 import _edgpu_lib as L
+from ed_lattice_b200.edlat import ring, square_lattice
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def disorder(ns, seed):
+    rng = np.random.default_rng(seed)
+    return np.round(rng.uniform(-1, 1, ns) * 65536) / 65536
+
+
+def models(h, **kw):
+    return E.Model(h, **kw), O.Model(h, **kw)
+
+
+# ----------------------------------------------------------------------------- basis / tables
+@pytest.mark.parametrize("ns", [1, 2, 5, 8, 12])
+def test_maps_bit_exact_all_sectors(ns):
+    gm = E.Model(ring(ns) if ns > 2 else np.zeros((ns, ns)))
+    for nup in range(ns + 1):
+        ndw = ns - nup
+        s = E.Sector(gm, nup, ndw)
+        mu, md = s.maps()
+        assert np.array_equal(mu, O.build_map(ns, nup))
+        assert np.array_equal(md, O.build_map(ns, ndw))
+        assert s.dim == math.comb(ns, nup) * math.comb(ns, ndw)
+
+
+@pytest.mark.parametrize("ns,n", [(16, 8), (18, 9), (20, 7), (24, 12)])
+def test_maps_bit_exact_large(ns, n):
+    gm = E.Model(np.zeros((ns, ns)))
+    s = E.Sector(gm, n, 1, E.EDG_FORM_DIRECT)
+    mu, _ = s.maps()
+    if ns <= 20:
+        assert np.array_equal(mu, O.build_map(ns, n))
+    assert mu.size == math.comb(ns, n)
+    assert np.all(np.diff(mu.astype(np.int64)) > 0)
+    pc = np.array([bin(int(x)).count("1") for x in mu[:: max(1, mu.size // 5000)]])
+    assert np.all(pc == n)
+
+
+@pytest.mark.parametrize("lat", ["ring8", "sq4x4", "sq3x4dis", "complete6"])
+def test_hop_tables_bit_exact(lat):
+    if lat == "ring8":
+        h, secs = ring(8), [(4, 4), (3, 5), (0, 8), (8, 1)]
+    elif lat == "sq4x4":
+        h, secs = square_lattice(4, 4), [(8, 8), (7, 8)]
+    elif lat == "sq3x4dis":
+        h = square_lattice(3, 4)
+        h[np.diag_indices(12)] = disorder(12, 7)
+        secs = [(6, 6), (3, 2)]
+    else:
+        rng = np.random.default_rng(2)
+        A = rng.normal(size=(6, 6))
+        h = A + A.T
+        secs = [(3, 3), (2, 4)]
+    gm, om = models(h, uloc=4.0, xmu=2.0, hfmode=False)
+    for nup, ndw in secs:
+        s = E.Sector(gm, nup, ndw)
+        for spin, n in ((1, nup), (2, ndw)):
+            rp, c, v = s.hops(spin)
+            rpo, co, vo = O.hop_csr(om, spin, n)
+            assert np.array_equal(rp, rpo)
+            assert np.array_equal(c, co)
+            assert np.array_equal(v, vo)
+
+
+def test_hop_tables_golden():
+    g = np.load(os.path.join(GOLDEN, "disorder3x4.npz"))
+    h = square_lattice(3, 4)
+    h[np.diag_indices(12)] = g["eps"]
+    s = E.Sector(E.Model(h, uloc=4.0, xmu=2.0, hfmode=False), 3, 2)
+    rp, c, v = s.hops(1)
+    assert np.array_equal(rp, g["rp_up"]) and np.array_equal(c, g["c_up"]) and np.array_equal(v, g["v_up"])
+    rp, c, v = s.hops(2)
+    assert np.array_equal(rp, g["rp_dw"]) and np.array_equal(c, g["c_dw"]) and np.array_equal(v, g["v_dw"])
+
+
+# ----------------------------------------------------------------------------- H x v
+def test_hxv_golden_config1_bit_exact():
+    g = np.load(os.path.join(GOLDEN, "config1_ring8.npz"))
+    gm = E.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 4, 4, E.EDG_FORM_STORED)
+    assert np.array_equal(s.maps()[0], g["map_up"])
+    hv = s.hxv_real(g["v0"])
+    # t=1, U=4, mu=2: every matrix element and diagonal is an exact small integer, and the
+    # engine sums in the reference's order, so the stored form reproduces spMatVec exactly
+    assert np.array_equal(hv, g["hv_stored"])
+    sd = E.Sector(gm, 4, 4, E.EDG_FORM_DIRECT)
+    assert np.array_equal(sd.hxv_real(g["v0"]), g["hv_direct"])
+
+
+@pytest.mark.parametrize("form", [E.EDG_FORM_STORED, E.EDG_FORM_DIRECT])
+@pytest.mark.parametrize("case", ["ring8_44", "sq3x4dis_53", "sq4x4_66", "rand6_33", "ring10_55_fill"])
+def test_hxv_f64_vs_oracle(form, case):
+    kw = dict(uloc=4.0, xmu=2.0, hfmode=False)
+    if case == "ring8_44":
+        h, nup, ndw = ring(8), 4, 4
+    elif case == "sq3x4dis_53":
+        h = square_lattice(3, 4)
+        h[np.diag_indices(12)] = disorder(12, 3)
+        nup, ndw = 5, 3
+    elif case == "sq4x4_66":
+        h, nup, ndw = square_lattice(4, 4), 6, 6
+    elif case == "rand6_33":
+        rng = np.random.default_rng(9)
+        A = rng.normal(size=(6, 6))
+        h, nup, ndw = (A + A.T) / 2, 3, 3
+        kw = dict(uloc=2.7, xmu=0.3, hfmode=True)
+    else:
+        h, nup, ndw = ring(10), 5, 5
+        kw = dict(uloc=3.0, xmu=1.0, hfmode=True, ed_filling=10)
+    gm, om = models(h, **kw)
+    s = E.Sector(gm, nup, ndw, form)
+    v = O.random_vector(17, s.dim)
+    hv = s.hxv_real(v)
+    ref = O.Stored(om, nup, ndw).matvec_d(v) if form == E.EDG_FORM_STORED else O.direct_matvec_d(om, nup, ndw, v)
+    scale = np.abs(ref).max()
+    assert np.abs(hv - ref).max() <= 1e-13 * scale
+
+
+def test_hxv_f32_and_device_entry():
+    import torch  # device buffers for the _dev entry points
+    gm, om = models(square_lattice(3, 4), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 6, 6)
+    v = O.random_vector(5, s.dim)
+    ref = O.Stored(om, 6, 6).matvec_d(v)
+    dv = torch.tensor(v, dtype=torch.float32, device="cuda")
+    dh = torch.empty_like(dv)
+    L.check(L.lib().edg_hxv_dev_f32(s.handle, C.c_void_p(dv.data_ptr()), C.c_void_p(dh.data_ptr())), "f32")
+    torch.cuda.synchronize()
+    h32 = dh.double().cpu().numpy()
+    assert np.abs(h32 - ref).max() <= 2e-6 * np.abs(ref).max()
+    dv64 = torch.tensor(v, dtype=torch.float64, device="cuda")
+    dh64 = torch.empty_like(dv64)
+    L.check(L.lib().edg_hxv_dev_f64(s.handle, C.c_void_p(dv64.data_ptr()), C.c_void_p(dh64.data_ptr())), "f64")
+    torch.cuda.synchronize()
+    assert np.array_equal(dh64.cpu().numpy(), ref)
+
+
+def test_hxv_complex_dropin():
+    gm, om = models(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 4, 3)
+    rng = np.random.default_rng(3)
+    v = rng.normal(size=s.dim) + 1j * rng.normal(size=s.dim)
+    hv = s.HxV(v)
+    ref = O.Stored(om, 4, 3).matvec_z(v)
+    assert np.abs(hv - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_hxv_nspin2():
+    h1 = ring(6)
+    h2 = 0.5 * ring(6) + np.diag(disorder(6, 1))
+    H = np.stack([h1, h2])
+    gm, om = models(H, uloc=2.0, xmu=0.5, hfmode=True)
+    s = E.Sector(gm, 3, 2)
+    v = O.random_vector(2, s.dim)
+    ref = O.Stored(om, 3, 2).matvec_d(v)
+    assert np.abs(s.hxv_real(v) - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("nup,ndw", [(0, 0), (0, 8), (8, 8), (1, 0), (8, 0)])
+def test_hxv_edge_sectors(nup, ndw):
+    gm, om = models(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
+    for form in (E.EDG_FORM_STORED, E.EDG_FORM_DIRECT):
+        s = E.Sector(gm, nup, ndw, form)
+        v = O.random_vector(1, s.dim)
+        ref = O.Stored(om, nup, ndw).matvec_d(v)
+        assert np.abs(s.hxv_real(v) - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())
+
+
+def test_hxv_errors():
+    gm = E.Model(ring(6), uloc=1.0)
+    s = E.Sector(gm, 3, 3)
+    with pytest.raises(E.EdgError) as ei:
+        s.hxv_real(np.zeros(s.dim + 1))
+    assert ei.value.status == L.EDG_ERR_ARG
+    with pytest.raises(E.EdgError):
+        E.Sector(gm, 7, 1)
+    hc = np.array([[0.0, -1.0 + 0.5j], [-1.0 - 0.5j, 0.0]])
+    with pytest.raises(E.EdgError) as ei:
+        E.Sector(E.Model(hc), 1, 1)
+    assert ei.value.status == L.EDG_ERR_UNSUPPORTED
+
+
+# ----------------------------------------------------------------------------- Lanczos
+def test_config1_lanczos_and_ground_state():
+    """Config 1: L=8 ring, U=4, mu=U/2, (4,4): a(1:100), b(2:100), E0, density, docc."""
+    g = np.load(os.path.join(GOLDEN, "config1_ring8.npz"))
+    gm = E.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 4, 4)
+    a, b, n2, n = E.tridiag_Hv_sector(s, g["v0"], 100)
+    assert n == 100 and b[0] == 0.0
+    assert abs(n2 - g["norm2"]) <= 1e-13 * n2
+    # plain Lanczos loses orthogonality; the first 40 steps agree to 1e-9 (FP64 contract)
+    assert np.abs(a[:40] - g["alanc"][:40]).max() < 1e-9
+    assert np.abs(b[:40] - g["blanc"][:40]).max() < 1e-9
+    # all 100: the spectra of T agree at the low end
+    wa = np.linalg.eigvalsh(np.diag(a) + np.diag(b[1:], 1) + np.diag(b[1:], -1))
+    wo = np.linalg.eigvalsh(np.diag(g["alanc"]) + np.diag(g["blanc"][1:], 1) + np.diag(g["blanc"][1:], -1))
+    assert abs(wa[0] - wo[0]) < 1e-10 * abs(wo[0])
+    e0, vec, it = E.sp_lanc_eigh(s, v0=g["v0"], tol=1e-14)
+    assert abs(e0 - float(g["e0"])) <= 1e-10 * abs(float(g["e0"]))
+    obs = s.observables()
+    assert np.allclose(obs["dens"], g["dens"], atol=1e-8)
+    assert np.allclose(obs["docc"], g["docc"], atol=1e-8)
+
+
+def test_tridiag_f32_close_to_f64():
+    gm, om = models(square_lattice(3, 4), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 6, 6)
+    v0 = O.random_vector(3, s.dim)
+    a64, b64, _, _ = E.tridiag_Hv_sector(s, v0, 30)
+    a32, b32, _, _ = E.tridiag_Hv_sector(s, v0, 30, precision=E.EDG_PREC_F32)
+    assert np.abs(a32[:15] - a64[:15]).max() < 1e-4
+    assert np.abs(b32[:15] - b64[:15]).max() < 1e-4
+
+
+def test_tridiag_early_stop_and_zero_vector():
+    gm = E.Model(ring(4), uloc=2.0, xmu=1.0, hfmode=False)
+    s = E.Sector(gm, 2, 1)  # dim 6*4 = 24: Krylov space exhausts before 40 steps
+    v = O.random_vector(1, s.dim)
+    a, b, n2, n = E.tridiag_Hv_sector(s, v, 40)
+    assert n <= s.dim and np.all(a[n:] == 0) and np.all(b[n:] == 0)
+    a, b, n2, n = E.tridiag_Hv_sector(s, np.zeros(s.dim), 10)
+    assert n2 == 0.0 and n == 0 and np.all(a == 0)
+
+
+@pytest.mark.parametrize("mode", [E.EDG_GS_F64, E.EDG_GS_F32_REFINE])
+def test_ground_state_vs_dense(mode):
+    h = square_lattice(3, 4)
+    h[np.diag_indices(12)] = disorder(12, 11)
+    gm, om = models(h, uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 3, 2)  # dim 220*66 = 14520: dense FP64 check is feasible
+    Hd = O.dense_h(om, 3, 2)
+    w = np.linalg.eigvalsh(Hd)
+    e0, vec, it = E.sp_lanc_eigh(s, seed=42, tol=1e-12, mode=mode)
+    tol = 1e-10 if mode == E.EDG_GS_F64 else 1e-8
+    assert abs(e0 - w[0]) <= tol * abs(w[0])
+    assert abs(np.linalg.norm(vec) - 1) < 1e-12
+    assert np.linalg.norm(Hd @ vec - e0 * vec) < 1e-4
+
+
+# ----------------------------------------------------------------------------- excitations / response
+def _gs_pair(h, nup, ndw, **kw):
+    gm, om = models(h, **kw)
+    s = E.Sector(gm, nup, ndw)
+    st = O.Stored(om, nup, ndw)
+    e0o, vo, _, _ = st.ground_state(O.random_vector(4, st.dim), maxit=400, tol=1e-15)
+    s.set_state(vo)  # same state on both sides: response parity isolates the chain
+    return gm, om, s, e0o, vo
+
+
+@pytest.mark.parametrize("op,spin", [(+1, 1), (-1, 1), (+1, 2), (-1, 2)])
+def test_cop_vectors_bit_exact(op, spin):
+    gm, om, s, e0, psi = _gs_pair(ring(8), 4, 3, uloc=4.0, xmu=2.0, hfmode=False)
+    import torch
+    nupJ, ndwJ = 4 + (op if spin == 1 else 0), 3 + (op if spin == 2 else 0)
+    sJ = E.Sector(gm, nupJ, ndwJ)
+    din = torch.tensor(psi, dtype=torch.float64, device="cuda")
+    dout = torch.empty(sJ.dim, dtype=torch.float64, device="cuda")
+    for site in (1, 5, 8):
+        L.check(L.lib().edg_apply_cop_dev_f64(s.handle, sJ.handle, op, site, spin, 1.0, 0, C.c_void_p(din.data_ptr()),
+                                              C.c_void_p(dout.data_ptr())), "cop")
+        torch.cuda.synchronize()
+        ref = O.apply_cop(8, 4, 3, op, site, spin, psi)
+        assert np.array_equal(dout.cpu().numpy(), ref)
+
+
+def test_gf_chain_vs_oracle_and_golden():
+    g = np.load(os.path.join(GOLDEN, "disorder3x4.npz"))
+    h = square_lattice(3, 4)
+    h[np.diag_indices(12)] = g["eps"]
+    gm, om = models(h, uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 3, 2)
+    e0, vec, _ = E.sp_lanc_eigh(s, v0=g["v0"], tol=1e-14, maxit=400)
+    assert abs(e0 - float(g["e0"])) < 1e-10 * abs(e0)
+    sJ = E.Sector(gm, 4, 2)
+    sp = E.gf_chain(s, sJ, +1, 5, 1, 60, e0)
+    assert abs(sp.norm2 - float(g["gf_norm2"])) < 1e-9
+    big = g["gf_weights"] > 1e-6
+    # converged poles carry the weight; compare weight-resolved low-energy poles
+    for p_ref, w_ref in zip(g["gf_poles"][big], g["gf_weights"][big]):
+        j = np.argmin(np.abs(sp.poles - p_ref))
+        assert abs(sp.poles[j] - p_ref) < 1e-6 and abs(sp.weight[j] - w_ref) < 1e-6
+    assert abs(sp.weight.sum() - sp.norm2) < 1e-12
+
+
+def test_gf_lanczos_vs_full_lehmann_gpu():
+    gm, om, s, e0, psi = _gs_pair(ring(6), 3, 3, uloc=3.0, xmu=1.5, hfmode=False)
+    wm = np.pi * 0.05 * (2 * np.arange(1, 33) - 1)
+    g_gpu = np.zeros(wm.size, complex)
+    g_full = np.zeros(wm.size, complex)
+    for op, (nu, nd) in ((+1, (4, 3)), (-1, (2, 3))):
+        sJ = E.Sector(gm, nu, nd)
+        sp = E.gf_chain(s, sJ, op, 2, 1, min(sJ.dim, 200), e0)
+        gm_, _ = E.eval_gf([sp], wm, np.zeros(1), 0.01)
+        g_gpu += gm_
+        x = O.apply_cop(6, 3, 3, op, 2, 1, psi)
+        wj, Vj = np.linalg.eigh(O.dense_h(om, nu, nd))
+        amp = (Vj.T @ x) ** 2
+        g_full += (amp[None, :] / (1j * wm[:, None] - op * (wj[None, :] - e0))).sum(1)
+    assert np.abs(g_gpu - g_full).max() < 1e-9
+
+
+@pytest.mark.parametrize("kind,site,site2", [(0, 3, 0), (1, 1, 0), (0, 2, 5)])
+def test_chi_chain_vs_oracle(kind, site, site2):
+    gm, om, s, e0, psi = _gs_pair(ring(8), 4, 4, uloc=4.0, xmu=2.0, hfmode=False)
+    sp = E.chi_chain(s, site, 80, e0, kind=kind, site2=site2)
+    x = O.apply_diagop(8, 4, 4, kind, site, psi, site2)
+    a, b, n2, n = O.Stored(om, 4, 4).tridiag(x, 80)
+    p, w = O.poles_weights(a[:n], b[:n], n2, e0, +1)
+    assert abs(sp.norm2 - n2) < 1e-12 * max(1.0, n2)
+    big = w > 1e-6
+    for pr, wr in zip(p[big], w[big]):
+        j = np.argmin(np.abs(sp.poles - pr))
+        assert abs(sp.poles[j] - pr) < 1e-6 and abs(sp.weight[j] - wr) < 1e-6
+
+
+def test_momentum_chi_vector():
+    import torch
+    gm, om, s, e0, psi = _gs_pair(ring(8), 4, 4, uloc=4.0, xmu=2.0, hfmode=False)
+    q = np.cos(np.pi / 2 * np.arange(8))
+    din = torch.tensor(psi, device="cuda")
+    dout = torch.empty_like(din)
+    L.check(L.lib().edg_apply_diagop_dev_f64(s.handle, 0, 0, 0, q.ctypes.data_as(L._pd), C.c_void_p(din.data_ptr()),
+                                             C.c_void_p(dout.data_ptr())), "sz_q")
+    torch.cuda.synchronize()
+    ref = sum(q[i] * O.apply_diagop(8, 4, 4, 0, i + 1, psi) for i in range(8))
+    assert np.abs(dout.cpu().numpy() - ref).max() < 1e-14
+
+
+def test_oc_chain_vs_oracle():
+    gm, om, s, e0, psi = _gs_pair(ring(8), 4, 4, uloc=4.0, xmu=2.0, hfmode=False)
+    sp = E.oc_chain(s, 80, e0)
+    x = O.apply_current(om, 4, 4, psi)
+    a, b, n2, n = O.Stored(om, 4, 4).tridiag(x, 80)
+    p, w = O.poles_weights(a[:n], b[:n], n2, e0, +1)
+    assert abs(sp.norm2 - n2) < 1e-12 * max(1.0, n2)
+    big = w > 1e-6
+    for pr, wr in zip(p[big], w[big]):
+        j = np.argmin(np.abs(sp.poles - pr))
+        assert abs(sp.poles[j] - pr) < 1e-6 and abs(sp.weight[j] - wr) < 1e-6
+
+
+def test_observables_vs_oracle():
+    gm, om, s, e0, psi = _gs_pair(square_lattice(3, 4), 5, 4, uloc=4.0, xmu=2.0, hfmode=False)
+    obs = s.observables(0.5)
+    ref = O.observables(12, 5, 4, psi, 0.5)
+    for k in ("dens", "dens_up", "dens_dw", "docc", "magz"):
+        assert np.allclose(obs[k], ref[k], atol=1e-13), k
