@@ -251,6 +251,8 @@ int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
   return EDG_OK;
 }
 
+int build_sell(edg_sector_s* s, SpinBasis& B);
+
 int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   cudaStream_t st = s->stream;
   const BondList& bl = s->bonds[spin - 1];
@@ -285,6 +287,61 @@ int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   k_hop_fill<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, bh.p, nb, s->binom.p, B.off.p, B.src.p, B.val64.p,
                                      B.val32.p);
   EDG_CUDA(cudaGetLastError());
+  EDG_CUDA(cudaStreamSynchronize(st));
+  return build_sell(s, B);
+}
+
+// SELL-32 copy of a gather table, built on the host from the device CSR (the tables are
+// O(DimUp) -- about 1 MB for a 4x4 lattice -- so this is a one-off of milliseconds).
+int build_sell(edg_sector_s* s, SpinBasis& B) {
+  cudaStream_t st = s->stream;
+  const int64_t dim = B.dim;
+  std::vector<uint32_t> off(dim + 1), src(B.nnz + 1);
+  std::vector<double> val(B.nnz + 1);
+  EDG_CUDA(cudaMemcpyAsync(off.data(), B.off.p, (dim + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (B.nnz) {
+    EDG_CUDA(cudaMemcpyAsync(src.data(), B.src.p, B.nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaMemcpyAsync(val.data(), B.val64.p, B.nnz * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  EDG_CUDA(cudaStreamSynchronize(st));
+  const int64_t nsl = (dim + 31) / 32;
+  std::vector<uint32_t> soff(nsl + 1, 0);
+  for (int64_t sl = 0; sl < nsl; ++sl) {
+    uint32_t w = 0;
+    for (int64_t r = sl * 32; r < std::min<int64_t>(dim, sl * 32 + 32); ++r) w = std::max(w, off[r + 1] - off[r]);
+    soff[sl + 1] = soff[sl] + 32 * w;
+  }
+  double h0 = B.nnz ? std::fabs(val[0]) : 0.0;
+  bool uniform = true;
+  for (int64_t k = 0; k < B.nnz; ++k)
+    if (std::fabs(val[k]) != h0) { uniform = false; break; }
+  const double hsgn = B.nnz ? (val[0] < 0 ? -h0 : h0) : 0.0;  // value encoded by code 0
+  std::vector<uint32_t> ent(soff[nsl] + 1, 2u << 30);
+  std::vector<double> sv(uniform ? 0 : soff[nsl] + 1, 0.0);
+  for (int64_t r = 0; r < dim; ++r) {
+    const int64_t sl = r / 32, lane = r % 32;
+    for (uint32_t k = 0; k < off[r + 1] - off[r]; ++k) {
+      const uint32_t e = off[r] + k;
+      const size_t pos = soff[sl] + size_t(k) * 32 + lane;
+      uint32_t code = 0;
+      if (uniform) code = (val[e] == hsgn) ? 0u : 1u;
+      else sv[pos] = val[e];
+      ent[pos] = src[e] | (code << 30);
+    }
+  }
+  B.sell_uniform = uniform;
+  B.sell_h = hsgn;
+  EDG_CHECK(B.sell_off.alloc(nsl + 1, "SELL offsets"));
+  EDG_CHECK(B.sell_ent.alloc(ent.size(), "SELL entries"));
+  EDG_CUDA(cudaMemcpyAsync(B.sell_off.p, soff.data(), soff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  EDG_CUDA(cudaMemcpyAsync(B.sell_ent.p, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  if (!uniform) {
+    std::vector<float> sv32(sv.begin(), sv.end());
+    EDG_CHECK(B.sell_v64.alloc(sv.size(), "SELL values"));
+    EDG_CHECK(B.sell_v32.alloc(sv.size(), "SELL values"));
+    EDG_CUDA(cudaMemcpyAsync(B.sell_v64.p, sv.data(), sv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    EDG_CUDA(cudaMemcpyAsync(B.sell_v32.p, sv32.data(), sv32.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  }
   EDG_CUDA(cudaStreamSynchronize(st));
   return EDG_OK;
 }

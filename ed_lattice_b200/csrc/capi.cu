@@ -439,7 +439,7 @@ static int finish_chain(edg_sector_s* s, const double* x, int nlanc, int precisi
                         double* poles, double* weights, double* norm2, int* nout) {
   std::vector<double> a(nlanc > 0 ? nlanc : 1), b(nlanc > 0 ? nlanc : 1);
   int steps = 0;
-  EDG_CHECK(tridiag_dev(s, x, nlanc, 1e-12, precision, a.data(), b.data(), norm2, &steps));
+  EDG_CHECK(tridiag_dev(s, x, nlanc, 1e-9, precision, a.data(), b.data(), norm2, &steps));
   *nout = steps;
   if (steps == 0) return EDG_OK;
   return edg_poles_weights(steps, a.data(), b.data(), *norm2, ei, isign, poles, weights);

@@ -65,6 +65,81 @@ __global__ void __launch_bounds__(256) k_up_rows(HxvArgs<T> a) {
   }
 }
 
+// Row pass with the rows staged in shared memory. A CTA takes RT consecutive rows, stores
+// them interleaved (S[jup] holds the RT values of column jup, one vector load per hop) and
+// gathers H_up's sources from there instead of from L1, where random 4-byte reads cost a
+// wavefront per distinct line. The table is SELL-32: the k-th entries of a warp's 32
+// target columns are one coalesced 128-byte read, shared by the RT rows.
+template <typename T, int RT>
+struct VecT;
+template <> struct VecT<float, 1> { using type = float; };
+template <> struct VecT<float, 2> { using type = float2; };
+template <> struct VecT<float, 4> { using type = float4; };
+template <> struct VecT<double, 1> { using type = double; };
+template <> struct VecT<double, 2> { using type = double2; };
+
+template <typename T>
+struct SellArgs {
+  const uint32_t* __restrict__ ent;
+  const uint32_t* __restrict__ off;
+  const T* __restrict__ val;  // non-uniform tables only
+  T h;                        // value of code 0 (uniform tables)
+};
+
+template <typename T, int RT, bool FIRST, bool UNIFORM>
+__global__ void __launch_bounds__(512) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+  using V = typename VecT<T, RT>::type;
+  extern __shared__ __align__(16) unsigned char smem_up[];
+  V* S = reinterpret_cast<V*>(smem_up);
+  const int64_t dimup = a.dimup;
+  for (int64_t rb = blockIdx.x; rb < nrowblk; rb += gridDim.x) {
+    const int64_t r0 = rb * RT;
+    for (int64_t j = threadIdx.x; j < dimup; j += blockDim.x) {
+      V x;
+      T* xs = reinterpret_cast<T*>(&x);
+#pragma unroll
+      for (int r = 0; r < RT; ++r) xs[r] = (r0 + r < a.dimdw) ? a.v[(r0 + r) * dimup + j] : T(0);
+      S[j] = x;
+    }
+    __syncthreads();
+    for (int64_t iup = threadIdx.x; iup < dimup; iup += blockDim.x) {
+      T acc[RT];
+      if (FIRST) {
+        const V xc = S[iup];
+        const T* xs = reinterpret_cast<const T*>(&xc);
+        const T eu = a.e_up[iup];
+        const uint32_t mu = a.map_up[iup];
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+          const int64_t row = r0 + r < a.dimdw ? r0 + r : a.dimdw - 1;
+          acc[r] = (eu + a.e_dw[row] + a.U * T(__popc(mu & a.map_dw[row]))) * xs[r];
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < RT; ++r) acc[r] = (r0 + r < a.dimdw) ? a.hv[(r0 + r) * dimup + iup] : T(0);
+      }
+      const int64_t slice = iup >> 5;
+      const int lane = int(iup & 31);
+      const uint32_t o = sl.off[slice], o1 = sl.off[slice + 1];
+      for (uint32_t p = o + lane; p < o1; p += 32) {
+        const uint32_t e = sl.ent[p];
+        const uint32_t code = e >> 30;
+        T h;
+        if (UNIFORM) h = code == 0 ? sl.h : (code == 1 ? -sl.h : T(0));
+        else h = sl.val[p];
+        const V x = S[e & 0x3fffffffu];
+        const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+        for (int r = 0; r < RT; ++r) acc[r] = fmaT<T>(h, xs[r], acc[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < RT; ++r)
+        if (r0 + r < a.dimdw) a.hv[(r0 + r) * dimup + iup] = acc[r];
+    }
+    __syncthreads();
+  }
+}
+
 // Column-slab pass: a tile is 32 consecutive iup x 8 rows; tiles are visited slab-major so
 // that the slab of V being combined (DimDw rows x 32 columns) stays resident in L2 while
 // every row of it is read ~(hops per row) times. FIRST: hv = diag*v + dw-part.
@@ -172,6 +247,64 @@ int sm_count() {
   return cached;
 }
 
+template <typename T>
+const T* pick_sell(const SpinBasis& B);
+template <>
+const double* pick_sell<double>(const SpinBasis& B) { return B.sell_v64.p; }
+template <>
+const float* pick_sell<float>(const SpinBasis& B) { return B.sell_v32.p; }
+
+constexpr size_t kSmemTwoPerSM = 113 * 1024;  // two CTAs per SM
+constexpr size_t kSmemOnePerSM = 227 * 1024;  // opt-in maximum per CTA
+
+template <typename T, int RT, bool FIRST, bool UNIFORM>
+int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, int sms) {
+  const size_t smem = size_t(a.dimup) * RT * sizeof(T);
+  auto kern = k_up_smem<T, RT, FIRST, UNIFORM>;
+  if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int64_t nrb = (a.dimdw + RT - 1) / RT;
+  const int per_sm = smem <= kSmemTwoPerSM ? 2 : 1;
+  const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
+  kern<<<int(g), 512, smem, st>>>(a, sl, nrb);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+// Rows per CTA: the most that fit two CTAs per SM, else one row with one CTA per SM;
+// 0 when a row does not fit shared memory at all (the L1-gather kernel takes over).
+template <typename T>
+int rows_per_cta(int64_t dimup) {
+  const size_t row = size_t(dimup) * sizeof(T);
+  if (sizeof(T) == 4 && 4 * row <= kSmemTwoPerSM) return 4;
+  if (2 * row <= kSmemTwoPerSM) return 2;
+  if (row <= kSmemOnePerSM) return 1;
+  return 0;
+}
+
+template <typename T, bool FIRST>
+int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms) {
+  const int rt = rows_per_cta<T>(a.dimup);
+  if (rt == 0) {
+    const int g = int(a.dimdw < int64_t(sms) * 8 ? a.dimdw : int64_t(sms) * 8);
+    k_up_rows<T, FIRST><<<g, 256, 0, st>>>(a);
+    EDG_CUDA(cudaGetLastError());
+    return EDG_OK;
+  }
+  SellArgs<T> sl;
+  sl.ent = B.sell_ent.p;
+  sl.off = B.sell_off.p;
+  sl.val = pick_sell<T>(B);
+  sl.h = T(B.sell_h);
+  if (B.sell_uniform) {
+    if (rt == 4) return launch_up_smem<T, (sizeof(T) == 4 ? 4 : 2), FIRST, true>(a, sl, st, sms);
+    if (rt == 2) return launch_up_smem<T, 2, FIRST, true>(a, sl, st, sms);
+    return launch_up_smem<T, 1, FIRST, true>(a, sl, st, sms);
+  }
+  if (rt == 4) return launch_up_smem<T, (sizeof(T) == 4 ? 4 : 2), FIRST, false>(a, sl, st, sms);
+  if (rt == 2) return launch_up_smem<T, 2, FIRST, false>(a, sl, st, sms);
+  return launch_up_smem<T, 1, FIRST, false>(a, sl, st, sms);
+}
+
 }  // namespace
 
 template <typename T>
@@ -200,9 +333,7 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
     const int g1 = int(ntiles < int64_t(sms) * 8 ? ntiles : int64_t(sms) * 8);
     k_dw_slab<T, true><<<g1, dim3(32, 8), 0, st>>>(a, nrb, ntiles);
     EDG_CUDA(cudaGetLastError());
-    const int g2 = int(a.dimdw < int64_t(sms) * 8 ? a.dimdw : int64_t(sms) * 8);
-    k_up_rows<T, false><<<g2, 256, 0, st>>>(a);
-    EDG_CUDA(cudaGetLastError());
+    EDG_CHECK((up_pass<T, false>(a, s->up, st, sms)));
   } else {
     DirectArgsHdr d;
     d.nb_up = s->bonds[0].nb;

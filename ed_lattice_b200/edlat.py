@@ -240,7 +240,7 @@ def random_vector(seed: int, n: int) -> np.ndarray:
     return out
 
 
-def tridiag_Hv_sector(sector: Sector, vvinit: np.ndarray, nlanc: int | None = None, threshold: float = 1e-12,
+def tridiag_Hv_sector(sector: Sector, vvinit: np.ndarray, nlanc: int | None = None, threshold: float = 1e-9,
                       precision: int = L.EDG_PREC_F64):
     """tridiag_Hv_sector(isector,vvinit,alanc,blanc,norm2) (src/DIAG/HAMILTONIAN.f90:242-275).
     nlanc defaults to Nlanc = min(Dim, lanc_nGFiter=200) (src/SECTOR.f90:112).

@@ -184,7 +184,7 @@ class Stored:
         lib().orc_stored_matvec_z(self.h, _ptr(v), _ptr(hv))
         return hv
 
-    def tridiag(self, vvinit, nlanc, threshold=1e-12):
+    def tridiag(self, vvinit, nlanc, threshold=1e-9):
         a, b, n2 = np.zeros(nlanc), np.zeros(nlanc), C.c_double()
         v = np.ascontiguousarray(vvinit, dtype=np.float64)
         n = lib().orc_tridiag_d(self.h, _ptr(v), nlanc, threshold, _ptr(a), _ptr(b), C.byref(n2))

@@ -76,10 +76,11 @@ def disorder3x4():
     # c^+_{5,up}|GS> into (4,2), 60 steps
     x = O.apply_cop(12, 3, 2, +1, 5, 1, vec)
     stJ = O.Stored(m, 4, 2)
-    a, b, n2, n = stJ.tridiag(x, 60)
+    a, b, n2, n = stJ.tridiag(x, 60, 1e-9)
     p, w = O.poles_weights(a[:n], b[:n], n2, e0, +1)
     np.savez_compressed(os.path.join(HERE, "disorder3x4.npz"), eps=eps, v0=v0, hv=hv, rp_up=rp_up, c_up=c_up,
-                        v_up=v_up, rp_dw=rp_dw, c_dw=c_dw, v_dw=v_dw, e0=e0, gf_poles=p, gf_weights=w, gf_norm2=n2)
+                        v_up=v_up, rp_dw=rp_dw, c_dw=c_dw, v_dw=v_dw, e0=e0, gs_vec=vec, gf_poles=p, gf_weights=w,
+                        gf_norm2=n2)
 
 
 if __name__ == "__main__":

@@ -26,6 +26,23 @@ def models(h, **kw):
     return E.Model(h, **kw), O.Model(h, **kw)
 
 
+def assert_spectra_close(sp, p_ref, w_ref, n2_ref, temp=0.02, nmats=64):
+    """Chains from two implementations agree as functions, not pole by pole: unconverged
+    high-energy Ritz values of a finite chain depend on rounding once orthogonality is
+    lost. Checked: norm2, the weight sum rule, G(iw_n) on a Matsubara grid, and the poles
+    that carry weight (> 1e-3 of norm2)."""
+    assert abs(sp.norm2 - n2_ref) <= 1e-12 * max(1.0, n2_ref)
+    assert abs(sp.weight.sum() - sp.norm2) <= 1e-12 * max(1.0, sp.norm2)
+    wm = np.pi * temp * (2 * np.arange(1, nmats + 1) - 1)
+    g = (sp.weight[None, :] / (1j * wm[:, None] - sp.poles[None, :])).sum(1)
+    gr = (w_ref[None, :] / (1j * wm[:, None] - p_ref[None, :])).sum(1)
+    assert np.abs(g - gr).max() <= 1e-8 * np.abs(gr).max()
+    for pr, wr in zip(p_ref, w_ref):
+        if wr > 1e-3 * n2_ref:
+            j = np.argmin(np.abs(sp.poles - pr))
+            assert abs(sp.poles[j] - pr) < 1e-7 and abs(sp.weight[j] - wr) < 1e-7 * max(1.0, n2_ref)
+
+
 # ----------------------------------------------------------------------------- basis / tables
 @pytest.mark.parametrize("ns", [1, 2, 5, 8, 12])
 def test_maps_bit_exact_all_sectors(ns):
@@ -233,8 +250,12 @@ def test_tridiag_early_stop_and_zero_vector():
     gm = E.Model(ring(4), uloc=2.0, xmu=1.0, hfmode=False)
     s = E.Sector(gm, 2, 1)  # dim 6*4 = 24: Krylov space exhausts before 40 steps
     v = O.random_vector(1, s.dim)
-    a, b, n2, n = E.tridiag_Hv_sector(s, v, 40)
-    assert n <= s.dim and np.all(a[n:] == 0) and np.all(b[n:] == 0)
+    # the Krylov space has 12 dimensions (distinct eigenvalues); after it is exhausted b
+    # falls to round-off (~1e-12 after the orthogonality loss), far below the threshold
+    a, b, n2, n = E.tridiag_Hv_sector(s, v, 40, threshold=1e-9)
+    ao, bo, n2o, no = O.Stored(O.Model(ring(4), uloc=2.0, xmu=1.0, hfmode=False), 2, 1).tridiag(v, 40, 1e-9)
+    assert n == no == 12 and np.all(a[n:] == 0) and np.all(b[n:] == 0)
+    assert np.abs(a[:n] - ao[:n]).max() < 1e-10
     a, b, n2, n = E.tridiag_Hv_sector(s, np.zeros(s.dim), 10)
     assert n2 == 0.0 and n == 0 and np.all(a == 0)
 
@@ -288,15 +309,11 @@ def test_gf_chain_vs_oracle_and_golden():
     s = E.Sector(gm, 3, 2)
     e0, vec, _ = E.sp_lanc_eigh(s, v0=g["v0"], tol=1e-14, maxit=400)
     assert abs(e0 - float(g["e0"])) < 1e-10 * abs(e0)
+    # the chain from the fixture's own ground-state vector isolates the chain arithmetic
+    s.set_state(g["gs_vec"])
     sJ = E.Sector(gm, 4, 2)
-    sp = E.gf_chain(s, sJ, +1, 5, 1, 60, e0)
-    assert abs(sp.norm2 - float(g["gf_norm2"])) < 1e-9
-    big = g["gf_weights"] > 1e-6
-    # converged poles carry the weight; compare weight-resolved low-energy poles
-    for p_ref, w_ref in zip(g["gf_poles"][big], g["gf_weights"][big]):
-        j = np.argmin(np.abs(sp.poles - p_ref))
-        assert abs(sp.poles[j] - p_ref) < 1e-6 and abs(sp.weight[j] - w_ref) < 1e-6
-    assert abs(sp.weight.sum() - sp.norm2) < 1e-12
+    sp = E.gf_chain(s, sJ, +1, 5, 1, 60, float(g["e0"]))
+    assert_spectra_close(sp, g["gf_poles"], g["gf_weights"], float(g["gf_norm2"]))
 
 
 def test_gf_lanczos_vs_full_lehmann_gpu():
@@ -321,13 +338,9 @@ def test_chi_chain_vs_oracle(kind, site, site2):
     gm, om, s, e0, psi = _gs_pair(ring(8), 4, 4, uloc=4.0, xmu=2.0, hfmode=False)
     sp = E.chi_chain(s, site, 80, e0, kind=kind, site2=site2)
     x = O.apply_diagop(8, 4, 4, kind, site, psi, site2)
-    a, b, n2, n = O.Stored(om, 4, 4).tridiag(x, 80)
+    a, b, n2, n = O.Stored(om, 4, 4).tridiag(x, 80, 1e-9)
     p, w = O.poles_weights(a[:n], b[:n], n2, e0, +1)
-    assert abs(sp.norm2 - n2) < 1e-12 * max(1.0, n2)
-    big = w > 1e-6
-    for pr, wr in zip(p[big], w[big]):
-        j = np.argmin(np.abs(sp.poles - pr))
-        assert abs(sp.poles[j] - pr) < 1e-6 and abs(sp.weight[j] - wr) < 1e-6
+    assert_spectra_close(sp, p, w, n2)
 
 
 def test_momentum_chi_vector():
@@ -347,13 +360,9 @@ def test_oc_chain_vs_oracle():
     gm, om, s, e0, psi = _gs_pair(ring(8), 4, 4, uloc=4.0, xmu=2.0, hfmode=False)
     sp = E.oc_chain(s, 80, e0)
     x = O.apply_current(om, 4, 4, psi)
-    a, b, n2, n = O.Stored(om, 4, 4).tridiag(x, 80)
+    a, b, n2, n = O.Stored(om, 4, 4).tridiag(x, 80, 1e-9)
     p, w = O.poles_weights(a[:n], b[:n], n2, e0, +1)
-    assert abs(sp.norm2 - n2) < 1e-12 * max(1.0, n2)
-    big = w > 1e-6
-    for pr, wr in zip(p[big], w[big]):
-        j = np.argmin(np.abs(sp.poles - pr))
-        assert abs(sp.poles[j] - pr) < 1e-6 and abs(sp.weight[j] - wr) < 1e-6
+    assert_spectra_close(sp, p, w, n2)
 
 
 def test_observables_vs_oracle():
