@@ -87,7 +87,7 @@ struct SellArgs {
 };
 
 template <typename T, int RT, bool FIRST, bool UNIFORM>
-__global__ void __launch_bounds__(512) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+__global__ void __launch_bounds__(1024) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
@@ -104,6 +104,9 @@ __global__ void __launch_bounds__(512) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, i
     __syncthreads();
     for (int64_t iup = threadIdx.x; iup < dimup; iup += blockDim.x) {
       T acc[RT];
+      const int64_t slice = iup >> 5;
+      const int lane = int(iup & 31);
+      const uint32_t o = sl.off[slice], o1 = sl.off[slice + 1];
       if (FIRST) {
         const V xc = S[iup];
         const T* xs = reinterpret_cast<const T*>(&xc);
@@ -118,25 +121,122 @@ __global__ void __launch_bounds__(512) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, i
 #pragma unroll
         for (int r = 0; r < RT; ++r) acc[r] = (r0 + r < a.dimdw) ? a.hv[(r0 + r) * dimup + iup] : T(0);
       }
-      const int64_t slice = iup >> 5;
-      const int lane = int(iup & 31);
-      const uint32_t o = sl.off[slice], o1 = sl.off[slice + 1];
-      for (uint32_t p = o + lane; p < o1; p += 32) {
-        const uint32_t e = sl.ent[p];
-        const uint32_t code = e >> 30;
-        T h;
-        if (UNIFORM) h = code == 0 ? sl.h : (code == 1 ? -sl.h : T(0));
-        else h = sl.val[p];
-        const V x = S[e & 0x3fffffffu];
-        const T* xs = reinterpret_cast<const T*>(&x);
+      // entries in batches of kUpBatch independent loads (padding entries past the slice
+      // end read as code 2 = zero weight), then the shared-memory gathers
+      constexpr int kUpBatch = 8;
+      for (uint32_t p0 = o + lane; p0 < o1; p0 += 32 * kUpBatch) {
+        uint32_t e[kUpBatch];
+        T hv_[kUpBatch];
 #pragma unroll
-        for (int r = 0; r < RT; ++r) acc[r] = fmaT<T>(h, xs[r], acc[r]);
+        for (int u = 0; u < kUpBatch; ++u) {
+          const uint32_t p = p0 + 32u * u;
+          e[u] = p < o1 ? __ldg(sl.ent + p) : (2u << 30);
+          if (!UNIFORM) hv_[u] = p < o1 ? __ldg(sl.val + p) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < kUpBatch; ++u) {
+          const uint32_t code = e[u] >> 30;
+          const T h = UNIFORM ? (code == 0 ? sl.h : (code == 1 ? -sl.h : T(0))) : hv_[u];
+          const V x = S[e[u] & 0x3fffffffu];
+          const T* xs = reinterpret_cast<const T*>(&x);
+#pragma unroll
+          for (int r = 0; r < RT; ++r) acc[r] = fmaT<T>(h, xs[r], acc[r]);
+        }
       }
 #pragma unroll
       for (int r = 0; r < RT; ++r)
         if (r0 + r < a.dimdw) a.hv[(r0 + r) * dimup + iup] = acc[r];
     }
     __syncthreads();
+  }
+}
+
+// Down-spin pass, one warp per (row idw', segment of 32*VEC consecutive iup). The row's hop
+// list is uniform across the warp: lanes load up to 32 (source, value) pairs in one
+// coalesced read and hand them out with shuffles; the source rows are then read as
+// independent VEC-wide loads, unrolled so several are in flight per thread. Segments are
+// visited slab-major (all rows of a 32*VEC-column slab before the next slab) so the slab
+// (DimDw * 32*VEC*sizeof(T) bytes) stays in L2 while each of its rows is read ~hops times.
+template <typename T, int VEC>
+struct VecLd;
+template <typename T>
+struct VecLd<T, 1> {
+  static __device__ __forceinline__ void load(const T* p, T* x) { x[0] = __ldg(p); }
+};
+template <>
+struct VecLd<float, 2> {
+  static __device__ __forceinline__ void load(const float* p, float* x) {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+    x[0] = t.x;
+    x[1] = t.y;
+  }
+};
+template <>
+struct VecLd<double, 2> {
+  static __device__ __forceinline__ void load(const double* p, double* x) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+    x[0] = t.x;
+    x[1] = t.y;
+  }
+};
+
+template <typename T, int VEC, bool FIRST>
+__global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wpb = blockDim.x >> 5;
+  const int64_t dimup = a.dimup, dimdw = a.dimdw;
+  for (int64_t tile = blockIdx.x * wpb + (threadIdx.x >> 5); tile < ntiles; tile += int64_t(gridDim.x) * wpb) {
+    const int64_t slab = tile / dimdw, idw = tile - slab * dimdw;
+    const int64_t col = slab * (32 * VEC) + int64_t(lane) * VEC;
+    const bool active = col < dimup;
+    const int64_t e0 = idw * dimup + col;
+    T acc[VEC];
+    if (active) {
+      if (FIRST) {
+        const T edw = a.e_dw[idw];
+        const uint32_t mdw = a.map_dw[idw];
+        T x[VEC];
+        VecLd<T, VEC>::load(a.v + e0, x);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q)
+          acc[q] = (a.e_up[col + q] + edw + a.U * T(__popc(a.map_up[col + q] & mdw))) * x[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) acc[q] = a.hv[e0 + q];
+      }
+    }
+    const uint32_t k0 = a.off_dw[idw], k1 = a.off_dw[idw + 1];
+    for (uint32_t base = k0; base < k1; base += 32) {
+      const int cnt = int(k1 - base < 32u ? k1 - base : 32u);
+      const uint32_t my_src = lane < cnt ? a.src_dw[base + lane] : 0u;
+      const T my_val = lane < cnt ? a.val_dw[base + lane] : T(0);
+      constexpr int kU = 4;
+      for (int k = 0; k < cnt; k += kU) {
+        T x[kU][VEC];
+        T h[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int kk = k + u < cnt ? k + u : k;  // out-of-range slots repeat a valid row
+          const uint32_t sr = __shfl_sync(0xffffffffu, my_src, kk);
+          h[u] = __shfl_sync(0xffffffffu, my_val, kk);
+          if (k + u >= cnt) h[u] = T(0);
+          if (active) VecLd<T, VEC>::load(a.v + int64_t(sr) * dimup + col, x[u]);
+        }
+        if (active) {
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            if (k + u < cnt) {
+#pragma unroll
+              for (int q = 0; q < VEC; ++q) acc[q] = fmaT<T>(h[u], x[u][q], acc[q]);
+            }
+          }
+        }
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < VEC; ++q) a.hv[e0 + q] = acc[q];
+    }
   }
 }
 
@@ -265,7 +365,7 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   const int per_sm = smem <= kSmemTwoPerSM ? 2 : 1;
   const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
-  kern<<<int(g), 512, smem, st>>>(a, sl, nrb);
+  kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -279,6 +379,23 @@ int rows_per_cta(int64_t dimup) {
   if (2 * row <= kSmemTwoPerSM) return 2;
   if (row <= kSmemOnePerSM) return 1;
   return 0;
+}
+
+// VEC-wide loads need every row start aligned: DimUp a multiple of VEC and 2*sizeof(T)
+// aligned vector pointers (always true for our own buffers; checked for callers' pointers).
+template <typename T, bool FIRST>
+int dw_pass(const HxvArgs<T>& a, cudaStream_t st, int sms) {
+  const bool v2 = (a.dimup % 2 == 0) && (reinterpret_cast<uintptr_t>(a.v) % (2 * sizeof(T)) == 0) &&
+                  (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
+  const int vec = v2 ? 2 : 1;
+  const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
+  const int64_t ntiles = nslab * a.dimdw;
+  const int64_t want = (ntiles + 7) / 8;
+  const int g = int(want < int64_t(sms) * 8 ? want : int64_t(sms) * 8);
+  if (v2) k_dw_seg<T, 2, FIRST><<<g, 256, 0, st>>>(a, ntiles);
+  else k_dw_seg<T, 1, FIRST><<<g, 256, 0, st>>>(a, ntiles);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
 }
 
 template <typename T, bool FIRST>
@@ -328,11 +445,7 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
   const int sms = sm_count();
   cudaStream_t st = s->stream;
   if (s->form == EDG_FORM_STORED) {
-    const int64_t nslab = (a.dimup + 31) / 32, nrb = (a.dimdw + 7) / 8;
-    const int64_t ntiles = nslab * nrb;
-    const int g1 = int(ntiles < int64_t(sms) * 8 ? ntiles : int64_t(sms) * 8);
-    k_dw_slab<T, true><<<g1, dim3(32, 8), 0, st>>>(a, nrb, ntiles);
-    EDG_CUDA(cudaGetLastError());
+    EDG_CHECK((dw_pass<T, true>(a, st, sms)));
     EDG_CHECK((up_pass<T, false>(a, s->up, st, sms)));
   } else {
     DirectArgsHdr d;

@@ -40,7 +40,7 @@ def assert_spectra_close(sp, p_ref, w_ref, n2_ref, temp=0.02, nmats=64):
     for pr, wr in zip(p_ref, w_ref):
         if wr > 1e-3 * n2_ref:
             j = np.argmin(np.abs(sp.poles - pr))
-            assert abs(sp.poles[j] - pr) < 1e-7 and abs(sp.weight[j] - wr) < 1e-7 * max(1.0, n2_ref)
+            assert abs(sp.poles[j] - pr) < 1e-6 and abs(sp.weight[j] - wr) < 1e-6 * max(1.0, n2_ref)
 
 
 # ----------------------------------------------------------------------------- basis / tables
