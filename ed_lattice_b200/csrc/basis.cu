@@ -316,17 +316,19 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
   for (int64_t k = 0; k < B.nnz; ++k)
     if (std::fabs(val[k]) != h0) { uniform = false; break; }
   const double hsgn = B.nnz ? (val[0] < 0 ? -h0 : h0) : 0.0;  // value encoded by code 0
-  std::vector<uint32_t> ent(soff[nsl] + 1, 2u << 30);
+  // entry: bit 31 = sign (uniform tables), bits 0..30 = source; padding points at the
+  // zero slot dim that the up pass keeps after the staged rows
+  std::vector<uint32_t> ent(soff[nsl] + 1, uint32_t(dim));
   std::vector<double> sv(uniform ? 0 : soff[nsl] + 1, 0.0);
   for (int64_t r = 0; r < dim; ++r) {
     const int64_t sl = r / 32, lane = r % 32;
     for (uint32_t k = 0; k < off[r + 1] - off[r]; ++k) {
       const uint32_t e = off[r] + k;
       const size_t pos = soff[sl] + size_t(k) * 32 + lane;
-      uint32_t code = 0;
-      if (uniform) code = (val[e] == hsgn) ? 0u : 1u;
+      uint32_t sign = 0;
+      if (uniform) sign = (val[e] == hsgn) ? 0u : 1u;
       else sv[pos] = val[e];
-      ent[pos] = src[e] | (code << 30);
+      ent[pos] = src[e] | (sign << 31);
     }
   }
   B.sell_uniform = uniform;

@@ -78,8 +78,9 @@ struct SpinBasis {
   int64_t nnz = 0;
   // The same table in SELL-32 layout (slices of 32 consecutive target rows padded to the
   // slice's longest row, stored entry-major) so a warp reading the k-th entry of its 32
-  // rows touches one 128-byte line. Entry = src | code << 30 with code 0: +hval,
-  // 1: -hval, 2: padding (adds nothing). Non-uniform |values| keep a parallel value array.
+  // rows touches one 128-byte line.
+  // Entry = src | sign << 31 (sign of hval; padding = src DimUp, a zero slot). Non-uniform
+  // |values| keep a parallel value array.
   DevBuf<uint32_t> sell_ent;    // [sell_len]
   DevBuf<uint32_t> sell_off;    // [nslices+1], entry offsets, multiples of 32
   DevBuf<double> sell_v64;      // only when !sell_uniform

@@ -83,15 +83,61 @@ struct SellArgs {
   const uint32_t* __restrict__ ent;
   const uint32_t* __restrict__ off;
   const T* __restrict__ val;  // non-uniform tables only
-  T h;                        // value of code 0 (uniform tables)
+  T h;                        // |value| with the sign of code 0 (uniform tables)
 };
 
+// acc[0..RT) += h * x[0..RT): packed FP32x2 FMAs where the pair shares h (Blackwell
+// fma.rn.f32x2; each lane is an IEEE fma, identical to two scalar ones).
+template <typename T, int RT>
+struct Fma {
+  static __device__ __forceinline__ void run(T h, const T* x, T* acc) {
+#pragma unroll
+    for (int r = 0; r < RT; ++r) acc[r] = fmaT<T>(h, x[r], acc[r]);
+  }
+};
+__device__ __forceinline__ void ffma2(float h, const float* x, float* acc) {
+  uint64_t d;
+  const uint64_t uh = (uint64_t(__float_as_uint(h)) << 32) | __float_as_uint(h);
+  const uint64_t ux = (uint64_t(__float_as_uint(x[1])) << 32) | __float_as_uint(x[0]);
+  const uint64_t ua = (uint64_t(__float_as_uint(acc[1])) << 32) | __float_as_uint(acc[0]);
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(uh), "l"(ux), "l"(ua));
+  acc[0] = __uint_as_float(uint32_t(d));
+  acc[1] = __uint_as_float(uint32_t(d >> 32));
+}
+template <>
+struct Fma<float, 2> {
+  static __device__ __forceinline__ void run(float h, const float* x, float* acc) { ffma2(h, x, acc); }
+};
+template <>
+struct Fma<float, 4> {
+  static __device__ __forceinline__ void run(float h, const float* x, float* acc) {
+    ffma2(h, x, acc);
+    ffma2(h, x + 2, acc + 2);
+  }
+};
+
+__device__ __forceinline__ float flip_sign(float h, uint32_t e) {
+  return __uint_as_float(__float_as_uint(h) ^ (e & 0x80000000u));
+}
+__device__ __forceinline__ double flip_sign(double h, uint32_t e) {
+  return __longlong_as_double(__double_as_longlong(h) ^ (static_cast<long long>(e & 0x80000000u) << 32));
+}
+
+// SELL entry: bit 31 = sign of the uniform value, bits 0..30 = source column (DimUp for
+// padding: a zero slot after the staged rows, so padding needs no branch).
 template <typename T, int RT, bool FIRST, bool UNIFORM>
-__global__ void __launch_bounds__(1024) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+__global__ void __launch_bounds__(512) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
   const int64_t dimup = a.dimup;
+  if (threadIdx.x == 0) {
+    V z;
+    T* zs = reinterpret_cast<T*>(&z);
+#pragma unroll
+    for (int r = 0; r < RT; ++r) zs[r] = T(0);
+    S[dimup] = z;
+  }
   for (int64_t rb = blockIdx.x; rb < nrowblk; rb += gridDim.x) {
     const int64_t r0 = rb * RT;
     for (int64_t j = threadIdx.x; j < dimup; j += blockDim.x) {
@@ -121,31 +167,28 @@ __global__ void __launch_bounds__(1024) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, 
 #pragma unroll
         for (int r = 0; r < RT; ++r) acc[r] = (r0 + r < a.dimdw) ? a.hv[(r0 + r) * dimup + iup] : T(0);
       }
-      // entries in batches of kUpBatch independent loads (padding entries past the slice
-      // end read as code 2 = zero weight), then the shared-memory gathers
+      // entries in batches of independent loads; slots past the slice end read the zero slot
       constexpr int kUpBatch = 8;
+      const uint32_t pad = uint32_t(dimup);
       for (uint32_t p0 = o + lane; p0 < o1; p0 += 32 * kUpBatch) {
         uint32_t e[kUpBatch];
         T hv_[kUpBatch];
 #pragma unroll
         for (int u = 0; u < kUpBatch; ++u) {
           const uint32_t p = p0 + 32u * u;
-          e[u] = p < o1 ? __ldg(sl.ent + p) : (2u << 30);
+          e[u] = p < o1 ? __ldg(sl.ent + p) : pad;
           if (!UNIFORM) hv_[u] = p < o1 ? __ldg(sl.val + p) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < kUpBatch; ++u) {
-          const uint32_t code = e[u] >> 30;
-          const T h = UNIFORM ? (code == 0 ? sl.h : (code == 1 ? -sl.h : T(0))) : hv_[u];
-          const V x = S[e[u] & 0x3fffffffu];
-          const T* xs = reinterpret_cast<const T*>(&x);
-#pragma unroll
-          for (int r = 0; r < RT; ++r) acc[r] = fmaT<T>(h, xs[r], acc[r]);
+          const T h = UNIFORM ? flip_sign(sl.h, e[u]) : hv_[u];
+          const V x = S[e[u] & 0x7fffffffu];
+          Fma<T, RT>::run(h, reinterpret_cast<const T*>(&x), acc);
         }
       }
 #pragma unroll
       for (int r = 0; r < RT; ++r)
-        if (r0 + r < a.dimdw) a.hv[(r0 + r) * dimup + iup] = acc[r];
+        if (r0 + r < a.dimdw) __stcs(a.hv + (r0 + r) * dimup + iup, acc[r]);
     }
     __syncthreads();
   }
@@ -210,7 +253,7 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
       const int cnt = int(k1 - base < 32u ? k1 - base : 32u);
       const uint32_t my_src = lane < cnt ? a.src_dw[base + lane] : 0u;
       const T my_val = lane < cnt ? a.val_dw[base + lane] : T(0);
-      constexpr int kU = 4;
+      constexpr int kU = 8;
       for (int k = 0; k < cnt; k += kU) {
         T x[kU][VEC];
         T h[kU];
@@ -235,7 +278,7 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
     }
     if (active) {
 #pragma unroll
-      for (int q = 0; q < VEC; ++q) a.hv[e0 + q] = acc[q];
+      for (int q = 0; q < VEC; ++q) __stcs(a.hv + e0 + q, acc[q]);  // streamed: read back only by the next pass
     }
   }
 }
@@ -359,13 +402,13 @@ constexpr size_t kSmemOnePerSM = 227 * 1024;  // opt-in maximum per CTA
 
 template <typename T, int RT, bool FIRST, bool UNIFORM>
 int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, int sms) {
-  const size_t smem = size_t(a.dimup) * RT * sizeof(T);
+  const size_t smem = size_t(a.dimup + 1) * RT * sizeof(T);
   auto kern = k_up_smem<T, RT, FIRST, UNIFORM>;
   if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   const int per_sm = smem <= kSmemTwoPerSM ? 2 : 1;
   const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
-  kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
+  kern<<<int(g), 512, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -374,7 +417,7 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
 // 0 when a row does not fit shared memory at all (the L1-gather kernel takes over).
 template <typename T>
 int rows_per_cta(int64_t dimup) {
-  const size_t row = size_t(dimup) * sizeof(T);
+  const size_t row = size_t(dimup + 1) * sizeof(T);
   if (sizeof(T) == 4 && 4 * row <= kSmemTwoPerSM) return 4;
   if (2 * row <= kSmemTwoPerSM) return 2;
   if (row <= kSmemOnePerSM) return 1;
