@@ -305,6 +305,8 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
   }
   EDG_CUDA(cudaStreamSynchronize(st));
   const int64_t nsl = (dim + 31) / 32;
+  B.max_row = 0;
+  for (int64_t r = 0; r < dim; ++r) B.max_row = std::max<int>(B.max_row, int(off[r + 1] - off[r]));
   std::vector<uint32_t> soff(nsl + 1, 0);
   for (int64_t sl = 0; sl < nsl; ++sl) {
     uint32_t w = 0;

@@ -87,6 +87,7 @@ struct SpinBasis {
   DevBuf<float> sell_v32;
   bool sell_uniform = true;
   double sell_h = 0.0;
+  int max_row = 0;              // longest hop list of any configuration
 };
 
 // Directed bond list for one spin: Hij(a,b) != 0, a != b, value = matrix element used when

@@ -126,7 +126,7 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 // SELL entry: bit 31 = sign of the uniform value, bits 0..30 = source column (DimUp for
 // padding: a zero slot after the staged rows, so padding needs no branch).
 template <typename T, int RT, bool FIRST, bool UNIFORM>
-__global__ void __launch_bounds__(512) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+__global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
@@ -283,6 +283,88 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
   }
 }
 
+// Down-spin pass, persistent form. Warp w owns the rows idw = w, w+W, w+2W, ... (W = warps
+// in the grid); their hop lists are copied once into shared memory, then all warps sweep the
+// column slabs in lockstep, so at any moment the grid works on about one slab (DimDw rows x
+// 32*VEC columns) that stays in L2 while each of its rows is read once per hop. No global
+// load on the hop list is left in the inner loop, and a warp keeps kU source-row loads in
+// flight.
+constexpr int kDwRowsPerWarp = 8;   // rows a warp can own (grid sized so W*8 >= DimDw)
+constexpr int kDwHops = 32;         // hop-list capacity per owned row held in shared memory
+
+template <typename T, int VEC, bool FIRST>
+__global__ void __launch_bounds__(256) k_dw_rows(HxvArgs<T> a, int64_t nslab) {
+  __shared__ uint32_t s_src[8][kDwRowsPerWarp][kDwHops];
+  __shared__ T s_val[8][kDwRowsPerWarp][kDwHops];
+  __shared__ int s_cnt[8][kDwRowsPerWarp];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t W = int64_t(gridDim.x) * (blockDim.x >> 5);
+  const int64_t w = blockIdx.x * int64_t(blockDim.x >> 5) + wib;
+  const int64_t dimup = a.dimup, dimdw = a.dimdw;
+  int nown = 0;
+  for (int q = 0; q < kDwRowsPerWarp; ++q) {
+    const int64_t idw = w + q * W;
+    if (idw >= dimdw) break;
+    const uint32_t k0 = a.off_dw[idw], k1 = a.off_dw[idw + 1];
+    const int cnt = int(k1 - k0);
+    if (lane < cnt && lane < kDwHops) {
+      s_src[wib][q][lane] = a.src_dw[k0 + lane];
+      s_val[wib][q][lane] = a.val_dw[k0 + lane];
+    }
+    if (lane == 0) s_cnt[wib][q] = cnt;
+    ++nown;
+  }
+  __syncwarp();
+  for (int64_t slab = 0; slab < nslab; ++slab) {
+    const int64_t col = slab * (32 * VEC) + int64_t(lane) * VEC;
+    const bool active = col < dimup;
+    for (int q = 0; q < nown; ++q) {
+      const int64_t idw = w + q * W;
+      const int64_t e0 = idw * dimup + col;
+      const int cnt = s_cnt[wib][q];
+      T acc[VEC];
+      if (active) {
+        if (FIRST) {
+          const T edw = a.e_dw[idw];
+          const uint32_t mdw = a.map_dw[idw];
+          T x[VEC];
+          VecLd<T, VEC>::load(a.v + e0, x);
+#pragma unroll
+          for (int r = 0; r < VEC; ++r)
+            acc[r] = (a.e_up[col + r] + edw + a.U * T(__popc(a.map_up[col + r] & mdw))) * x[r];
+        } else {
+#pragma unroll
+          for (int r = 0; r < VEC; ++r) acc[r] = a.hv[e0 + r];
+        }
+      }
+      constexpr int kU = 8;
+      for (int k = 0; k < cnt; k += kU) {
+        T x[kU][VEC];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int kk = k + u < cnt ? k + u : k;
+          const uint32_t sr = s_src[wib][q][kk];
+          if (active) VecLd<T, VEC>::load(a.v + int64_t(sr) * dimup + col, x[u]);
+        }
+        if (active) {
+#pragma unroll
+          for (int u = 0; u < kU; ++u) {
+            if (k + u < cnt) {
+              const T h = s_val[wib][q][k + u];
+#pragma unroll
+              for (int r = 0; r < VEC; ++r) acc[r] = fmaT<T>(h, x[u][r], acc[r]);
+            }
+          }
+        }
+      }
+      if (active) {
+#pragma unroll
+        for (int r = 0; r < VEC; ++r) __stcs(a.hv + e0 + r, acc[r]);
+      }
+    }
+  }
+}
+
 // Column-slab pass: a tile is 32 consecutive iup x 8 rows; tiles are visited slab-major so
 // that the slab of V being combined (DimDw rows x 32 columns) stays resident in L2 while
 // every row of it is read ~(hops per row) times. FIRST: hv = diag*v + dw-part.
@@ -408,7 +490,7 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   const int per_sm = smem <= kSmemTwoPerSM ? 2 : 1;
   const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
-  kern<<<int(g), 512, smem, st>>>(a, sl, nrb);
+  kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -427,10 +509,27 @@ int rows_per_cta(int64_t dimup) {
 // VEC-wide loads need every row start aligned: DimUp a multiple of VEC and 2*sizeof(T)
 // aligned vector pointers (always true for our own buffers; checked for callers' pointers).
 template <typename T, bool FIRST>
-int dw_pass(const HxvArgs<T>& a, cudaStream_t st, int sms) {
+int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms) {
   const bool v2 = (a.dimup % 2 == 0) && (reinterpret_cast<uintptr_t>(a.v) % (2 * sizeof(T)) == 0) &&
                   (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
   const int vec = v2 ? 2 : 1;
+  if (Bdw.max_row <= kDwHops) {
+    // persistent row-owner kernel: enough warps that each owns at most kDwRowsPerWarp rows
+    // all CTAs resident at once (a second wave would break the lockstep slab sweep)
+    auto kern = v2 ? k_dw_rows<T, 2, FIRST> : k_dw_rows<T, 1, FIRST>;
+    int occ = 0;
+    EDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0));
+    if (occ < 1) occ = 1;
+    const int64_t need = (a.dimdw + 8 * kDwRowsPerWarp - 1) / (8 * kDwRowsPerWarp);
+    const int64_t per_row = (a.dimdw + 7) / 8;
+    int64_t g = int64_t(sms) * occ;
+    if (g > per_row) g = per_row;
+    if (g < need) g = need;
+    const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
+    kern<<<int(g), 256, 0, st>>>(a, nslab);
+    EDG_CUDA(cudaGetLastError());
+    return EDG_OK;
+  }
   const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
   const int64_t ntiles = nslab * a.dimdw;
   const int64_t want = (ntiles + 7) / 8;
@@ -488,7 +587,7 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
   const int sms = sm_count();
   cudaStream_t st = s->stream;
   if (s->form == EDG_FORM_STORED) {
-    EDG_CHECK((dw_pass<T, true>(a, st, sms)));
+    EDG_CHECK((dw_pass<T, true>(a, s->dw, st, sms)));
     EDG_CHECK((up_pass<T, false>(a, s->up, st, sms)));
   } else {
     DirectArgsHdr d;
