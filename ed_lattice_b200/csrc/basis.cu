@@ -307,6 +307,44 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
   const int64_t nsl = (dim + 31) / 32;
   B.max_row = 0;
   for (int64_t r = 0; r < dim; ++r) B.max_row = std::max<int>(B.max_row, int(off[r + 1] - off[r]));
+  // LPT grouping of rows for the down-spin pass: one group per resident CTA (4 per SM)
+  {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t G = std::max<int64_t>(1, std::min<int64_t>(int64_t(sms) * 4, dim));
+    std::vector<int64_t> order(dim);
+    for (int64_t r = 0; r < dim; ++r) order[r] = r;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t x, int64_t y) { return off[x + 1] - off[x] > off[y + 1] - off[y]; });
+    std::vector<std::pair<int64_t, int64_t>> heap;  // (load, group) min-heap
+    for (int64_t g = 0; g < G; ++g) heap.push_back({0, g});
+    auto cmp = [](const std::pair<int64_t, int64_t>& x, const std::pair<int64_t, int64_t>& y) { return x > y; };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    std::vector<std::vector<uint32_t>> members(G);
+    for (int64_t r : order) {
+      std::pop_heap(heap.begin(), heap.end(), cmp);
+      auto& top = heap.back();
+      members[top.second].push_back(uint32_t(r));
+      top.first += 1 + int64_t(off[r + 1] - off[r]);  // diagonal + hops
+      std::push_heap(heap.begin(), heap.end(), cmp);
+    }
+    std::vector<uint32_t> goff(G + 1, 0), grows;
+    grows.reserve(dim);
+    B.group_max = 0;
+    for (int64_t g = 0; g < G; ++g) {
+      std::sort(members[g].begin(), members[g].end());
+      grows.insert(grows.end(), members[g].begin(), members[g].end());
+      goff[g + 1] = uint32_t(grows.size());
+      B.group_max = std::max<int>(B.group_max, int(members[g].size()));
+    }
+    B.groups = int(G);
+    EDG_CHECK(B.group_off.alloc(G + 1, "row groups"));
+    EDG_CHECK(B.group_rows.alloc(grows.size() + 1, "row groups"));
+    EDG_CUDA(cudaMemcpyAsync(B.group_off.p, goff.data(), goff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    EDG_CUDA(cudaMemcpyAsync(B.group_rows.p, grows.data(), grows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+  }
   std::vector<uint32_t> soff(nsl + 1, 0);
   for (int64_t sl = 0; sl < nsl; ++sl) {
     uint32_t w = 0;

@@ -88,6 +88,12 @@ struct SpinBasis {
   bool sell_uniform = true;
   double sell_h = 0.0;
   int max_row = 0;              // longest hop list of any configuration
+  // Down-spin pass work split: rows grouped into `groups` CTAs with near-equal total hop
+  // counts (longest-processing-time-first assignment), CSR: group_off[groups+1], group_rows.
+  DevBuf<uint32_t> group_off;
+  DevBuf<uint32_t> group_rows;
+  int groups = 0;
+  int group_max = 0;            // most rows in one group
 };
 
 // Directed bond list for one spin: Hij(a,b) != 0, a != b, value = matrix element used when

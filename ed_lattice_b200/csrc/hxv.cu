@@ -283,50 +283,65 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
   }
 }
 
-// Down-spin pass, persistent form. Warp w owns the rows idw = w, w+W, w+2W, ... (W = warps
-// in the grid); their hop lists are copied once into shared memory, then all warps sweep the
-// column slabs in lockstep, so at any moment the grid works on about one slab (DimDw rows x
-// 32*VEC columns) that stays in L2 while each of its rows is read once per hop. No global
-// load on the hop list is left in the inner loop, and a warp keeps kU source-row loads in
-// flight.
-constexpr int kDwRowsPerWarp = 8;   // rows a warp can own (grid sized so W*8 >= DimDw)
-constexpr int kDwHops = 32;         // hop-list capacity per owned row held in shared memory
+// Down-spin pass, balanced persistent form. CTA g owns the rows of group g (rows grouped on
+// the host so every group carries the same total number of hops); their hop lists sit in
+// shared memory. All CTAs sweep the column slabs (32*VEC columns) in the same order; inside
+// a CTA the warps take the group's rows from a shared counter, and a CTA barrier closes
+// each slab. Equal work per CTA keeps the whole grid within a few slabs of each other, so
+// the slab being combined (DimDw rows x 32*VEC columns) stays in L2 while each of its rows
+// is read once per hop; no global load of the hop list sits in the inner loop.
+constexpr int kDwHops = 32;  // hop-list capacity per row held in shared memory
 
 template <typename T, int VEC, bool FIRST>
-__global__ void __launch_bounds__(256) k_dw_rows(HxvArgs<T> a, int64_t nslab) {
-  __shared__ uint32_t s_src[8][kDwRowsPerWarp][kDwHops];
-  __shared__ T s_val[8][kDwRowsPerWarp][kDwHops];
-  __shared__ int s_cnt[8][kDwRowsPerWarp];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int64_t W = int64_t(gridDim.x) * (blockDim.x >> 5);
-  const int64_t w = blockIdx.x * int64_t(blockDim.x >> 5) + wib;
-  const int64_t dimup = a.dimup, dimdw = a.dimdw;
-  int nown = 0;
-  for (int q = 0; q < kDwRowsPerWarp; ++q) {
-    const int64_t idw = w + q * W;
-    if (idw >= dimdw) break;
-    const uint32_t k0 = a.off_dw[idw], k1 = a.off_dw[idw + 1];
-    const int cnt = int(k1 - k0);
-    if (lane < cnt && lane < kDwHops) {
-      s_src[wib][q][lane] = a.src_dw[k0 + lane];
-      s_val[wib][q][lane] = a.val_dw[k0 + lane];
+__global__ void __launch_bounds__(256) k_dw_grp(HxvArgs<T> a, const uint32_t* __restrict__ goff,
+                                                const uint32_t* __restrict__ grows, int64_t nslab) {
+  extern __shared__ __align__(16) unsigned char smem_dw[];
+  __shared__ int s_ctr;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t gr0 = goff[blockIdx.x];
+  const int nr = int(goff[blockIdx.x + 1] - gr0);
+  T* s_val = reinterpret_cast<T*>(smem_dw);            // [nr][kDwHops]
+  T* s_edw = s_val + size_t(nr) * kDwHops;              // [nr]
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(s_edw + nr);  // [nr][kDwHops]
+  uint32_t* s_row = s_src + size_t(nr) * kDwHops;       // [nr]
+  uint32_t* s_mdw = s_row + nr;                         // [nr]
+  int* s_cnt = reinterpret_cast<int*>(s_mdw + nr);      // [nr]
+  for (int rr = wib; rr < nr; rr += nw) {
+    const uint32_t row = grows[gr0 + rr];
+    const uint32_t k0 = a.off_dw[row];
+    const int cnt = int(a.off_dw[row + 1] - k0);
+    if (lane < cnt) {
+      s_src[rr * kDwHops + lane] = a.src_dw[k0 + lane];
+      s_val[rr * kDwHops + lane] = a.val_dw[k0 + lane];
     }
-    if (lane == 0) s_cnt[wib][q] = cnt;
-    ++nown;
+    if (lane == 0) {
+      s_row[rr] = row;
+      s_cnt[rr] = cnt;
+      s_edw[rr] = a.e_dw[row];
+      s_mdw[rr] = a.map_dw[row];
+    }
   }
-  __syncwarp();
+  const int64_t dimup = a.dimup;
   for (int64_t slab = 0; slab < nslab; ++slab) {
+    if (threadIdx.x == 0) s_ctr = 0;
+    __syncthreads();
     const int64_t col = slab * (32 * VEC) + int64_t(lane) * VEC;
     const bool active = col < dimup;
-    for (int q = 0; q < nown; ++q) {
-      const int64_t idw = w + q * W;
+    for (;;) {
+      int rr = 0;
+      if (lane == 0) rr = atomicAdd(&s_ctr, 1);
+      rr = __shfl_sync(0xffffffffu, rr, 0);
+      if (rr >= nr) break;
+      const int64_t idw = s_row[rr];
       const int64_t e0 = idw * dimup + col;
-      const int cnt = s_cnt[wib][q];
+      const int cnt = s_cnt[rr];
+      const uint32_t* hs = s_src + rr * kDwHops;
+      const T* hvv = s_val + rr * kDwHops;
       T acc[VEC];
       if (active) {
         if (FIRST) {
-          const T edw = a.e_dw[idw];
-          const uint32_t mdw = a.map_dw[idw];
+          const T edw = s_edw[rr];
+          const uint32_t mdw = s_mdw[rr];
           T x[VEC];
           VecLd<T, VEC>::load(a.v + e0, x);
 #pragma unroll
@@ -343,14 +358,13 @@ __global__ void __launch_bounds__(256) k_dw_rows(HxvArgs<T> a, int64_t nslab) {
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
           const int kk = k + u < cnt ? k + u : k;
-          const uint32_t sr = s_src[wib][q][kk];
-          if (active) VecLd<T, VEC>::load(a.v + int64_t(sr) * dimup + col, x[u]);
+          if (active) VecLd<T, VEC>::load(a.v + int64_t(hs[kk]) * dimup + col, x[u]);
         }
         if (active) {
 #pragma unroll
           for (int u = 0; u < kU; ++u) {
             if (k + u < cnt) {
-              const T h = s_val[wib][q][k + u];
+              const T h = hvv[k + u];
 #pragma unroll
               for (int r = 0; r < VEC; ++r) acc[r] = fmaT<T>(h, x[u][r], acc[r]);
             }
@@ -362,6 +376,7 @@ __global__ void __launch_bounds__(256) k_dw_rows(HxvArgs<T> a, int64_t nslab) {
         for (int r = 0; r < VEC; ++r) __stcs(a.hv + e0 + r, acc[r]);
       }
     }
+    __syncthreads();
   }
 }
 
@@ -513,20 +528,12 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
   const bool v2 = (a.dimup % 2 == 0) && (reinterpret_cast<uintptr_t>(a.v) % (2 * sizeof(T)) == 0) &&
                   (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
   const int vec = v2 ? 2 : 1;
-  if (Bdw.max_row <= kDwHops) {
-    // persistent row-owner kernel: enough warps that each owns at most kDwRowsPerWarp rows
-    // all CTAs resident at once (a second wave would break the lockstep slab sweep)
-    auto kern = v2 ? k_dw_rows<T, 2, FIRST> : k_dw_rows<T, 1, FIRST>;
-    int occ = 0;
-    EDG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0));
-    if (occ < 1) occ = 1;
-    const int64_t need = (a.dimdw + 8 * kDwRowsPerWarp - 1) / (8 * kDwRowsPerWarp);
-    const int64_t per_row = (a.dimdw + 7) / 8;
-    int64_t g = int64_t(sms) * occ;
-    if (g > per_row) g = per_row;
-    if (g < need) g = need;
+  if (Bdw.max_row <= kDwHops && Bdw.groups > 0) {
+    auto kern = v2 ? k_dw_grp<T, 2, FIRST> : k_dw_grp<T, 1, FIRST>;
+    const size_t smem = size_t(Bdw.group_max) * (kDwHops * (sizeof(T) + 4) + sizeof(T) + 12) + 16;
+    if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
-    kern<<<int(g), 256, 0, st>>>(a, nslab);
+    kern<<<Bdw.groups, 256, smem, st>>>(a, Bdw.group_off.p, Bdw.group_rows.p, nslab);
     EDG_CUDA(cudaGetLastError());
     return EDG_OK;
   }
