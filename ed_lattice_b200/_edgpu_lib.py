@@ -62,6 +62,7 @@ SIGNATURES = {
     "edg_hxv_dev_f32": (_i, [_p, _p, _p]),
     "edg_tridiag_d": (_i, [_p, _pd, _i, _d, _i, _pd, _pd, _pd, _pi]),
     "edg_tridiag_dev_f64": (_i, [_p, _p, _i, _d, _i, _pd, _pd, _pd, _pi]),
+    "edg_tridiag_dev_f64_noalloc": (_i, [_p, _p, _i, _d, _pd, _pd, _pd, _pi]),
     "edg_ground_state": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pd, _pi]),
     "edg_ground_state_keep": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pi]),
     "edg_state_get": (_i, [_p, _pd]),
@@ -90,7 +91,7 @@ class EdgError(RuntimeError):
 
 def load(path: str = LIB_PATH) -> C.CDLL:
     if not os.path.exists(path):
-        raise ImportError(f"libedgpu.so not built at {path}; run `python -m ed_lattice_b200.build`")
+        raise ImportError(f"libedgpu.so not built at {path}; run `python ed_lattice_b200/build.py`")
     lib = C.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)

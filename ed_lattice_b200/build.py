@@ -1,6 +1,6 @@
 """Build libedgpu.so (the sm_100a engine) in-tree with nvcc.
 
-Usage: python -m ed_lattice_b200.build [--force]
+Usage: python ed_lattice_b200/build.py [--force]   (by path: the package import needs the library)
 
 The library is written next to this file so that it travels with the source tree;
 ed_lattice_b200/_edgpu_lib.py loads it from there and fails loudly when it is missing.
@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libedgpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["basis.cu", "hxv.cu", "vecops.cu", "lanczos.cu", "excite.cu", "capi.cu", "tridiag_host.cpp"]
+SOURCES = ["basis.cu", "hxv.cu", "vecops.cu", "lanczos.cu", "excite.cu", "capi.cu", "noalloc.cu", "tridiag_host.cpp"]
 HEADERS = ["common.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -120,6 +120,19 @@ int edg_tridiag_d(edg_sector* s, const double* vvinit, int nlanc, double thresho
 int edg_tridiag_dev_f64(edg_sector* s, const double* dvinit, int nlanc, double threshold,
                         int precision, double* alanc, double* blanc, double* norm2, int* nsteps);
 
+/* Allocation-free variant of edg_tridiag_dev_f64 (FP64 only). It has no counterpart in the
+ * reference: it exists for callers that cannot allocate device memory themselves, such as a
+ * host code whose device memory is owned by another runtime's pool or arena, or a loop that
+ * must never wait on the allocator. All scratch (three Lanczos vectors, reduction partials,
+ * scalar slots) lives in one file-scope device array of about 25 MB that every GPU loading
+ * the library holds until exit; the call allocates nothing. Limits: sector dimension <=
+ * 2^20 and nlanc <= 1024, else EDG_ERR_ARG. Calls share that array (it keeps the previous
+ * call's contents; the call clears what must start at zero), so calls that overlap on the
+ * GPU race and must be serialised by the caller. The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) and should come before any stream capture. */
+int edg_tridiag_dev_f64_noalloc(edg_sector* s, const double* dvinit, int nlanc, double threshold,
+                                double* alanc, double* blanc, double* norm2, int* nsteps);
+
 /* Ground state: the contract of sp_lanc_eigh(Hv_p,E,v,Nitermax,threshold) as called from
  * ed_diag_d (src/DIAG/DIAG.f90:212-217). v0: host start vector or NULL for the seeded
  * uniform[-1,1) start vector of edg_random_vector. Stops when the lowest Ritz value changes
