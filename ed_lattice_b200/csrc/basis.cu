@@ -291,6 +291,116 @@ int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   return build_sell(s, B);
 }
 
+// Proper edge colouring of a bipartite multigraph (left: lanes [0,G), right: banks [0,M))
+// with max-degree colours (Konig's theorem), by the classic alternating-path recolouring:
+// for edge (u,v) take colour a free at u and b free at v; if a is taken at v, swap a and b
+// along the a/b path that starts at v (it cannot reach u), after which a is free at both.
+// Returns the number of colours, or -1 when it would exceed kMaxColours.
+static int edge_colour(int G, int M, const std::vector<std::pair<int, int>>& edges, std::vector<int>& colour) {
+  constexpr int kMaxColours = 64;
+  std::vector<int> dl(G, 0), db(M, 0);
+  for (const auto& e : edges) { ++dl[e.first]; ++db[e.second]; }
+  int D = 0;
+  for (int x : dl) D = std::max(D, x);
+  for (int x : db) D = std::max(D, x);
+  if (D > kMaxColours) return -1;
+  if (D == 0) return 0;
+  std::vector<int> lc(size_t(G) * D, -1), bc(size_t(M) * D, -1);
+  colour.assign(edges.size(), -1);
+  std::vector<int> path;
+  for (int e = 0; e < int(edges.size()); ++e) {
+    const int u = edges[e].first, v = edges[e].second;
+    int a = 0, b = 0;
+    while (lc[size_t(u) * D + a] != -1) ++a;
+    while (bc[size_t(v) * D + b] != -1) ++b;
+    if (bc[size_t(v) * D + a] != -1) {
+      path.clear();
+      int x = v, c = a;
+      bool on_bank = true;
+      for (;;) {
+        const int f = on_bank ? bc[size_t(x) * D + c] : lc[size_t(x) * D + c];
+        if (f < 0) break;
+        path.push_back(f);
+        x = on_bank ? edges[f].first : edges[f].second;
+        on_bank = !on_bank;
+        c = (c == a) ? b : a;
+      }
+      for (int f : path) {
+        lc[size_t(edges[f].first) * D + colour[f]] = -1;
+        bc[size_t(edges[f].second) * D + colour[f]] = -1;
+      }
+      for (int f : path) {
+        colour[f] = colour[f] == a ? b : a;
+        lc[size_t(edges[f].first) * D + colour[f]] = f;
+        bc[size_t(edges[f].second) * D + colour[f]] = f;
+      }
+    }
+    colour[e] = a;
+    lc[size_t(u) * D + a] = e;
+    bc[size_t(v) * D + a] = e;
+  }
+  return D;
+}
+
+// Bank-conflict-free slot schedule of a uniform SELL table for the FP32 up pass with `rt`
+// rows per CTA: a shared-memory wavefront serves G = 32/(rt) lanes reading rt*4-byte
+// columns from M = G bank groups (column src sits in group src % M). Per slice and lane
+// group, lanes x groups are edge-coloured; colour = slot. Lanes without an entry in a slot
+// read one of the zero columns DimUp..DimUp+31 whose bank group is free in that slot.
+static void build_schedule(int64_t dim, int rt, const std::vector<uint32_t>& off, const std::vector<uint32_t>& src,
+                           const std::vector<uint32_t>& sgn, std::vector<uint32_t>& soff, std::vector<uint32_t>& ent,
+                           bool* ok) {
+  const int G = 32 / rt, M = G;
+  const int64_t nsl = (dim + 31) / 32;
+  soff.assign(nsl + 1, 0);
+  ent.clear();
+  *ok = true;
+  for (int64_t sl = 0; sl < nsl; ++sl) {
+    int width = 0;
+    std::vector<std::vector<int>> grp_colour(32 / G);
+    std::vector<std::vector<std::pair<int, int>>> grp_edges(32 / G);
+    std::vector<std::vector<int>> grp_eidx(32 / G);
+    for (int g = 0; g < 32 / G; ++g) {
+      auto& E = grp_edges[g];
+      auto& I = grp_eidx[g];
+      for (int l = 0; l < G; ++l) {
+        const int64_t r = sl * 32 + g * G + l;
+        if (r >= dim) continue;
+        for (uint32_t k = off[r]; k < off[r + 1]; ++k) {
+          E.push_back({l, int(src[k] % uint32_t(M))});
+          I.push_back(int(k));
+        }
+      }
+      const int D = edge_colour(G, M, E, grp_colour[g]);
+      if (D < 0) { *ok = false; return; }
+      width = std::max(width, D);
+    }
+    const size_t base = ent.size();
+    soff[sl + 1] = soff[sl] + 32u * uint32_t(width);
+    ent.resize(base + size_t(32) * width, 0u);
+    std::vector<char> used(size_t(width) * M);
+    std::vector<char> filled(size_t(width) * 32);
+    for (int g = 0; g < 32 / G; ++g) {
+      std::fill(used.begin(), used.end(), 0);
+      for (size_t q = 0; q < grp_edges[g].size(); ++q) {
+        const int l = grp_edges[g][q].first, c = grp_colour[g][q], k = grp_eidx[g][q];
+        const int lane = g * G + l;
+        ent[base + size_t(c) * 32 + lane] = src[k] | (sgn[k] << 31);
+        filled[size_t(c) * 32 + lane] = 1;
+        used[size_t(c) * M + grp_edges[g][q].second] = 1;
+      }
+      for (int c = 0; c < width; ++c) {
+        int free_bank = 0;
+        while (free_bank < M && used[size_t(c) * M + free_bank]) ++free_bank;
+        if (free_bank == M) free_bank = 0;  // every lane of the group has an entry: no padding here
+        const uint32_t zcol = uint32_t(dim) + uint32_t((free_bank - int(dim % M) + M) % M);
+        for (int l = 0; l < G; ++l)
+          if (!filled[size_t(c) * 32 + g * G + l]) ent[base + size_t(c) * 32 + g * G + l] = zcol;
+      }
+    }
+  }
+}
+
 // SELL-32 copy of a gather table, built on the host from the device CSR (the tables are
 // O(DimUp) -- about 1 MB for a 4x4 lattice -- so this is a one-off of milliseconds).
 int build_sell(edg_sector_s* s, SpinBasis& B) {
@@ -373,6 +483,26 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
   }
   B.sell_uniform = uniform;
   B.sell_h = hsgn;
+  // FP32 conflict-free schedule (uniform tables whose rows fit the shared-memory up pass)
+  B.sched_rt = 0;
+  B.sched_ent.reset();
+  B.sched_off.reset();
+  const int rt32 = up_rows_per_cta(dim, sizeof(float));
+  if (uniform && rt32 > 0 && B.nnz > 0) {
+    std::vector<uint32_t> sg(B.nnz);
+    for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
+    std::vector<uint32_t> qoff, qent;
+    bool ok = false;
+    build_schedule(dim, rt32, off, src, sg, qoff, qent, &ok);
+    if (ok) {
+      qent.push_back(uint32_t(dim));
+      EDG_CHECK(B.sched_off.alloc(qoff.size(), "SELL schedule"));
+      EDG_CHECK(B.sched_ent.alloc(qent.size(), "SELL schedule"));
+      EDG_CUDA(cudaMemcpyAsync(B.sched_off.p, qoff.data(), qoff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      EDG_CUDA(cudaMemcpyAsync(B.sched_ent.p, qent.data(), qent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      B.sched_rt = rt32;
+    }
+  }
   EDG_CHECK(B.sell_off.alloc(nsl + 1, "SELL offsets"));
   EDG_CHECK(B.sell_ent.alloc(ent.size(), "SELL entries"));
   EDG_CUDA(cudaMemcpyAsync(B.sell_off.p, soff.data(), soff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));

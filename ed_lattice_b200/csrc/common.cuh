@@ -87,6 +87,14 @@ struct SpinBasis {
   DevBuf<float> sell_v32;
   bool sell_uniform = true;
   double sell_h = 0.0;
+  // FP32 copy of the SELL table with each row's entries permuted so that, in every slot, the
+  // lanes served together by one shared-memory wavefront read distinct banks (a bipartite
+  // edge colouring of lanes x banks per lane group). Same rows and values; only the order
+  // of the terms in each row's sum changes, so it is used for FP32 only. Empty when the
+  // colouring would need too many slots.
+  DevBuf<uint32_t> sched_ent;
+  DevBuf<uint32_t> sched_off;
+  int sched_rt = 0;             // rows-per-CTA of the FP32 up pass the schedule was built for
   int max_row = 0;              // longest hop list of any configuration
   // Down-spin pass work split: rows grouped into `groups` CTAs with near-equal total hop
   // counts (longest-processing-time-first assignment), CSR: group_off[groups+1], group_rows.
@@ -139,6 +147,21 @@ struct edg_sector_s {
 };
 
 namespace edg {
+
+// Rows per CTA of the shared-memory up pass for element size `elem` (4 or 8 bytes): the most
+// that fit two CTAs per SM (113 KB each), else one row with one CTA per SM (227 KB), else 0
+// (the row does not fit; the L1-gather kernel takes over). The staged rows carry 32 zero
+// columns after DimUp (padding targets).
+constexpr size_t kUpSmemTwoPerSM = 113 * 1024;
+constexpr size_t kUpSmemOnePerSM = 227 * 1024;
+constexpr int kUpZeroSlots = 32;
+inline int up_rows_per_cta(int64_t dimup, size_t elem) {
+  const size_t row = size_t(dimup + kUpZeroSlots) * elem;
+  if (elem == 4 && 4 * row <= kUpSmemTwoPerSM) return 4;
+  if (2 * row <= kUpSmemTwoPerSM) return 2;
+  if (row <= kUpSmemOnePerSM) return 1;
+  return 0;
+}
 
 // ---- basis.cu
 int sector_build(edg_sector_s* s);

@@ -131,12 +131,12 @@ __global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> s
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
   const int64_t dimup = a.dimup;
-  if (threadIdx.x == 0) {
+  for (int zq = threadIdx.x; zq < kUpZeroSlots; zq += blockDim.x) {  // padding targets
     V z;
     T* zs = reinterpret_cast<T*>(&z);
 #pragma unroll
     for (int r = 0; r < RT; ++r) zs[r] = T(0);
-    S[dimup] = z;
+    S[dimup + zq] = z;
   }
   for (int64_t rb = blockIdx.x; rb < nrowblk; rb += gridDim.x) {
     const int64_t r0 = rb * RT;
@@ -292,8 +292,8 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
 // is read once per hop; no global load of the hop list sits in the inner loop.
 constexpr int kDwHops = 32;  // hop-list capacity per row held in shared memory
 
-template <typename T, int VEC, bool FIRST>
-__global__ void __launch_bounds__(256) k_dw_grp(HxvArgs<T> a, const uint32_t* __restrict__ goff,
+template <typename T, int VEC, int NSEG, int KU, bool FIRST>
+__global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t* __restrict__ goff,
                                                 const uint32_t* __restrict__ grows, int64_t nslab) {
   extern __shared__ __align__(16) unsigned char smem_dw[];
   __shared__ int s_ctr;
@@ -322,59 +322,69 @@ __global__ void __launch_bounds__(256) k_dw_grp(HxvArgs<T> a, const uint32_t* __
     }
   }
   const int64_t dimup = a.dimup;
+  constexpr int SEGW = 32 * VEC;  // columns per warp-wide segment
   for (int64_t slab = 0; slab < nslab; ++slab) {
     if (threadIdx.x == 0) s_ctr = 0;
     __syncthreads();
-    const int64_t col = slab * (32 * VEC) + int64_t(lane) * VEC;
-    const bool active = col < dimup;
+    const int64_t col0 = slab * (SEGW * NSEG) + int64_t(lane) * VEC;
+    bool act[NSEG];
+#pragma unroll
+    for (int g = 0; g < NSEG; ++g) act[g] = col0 + g * SEGW < dimup;
     for (;;) {
       int rr = 0;
       if (lane == 0) rr = atomicAdd(&s_ctr, 1);
       rr = __shfl_sync(0xffffffffu, rr, 0);
       if (rr >= nr) break;
       const int64_t idw = s_row[rr];
-      const int64_t e0 = idw * dimup + col;
+      const T* __restrict__ vrow0 = a.v + col0;   // + src*dimup per hop
+      const int64_t e0 = idw * dimup + col0;
       const int cnt = s_cnt[rr];
       const uint32_t* hs = s_src + rr * kDwHops;
       const T* hvv = s_val + rr * kDwHops;
-      T acc[VEC];
-      if (active) {
+      T acc[NSEG][VEC];
+#pragma unroll
+      for (int g = 0; g < NSEG; ++g) {
+        if (!act[g]) continue;
+        const int64_t c = col0 + g * SEGW;
         if (FIRST) {
           const T edw = s_edw[rr];
           const uint32_t mdw = s_mdw[rr];
           T x[VEC];
-          VecLd<T, VEC>::load(a.v + e0, x);
+          VecLd<T, VEC>::load(a.v + e0 + g * SEGW, x);
 #pragma unroll
           for (int r = 0; r < VEC; ++r)
-            acc[r] = (a.e_up[col + r] + edw + a.U * T(__popc(a.map_up[col + r] & mdw))) * x[r];
+            acc[g][r] = (a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw))) * x[r];
         } else {
 #pragma unroll
-          for (int r = 0; r < VEC; ++r) acc[r] = a.hv[e0 + r];
+          for (int r = 0; r < VEC; ++r) acc[g][r] = a.hv[e0 + g * SEGW + r];
         }
       }
-      constexpr int kU = 8;
-      for (int k = 0; k < cnt; k += kU) {
-        T x[kU][VEC];
+      for (int k = 0; k < cnt; k += KU) {
+        T x[KU][NSEG][VEC];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < KU; ++u) {
           const int kk = k + u < cnt ? k + u : k;
-          if (active) VecLd<T, VEC>::load(a.v + int64_t(hs[kk]) * dimup + col, x[u]);
+          const T* __restrict__ src = vrow0 + int64_t(hs[kk]) * dimup;
+#pragma unroll
+          for (int g = 0; g < NSEG; ++g)
+            if (act[g]) VecLd<T, VEC>::load(src + g * SEGW, x[u][g]);
         }
-        if (active) {
 #pragma unroll
-          for (int u = 0; u < kU; ++u) {
-            if (k + u < cnt) {
-              const T h = hvv[k + u];
+        for (int u = 0; u < KU; ++u) {
+          if (k + u < cnt) {
+            const T h = hvv[k + u];
 #pragma unroll
-              for (int r = 0; r < VEC; ++r) acc[r] = fmaT<T>(h, x[u][r], acc[r]);
-            }
+            for (int g = 0; g < NSEG; ++g)
+              if (act[g]) Fma<T, VEC>::run(h, x[u][g], acc[g]);
           }
         }
       }
-      if (active) {
 #pragma unroll
-        for (int r = 0; r < VEC; ++r) __stcs(a.hv + e0 + r, acc[r]);
-      }
+      for (int g = 0; g < NSEG; ++g)
+        if (act[g]) {
+#pragma unroll
+          for (int r = 0; r < VEC; ++r) __stcs(a.hv + e0 + g * SEGW + r, acc[g][r]);
+        }
     }
     __syncthreads();
   }
@@ -494,31 +504,17 @@ const double* pick_sell<double>(const SpinBasis& B) { return B.sell_v64.p; }
 template <>
 const float* pick_sell<float>(const SpinBasis& B) { return B.sell_v32.p; }
 
-constexpr size_t kSmemTwoPerSM = 113 * 1024;  // two CTAs per SM
-constexpr size_t kSmemOnePerSM = 227 * 1024;  // opt-in maximum per CTA
-
 template <typename T, int RT, bool FIRST, bool UNIFORM>
 int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, int sms) {
-  const size_t smem = size_t(a.dimup + 1) * RT * sizeof(T);
+  const size_t smem = size_t(a.dimup + kUpZeroSlots) * RT * sizeof(T);
   auto kern = k_up_smem<T, RT, FIRST, UNIFORM>;
   if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
-  const int per_sm = smem <= kSmemTwoPerSM ? 2 : 1;
+  const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
   const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
   kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
-}
-
-// Rows per CTA: the most that fit two CTAs per SM, else one row with one CTA per SM;
-// 0 when a row does not fit shared memory at all (the L1-gather kernel takes over).
-template <typename T>
-int rows_per_cta(int64_t dimup) {
-  const size_t row = size_t(dimup + 1) * sizeof(T);
-  if (sizeof(T) == 4 && 4 * row <= kSmemTwoPerSM) return 4;
-  if (2 * row <= kSmemTwoPerSM) return 2;
-  if (row <= kSmemOnePerSM) return 1;
-  return 0;
 }
 
 // VEC-wide loads need every row start aligned: DimUp a multiple of VEC and 2*sizeof(T)
@@ -529,10 +525,13 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
                   (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
   const int vec = v2 ? 2 : 1;
   if (Bdw.max_row <= kDwHops && Bdw.groups > 0) {
-    auto kern = v2 ? k_dw_grp<T, 2, FIRST> : k_dw_grp<T, 1, FIRST>;
+    // FP32: 4 float2 segments per lane (256 columns per slab); FP64: 2 double2 segments
+    constexpr int NSEG = sizeof(T) == 4 ? 4 : 2;
+    constexpr int KU = sizeof(T) == 4 ? 3 : 4;
+    auto kern = v2 ? k_dw_grp<T, 2, NSEG, KU, FIRST> : k_dw_grp<T, 1, NSEG, KU, FIRST>;
     const size_t smem = size_t(Bdw.group_max) * (kDwHops * (sizeof(T) + 4) + sizeof(T) + 12) + 16;
     if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
+    const int64_t nslab = (a.dimup + 32 * vec * NSEG - 1) / (32 * vec * NSEG);
     kern<<<Bdw.groups, 256, smem, st>>>(a, Bdw.group_off.p, Bdw.group_rows.p, nslab);
     EDG_CUDA(cudaGetLastError());
     return EDG_OK;
@@ -549,7 +548,7 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
 
 template <typename T, bool FIRST>
 int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms) {
-  const int rt = rows_per_cta<T>(a.dimup);
+  const int rt = up_rows_per_cta(a.dimup, sizeof(T));
   if (rt == 0) {
     const int g = int(a.dimdw < int64_t(sms) * 8 ? a.dimdw : int64_t(sms) * 8);
     k_up_rows<T, FIRST><<<g, 256, 0, st>>>(a);
@@ -559,6 +558,10 @@ int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms) {
   SellArgs<T> sl;
   sl.ent = B.sell_ent.p;
   sl.off = B.sell_off.p;
+  if (sizeof(T) == 4 && B.sched_rt == rt && B.sched_ent.p) {  // FP32: bank-conflict-free order
+    sl.ent = B.sched_ent.p;
+    sl.off = B.sched_off.p;
+  }
   sl.val = pick_sell<T>(B);
   sl.h = T(B.sell_h);
   if (B.sell_uniform) {
