@@ -189,13 +189,18 @@ def e0_time_to_solution(E, L, sector, seed=2024, maxit=600):
     e_ref, _, it_ref = E.sp_lanc_eigh(sector, seed=seed, maxit=maxit, tol=1e-13, mode=E.EDG_GS_F64,
                                       want_vector=False)
     out["e0_reference_tol1e-13"] = e_ref
+    # untimed warm-up of the FP32 path: allocates the FP32 Lanczos basis once per sector
+    E.sp_lanc_eigh(sector, seed=seed + 1, maxit=maxit, tol=1e-3, mode=E.EDG_GS_F32_REFINE, want_vector=False)
+    n32, n64 = C.c_int(), C.c_int()
     for name, mode in (("fp64", E.EDG_GS_F64), ("fp32_refine", E.EDG_GS_F32_REFINE)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e0, _, it = E.sp_lanc_eigh(sector, seed=seed, maxit=maxit, tol=1e-9, mode=mode, want_vector=False)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        out[name] = {"seconds": dt, "hxv_applications": it, "e0": e0, "rel_err": abs(e0 - e_ref) / abs(e_ref)}
+        L.check(L.lib().edg_ground_state_stats(sector.handle, C.byref(n32), C.byref(n64)), "stats")
+        out[name] = {"seconds": dt, "hxv_applications": it, "hxv_f32": n32.value, "hxv_f64": n64.value, "e0": e0,
+                     "rel_err": abs(e0 - e_ref) / abs(e_ref)}
     out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
     return out
 
@@ -278,9 +283,28 @@ def run_ours(args):
         del zin, zout
 
     extra = {}
-    if rank == 0 and not args.no_e0 and ws == 1:
+    if rank == 0 and ws == 1:
+        # FP64 H x v of the same sector, for the FP32/FP64 ratio behind the E0 comparison
         del v, hv
         torch.cuda.empty_cache()
+        v64 = torch.rand(D, device="cuda", dtype=torch.float64, generator=g) * 2 - 1
+        h64 = torch.empty_like(v64)
+        p64, q64 = C.c_void_p(v64.data_ptr()), C.c_void_p(h64.data_ptr())
+        for _ in range(3):
+            L.check(lib.edg_hxv_dev_f64(sector.handle, p64, q64), "hxv64")
+        k64 = max(5, min(args.steps, 30))
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(k64):
+            L.check(lib.edg_hxv_dev_f64(sector.handle, p64, q64), "hxv64")
+        s1.record()
+        torch.cuda.synchronize()
+        ms64 = s0.elapsed_time(s1) / k64
+        extra["hxv_f64"] = {"ms": ms64, "algorithmic_GBps": 2 * D * 8 / (ms64 * 1e-3) / 1e9,
+                            "f32_speedup": ms64 / avg_launch_ms}
+        del v64, h64
+        torch.cuda.empty_cache()
+    if rank == 0 and not args.no_e0 and ws == 1:
         extra["e0_time_to_1e-8"] = e0_time_to_solution(E, L, sector)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:

@@ -65,6 +65,7 @@ SIGNATURES = {
     "edg_tridiag_dev_f64_noalloc": (_i, [_p, _p, _i, _d, _pd, _pd, _pd, _pi]),
     "edg_ground_state": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pd, _pi]),
     "edg_ground_state_keep": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pi]),
+    "edg_ground_state_stats": (_i, [_p, _pi, _pi]),
     "edg_state_get": (_i, [_p, _pd]),
     "edg_state_set": (_i, [_p, _pd]),
     "edg_random_vector": (_i, [_u64, _i64, _pd]),

@@ -334,6 +334,13 @@ int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, 
   return EDG_OK;
 }
 
+int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64) {
+  EDG_CHECK(check_sector(s));
+  if (n_f32) *n_f32 = s->last_n32;
+  if (n_f64) *n_f64 = s->last_n64;
+  return EDG_OK;
+}
+
 int edg_state_get(const edg_sector* s, double* evec) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(evec, "edg_state_get: NULL");

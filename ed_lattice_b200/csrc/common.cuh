@@ -144,6 +144,7 @@ struct edg_sector_s {
   edg::DevBuf<float> basis32;     // FP32 Lanczos basis for Ritz vectors
   size_t basis32_cols = 0;
   bool has_state = false;
+  int last_n32 = 0, last_n64 = 0;  // H x v applications of the last ground-state run per precision
 };
 
 namespace edg {
@@ -189,6 +190,7 @@ int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale
 template <typename TD>
 int axpy_accum_dev(cudaStream_t st, double* dst, const TD* x, double coef, int64_t n);
 int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed);
+int ritz_dev(cudaStream_t st, const float* basis, const double* z_dev, int m, int64_t n, double* x);
 uint64_t splitmix64(uint64_t x);
 
 // ---- lanczos.cu

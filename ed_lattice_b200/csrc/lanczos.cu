@@ -11,6 +11,7 @@
 // The sector's work buffers hold v_j, v_{j-1}, w; scalars a_j, b_{j+1} are written by the
 // reduction kernels into device arrays and copied to the host once per step (16 bytes)
 // for the convergence test.
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -171,7 +172,12 @@ int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A
   EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), w.data(), nullptr, Z.data()));
   EDG_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
   if (basis && basis_cols >= m) {
-    for (int j = 0; j < m; ++j) EDG_CHECK(axpy_accum_dev<float>(st, x, basis + size_t(j) * n, Z[j], n));
+    // one pass over the stored columns (same FMA order as m successive axpys)
+    Scalars scz;
+    EDG_CHECK(scalars(s, m + 1, &scz));
+    EDG_CUDA(cudaMemcpyAsync(scz.a, Z.data(), size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st));
+    EDG_CHECK(ritz_dev(st, basis, scz.a, m, n, x));
+    EDG_CUDA(cudaStreamSynchronize(st));  // Z (host) must outlive the copy
   } else {
     Scalars sc;
     EDG_CHECK(scalars(s, m + 1, &sc));
@@ -246,46 +252,54 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
   EDG_CHECK(normalise(s, x0));
   std::vector<double> A, B;
   *niter = 0;
+  s->last_n32 = s->last_n64 = 0;
   s->has_state = false;
   const bool want_vec = !(mode & EDG_GS_E0_ONLY);
   mode &= 0xff;
   if (mode == EDG_GS_F64) {
     EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, e0));
-    *niter += int(A.size());
+    s->last_n64 += int(A.size());
     if (want_vec) {
       EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, s->state.p));
-      *niter += int(A.size()) - 1;
+      s->last_n64 += int(A.size()) - 1;
     }
   } else {
-    // phase 1: FP32 vectors; keep as many basis vectors as HBM admits (2 vectors of slack)
-    size_t freeb = 0, totb = 0;
-    EDG_CUDA(cudaMemGetInfo(&freeb, &totb));
-    const size_t vecb = size_t(n) * sizeof(float);
-    const size_t slack = (size_t(3) << 30) + 6 * vecb;
-    int cols = 0;
-    if (freeb > slack) cols = int(std::min<size_t>((freeb - slack) / 2 / vecb, size_t(maxit)));
-    if (s->basis32_cols < size_t(cols)) {
-      s->basis32.reset();
-      if (cols > 0 && s->basis32.alloc(size_t(cols) * n, "FP32 Lanczos basis") != EDG_OK) cols = 0;
-      s->basis32_cols = cols > 0 ? cols : 0;
-    } else {
-      cols = int(s->basis32_cols);
+    // phase 1: FP32 vectors. The basis is kept for the Ritz vector (no second pass) when
+    // HBM admits it: at most half the free memory, kMaxBasisCols columns, allocated once
+    // per sector and reused by later calls.
+    constexpr int kMaxBasisCols = 512;
+    const int want_cols = std::min(maxit, kMaxBasisCols);
+    if (s->basis32_cols < size_t(want_cols)) {
+      size_t freeb = 0, totb = 0;
+      EDG_CUDA(cudaMemGetInfo(&freeb, &totb));
+      const size_t vecb = size_t(n) * sizeof(float);
+      const size_t slack = (size_t(3) << 30) + 6 * vecb;
+      int cols = 0;
+      if (freeb > slack) cols = int(std::min<size_t>((freeb - slack) / 2 / vecb, size_t(want_cols)));
+      if (size_t(cols) > s->basis32_cols) {
+        s->basis32.reset();
+        s->basis32_cols = 0;
+        if (cols > 0 && s->basis32.alloc(size_t(cols) * n, "FP32 Lanczos basis") == EDG_OK) s->basis32_cols = cols;
+      }
     }
+    const int cols = int(s->basis32_cols);
+    // FP32 phase: stop once the lowest Ritz value settles at FP32 resolution
     const double tol32 = tol > 2e-7 ? tol : 2e-7;
     double e32 = 0.0;
     EDG_CHECK(gs_run<float>(s, x0, maxit, tol32, &A, &B, s->basis32.p, cols, &e32));
-    *niter += int(A.size());
+    s->last_n32 += int(A.size());
     EDG_CHECK(ritz_vector<float>(s, x0, A, B, s->basis32.p, cols, s->state.p));
-    if (cols < int(A.size())) *niter += int(A.size()) - 1;
+    if (cols < int(A.size())) s->last_n32 += int(A.size()) - 1;
     // phase 2: restarted FP64 Lanczos from the FP32 Ritz vector
     EDG_CUDA(cudaMemcpyAsync(x0, s->state.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, e0));
-    *niter += int(A.size());
+    s->last_n64 += int(A.size());
     if (want_vec) {
       EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, s->state.p));
-      *niter += int(A.size()) - 1;
+      s->last_n64 += int(A.size()) - 1;
     }
   }
+  *niter = s->last_n32 + s->last_n64;
   EDG_CUDA(cudaStreamSynchronize(st));
   s->has_state = want_vec;
   return EDG_OK;

@@ -98,6 +98,20 @@ __global__ void k_axpy_accum(double* __restrict__ dst, const TS* __restrict__ x,
     dst[i] = __fma_rn(coef, double(x[i]), dst[i]);
 }
 
+// x[i] = sum_j z[j] * basis[j][i] in one pass over the stored FP32 Lanczos basis (z in FP64,
+// j ascending: the same FMA sequence as m successive axpys, one read of each column).
+__global__ void __launch_bounds__(256) k_ritz(const float* __restrict__ basis, const double* __restrict__ z, int m,
+                                              int64_t n, double* __restrict__ x) {
+  extern __shared__ double s_z[];
+  for (int j = threadIdx.x; j < m; j += blockDim.x) s_z[j] = z[j];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double acc = 0.0;
+    for (int j = 0; j < m; ++j) acc = __fma_rn(s_z[j], double(__ldcs(basis + int64_t(j) * n + i)), acc);
+    x[i] = acc;
+  }
+}
+
 __device__ __host__ __forceinline__ uint64_t splitmix64_d(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -163,6 +177,17 @@ int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale
 template <typename TS>
 int axpy_accum_dev(cudaStream_t st, double* dst, const TS* x, double coef, int64_t n) {
   k_axpy_accum<TS><<<grid_for(n), 256, 0, st>>>(dst, x, coef, n);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+int ritz_dev(cudaStream_t st, const float* basis, const double* z_dev, int m, int64_t n, double* x) {
+  const size_t smem = size_t(m) * sizeof(double);
+  if (smem > 48 * 1024) {
+    set_error("ritz_dev: %d basis columns exceed the shared-memory coefficient cache", m);
+    return EDG_ERR_ARG;
+  }
+  k_ritz<<<grid_for(n), 256, smem, st>>>(basis, z_dev, m, n, x);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }

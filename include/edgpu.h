@@ -145,6 +145,9 @@ int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, 
  * with edg_state_get or use in the excitation builders below. */
 int edg_ground_state_keep(edg_sector* s, const double* v0, uint64_t seed, int maxit, double tol,
                           int mode, double* e0, int* niter);
+/* H x v applications of the last ground-state run, split by vector precision (FP32 phase,
+ * FP64 phase). No counterpart in the reference (sp_lanc_eigh reports no statistics). */
+int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64);
 int edg_state_get(const edg_sector* s, double* evec);
 int edg_state_set(edg_sector* s, const double* evec);
 

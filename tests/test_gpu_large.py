@@ -13,16 +13,25 @@ from ed_lattice_b200 import _edgpu_lib as L
 pytestmark = pytest.mark.gpu
 
 
+def on_torch_stream(s):
+    """The _dev entry points are ordered on the sector's stream; put it on torch's stream
+    so the kernels see tensors torch has just written."""
+    import torch
+    L.check(L.lib().edg_sector_set_stream(s.handle, C.c_void_p(torch.cuda.current_stream().cuda_stream)), "stream")
+    return s
+
+
 @pytest.fixture(scope="module")
 def sector():
     model = E.Model(E.square_lattice(4, 4), uloc=8.0, xmu=4.0, hfmode=False)
-    s = E.Sector(model, 8, 8)
+    s = on_torch_stream(E.Sector(model, 8, 8))
     yield s
     s.delete()
 
 
 def hxv(s, x):
     import torch
+    torch.cuda.synchronize()
     y = torch.empty_like(x)
     fn = L.lib().edg_hxv_dev_f64 if x.dtype == torch.float64 else L.lib().edg_hxv_dev_f32
     L.check(fn(s.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "hxv")
@@ -53,7 +62,7 @@ def test_large_f32_matches_f64(sector):
 def test_large_stored_vs_direct(sector):
     import torch
     model = E.Model(E.square_lattice(4, 4), uloc=8.0, xmu=4.0, hfmode=False)
-    sd = E.Sector(model, 8, 8, E.EDG_FORM_DIRECT)
+    sd = on_torch_stream(E.Sector(model, 8, 8, E.EDG_FORM_DIRECT))
     g = torch.Generator(device="cuda").manual_seed(4)
     x = torch.rand(sector.dim, device="cuda", dtype=torch.float64, generator=g) * 2 - 1
     ys = hxv(sector, x)
