@@ -200,6 +200,8 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
                  double* e0, int* niter);
 
 // ---- tridiag_host.cpp
-int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull);
+// zn (optional): last components of the eigenvectors (Ritz residual estimates b*|zn|).
+int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull,
+                      double* zn = nullptr);
 
 }  // namespace edg

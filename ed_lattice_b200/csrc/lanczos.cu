@@ -109,11 +109,22 @@ int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, d
   return EDG_OK;
 }
 
-double lowest_ritz(const std::vector<double>& a, const std::vector<double>& b) {
+// Lowest Ritz value of T(a, b) and the a-posteriori estimate of its error,
+// (b_next * |z_m|)^2 / gap: b_next*|z_m| is the residual norm of the Ritz pair and
+// theta_1 - E_0 <= r^2 / gap for the lowest eigenvalue (gap from the second Ritz value).
+struct Ritz {
+  double e0, err;
+};
+Ritz lowest_ritz(const std::vector<double>& a, const std::vector<double>& b, double b_next) {
   const int m = int(a.size());
-  std::vector<double> w(m);
-  tridiag_eigh_host(m, a.data(), b.data(), w.data(), nullptr, nullptr);
-  return w[0];
+  std::vector<double> w(m), zl(m);
+  tridiag_eigh_host(m, a.data(), b.data(), w.data(), nullptr, nullptr, zl.data());
+  Ritz r;
+  r.e0 = w[0];
+  const double res = b_next * std::fabs(zl[0]);
+  const double gap = m > 1 ? w[1] - w[0] : 0.0;
+  r.err = gap > 1e-12 ? res * res / gap : res;
+  return r;
 }
 
 // Plain Lanczos in precision T from the normalised FP64 device vector dv0 until the lowest
@@ -146,8 +157,12 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
       return EDG_ERR_NOCONV;
     }
     A->push_back(a);
-    const double e = lowest_ritz(*A, *B);
-    const bool conv = (j > 0 && std::fabs(e - eold) <= tol * std::fabs(e)) || b < 1e-14;
+    const Ritz rz = lowest_ritz(*A, *B, b);
+    const double e = rz.e0;
+    // converged when the error estimate is 10x below tol*|E0| (or, as a fallback for a
+    // degenerate lowest level, when E0 stops moving), or the Krylov space is exhausted
+    const bool conv = (j > 0 && rz.err <= 0.1 * tol * std::fabs(e)) ||
+                      (j > 0 && std::fabs(e - eold) <= 0.01 * tol * std::fabs(e)) || b < 1e-14;
     eold = e;
     B->push_back(b);
     *e0 = e;

@@ -20,18 +20,19 @@ namespace edg {
 // d[n] diagonal, e[n] couplings with e[k] between k-1 and k (e[0] ignored).
 // w[n] eigenvalues ascending; z1[n] (optional) first components; zfull[n*n] (optional)
 // column-major eigenvectors, column j for w[j].
-int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull) {
+int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull, double* zn) {
   if (n <= 0) return EDG_OK;
   std::vector<double> dd(d, d + n), sub(n, 0.0);
   for (int i = 0; i + 1 < n; ++i) sub[i] = e[i + 1];
   const bool full = zfull != nullptr;
   std::vector<double> Z;
-  std::vector<double> row0(n, 0.0);
+  std::vector<double> row0(n, 0.0), rowl(n, 0.0);  // first and last rows of Z
   if (full) {
     Z.assign(size_t(n) * n, 0.0);
     for (int i = 0; i < n; ++i) Z[i + size_t(i) * n] = 1.0;
   } else {
     row0[0] = 1.0;
+    rowl[n - 1] = 1.0;
   }
   const double eps = std::numeric_limits<double>::epsilon();
   for (int l = 0; l < n; ++l) {
@@ -81,6 +82,11 @@ int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double
           const double t = row0[i + 1];
           row0[i + 1] = s * row0[i] + c * t;
           row0[i] = c * row0[i] - s * t;
+          if (zn) {
+            const double tl = rowl[i + 1];
+            rowl[i + 1] = s * rowl[i] + c * tl;
+            rowl[i] = c * rowl[i] - s * tl;
+          }
         }
       }
       if (deflated) continue;
@@ -95,6 +101,7 @@ int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double
   for (int j = 0; j < n; ++j) {
     w[j] = dd[idx[j]];
     if (z1) z1[j] = full ? Z[0 + size_t(idx[j]) * n] : row0[idx[j]];
+    if (zn) zn[j] = full ? Z[size_t(n - 1) + size_t(idx[j]) * n] : rowl[idx[j]];
     if (full)
       for (int k = 0; k < n; ++k) zfull[k + size_t(j) * n] = Z[k + size_t(idx[j]) * n];
   }

@@ -135,10 +135,12 @@ int edg_tridiag_dev_f64_noalloc(edg_sector* s, const double* dvinit, int nlanc, 
 
 /* Ground state: the contract of sp_lanc_eigh(Hv_p,E,v,Nitermax,threshold) as called from
  * ed_diag_d (src/DIAG/DIAG.f90:212-217). v0: host start vector or NULL for the seeded
- * uniform[-1,1) start vector of edg_random_vector. Stops when the lowest Ritz value changes
- * by <= tol*|E0| between steps (or b underflows, or maxit). mode: EDG_GS_F64 or
- * EDG_GS_F32_REFINE. evec (host, may be NULL) receives the normalised eigenvector.
- * *niter = total H x v applications. */
+ * uniform[-1,1) start vector of edg_random_vector. Stops when the a-posteriori error of the
+ * lowest Ritz value, (b_{m+1} |z_m|)^2 / gap, falls below 0.1*tol*|E0| (fallbacks: E0
+ * moves by less than 0.01*tol*|E0| in a step, b underflows, or maxit). mode: EDG_GS_F64
+ * or EDG_GS_F32_REFINE (FP32 phase to max(tol, 2e-7), then FP64 from its Ritz vector).
+ * evec (host, may be NULL) receives the normalised eigenvector. *niter = total H x v
+ * applications. */
 int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, double tol, int mode,
                      double* e0, double* evec, int* niter);
 /* Device variant: the eigenvector stays on the device in the sector's state buffer; copy
