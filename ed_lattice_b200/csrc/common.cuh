@@ -171,6 +171,10 @@ uint64_t binom_host(int n, int k);
 // ---- hxv.cu
 template <typename T>
 int hxv_apply(edg_sector_s* s, const T* v, T* hv);
+template <typename T>
+int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double* bn, int j, double* partial,
+                 int* nblocks);
+bool hxv_lz_available(const edg_sector_s* s, size_t elem);
 
 // ---- vecops.cu
 constexpr int kRedBlocks = 592;  // 148 SMs x 4: fixed reduction grid (deterministic sums)
@@ -185,6 +189,10 @@ int lanczos_step_b(cudaStream_t st, T* w, const T* v, const double* a, int64_t n
                    double* bout);
 template <typename T>
 int scale_into(cudaStream_t st, T* dst, const T* src, const double* b, int64_t n);
+template <typename T>
+int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
+                    double* bn_next);
+int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, int do_sqrt);
 template <typename TD, typename TS>
 int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale);
 template <typename TD>

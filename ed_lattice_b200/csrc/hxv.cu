@@ -32,6 +32,12 @@ struct HxvArgs {
   const uint32_t* __restrict__ map_up;
   const uint32_t* __restrict__ map_dw;
   T U;
+  // Lanczos-fused mode (v = u / bn[jstep] is applied with the scale folded into the matrix
+  // elements; the up pass then forms w = Hv - (bn[j]/bn[j-1]) uprev and partial <v, w>)
+  const double* __restrict__ bn = nullptr;
+  int jstep = 0;
+  const T* __restrict__ uprev = nullptr;
+  double* __restrict__ partial = nullptr;
 };
 
 template <typename T>
@@ -125,12 +131,18 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 
 // SELL entry: bit 31 = sign of the uniform value, bits 0..30 = source column (DimUp for
 // padding: a zero slot after the staged rows, so padding needs no branch).
-template <typename T, int RT, bool FIRST, bool UNIFORM>
+template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ>
 __global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
   const int64_t dimup = a.dimup;
+  double sc = 1.0, cc = 0.0, pa = 0.0;
+  if (LZ) {
+    sc = 1.0 / a.bn[a.jstep];
+    cc = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+  }
+  const T hs = LZ ? T(double(sl.h) * sc) : sl.h;
   for (int zq = threadIdx.x; zq < kUpZeroSlots; zq += blockDim.x) {  // padding targets
     V z;
     T* zs = reinterpret_cast<T*>(&z);
@@ -181,16 +193,41 @@ __global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> s
         }
 #pragma unroll
         for (int u = 0; u < kUpBatch; ++u) {
-          const T h = UNIFORM ? flip_sign(sl.h, e[u]) : hv_[u];
+          const T h = UNIFORM ? flip_sign(hs, e[u]) : (LZ ? T(double(hv_[u]) * sc) : hv_[u]);
           const V x = S[e[u] & 0x7fffffffu];
           Fma<T, RT>::run(h, reinterpret_cast<const T*>(&x), acc);
         }
       }
+      if (LZ) {
+        // w = Hv - c * uprev ;  partial <v, w> with v = sc * u (staged in S)
+        const V xc = S[iup];
+        const T* xs = reinterpret_cast<const T*>(&xc);
 #pragma unroll
-      for (int r = 0; r < RT; ++r)
-        if (r0 + r < a.dimdw) __stcs(a.hv + (r0 + r) * dimup + iup, acc[r]);
+        for (int r = 0; r < RT; ++r)
+          if (r0 + r < a.dimdw) {
+            const int64_t e = (r0 + r) * dimup + iup;
+            const T wt = T(double(acc[r]) - cc * double(a.uprev[e]));
+            pa = __fma_rn(double(xs[r]) * sc, double(wt), pa);
+            __stcs(a.hv + e, wt);
+          }
+      } else {
+#pragma unroll
+        for (int r = 0; r < RT; ++r)
+          if (r0 + r < a.dimdw) __stcs(a.hv + (r0 + r) * dimup + iup, acc[r]);
+      }
     }
     __syncthreads();
+  }
+  if (LZ) {  // block partial of <v, w>, fixed order
+    __shared__ double s_red[32];
+    for (int o = 16; o > 0; o >>= 1) pa += __shfl_down_sync(0xffffffffu, pa, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = pa;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q = 0; q < int(blockDim.x >> 5); ++q) t += s_red[q];
+      a.partial[blockIdx.x] = t;
+    }
   }
 }
 
@@ -292,10 +329,11 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
 // is read once per hop; no global load of the hop list sits in the inner loop.
 constexpr int kDwHops = 32;  // hop-list capacity per row held in shared memory
 
-template <typename T, int VEC, int NSEG, int KU, bool FIRST>
+template <typename T, int VEC, int NSEG, int KU, bool FIRST, bool SCALED>
 __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t* __restrict__ goff,
                                                 const uint32_t* __restrict__ grows, int64_t nslab) {
   extern __shared__ __align__(16) unsigned char smem_dw[];
+  const double sc = SCALED ? 1.0 / a.bn[a.jstep] : 1.0;
   __shared__ int s_ctr;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t gr0 = goff[blockIdx.x];
@@ -312,7 +350,7 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
     const int cnt = int(a.off_dw[row + 1] - k0);
     if (lane < cnt) {
       s_src[rr * kDwHops + lane] = a.src_dw[k0 + lane];
-      s_val[rr * kDwHops + lane] = a.val_dw[k0 + lane];
+      s_val[rr * kDwHops + lane] = SCALED ? T(double(a.val_dw[k0 + lane]) * sc) : a.val_dw[k0 + lane];
     }
     if (lane == 0) {
       s_row[rr] = row;
@@ -352,8 +390,10 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
           T x[VEC];
           VecLd<T, VEC>::load(a.v + e0 + g * SEGW, x);
 #pragma unroll
-          for (int r = 0; r < VEC; ++r)
-            acc[g][r] = (a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw))) * x[r];
+          for (int r = 0; r < VEC; ++r) {
+            const T d = a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw));
+            acc[g][r] = (SCALED ? T(double(d) * sc) : d) * x[r];
+          }
         } else {
 #pragma unroll
           for (int r = 0; r < VEC; ++r) acc[g][r] = a.hv[e0 + g * SEGW + r];
@@ -504,22 +544,24 @@ const double* pick_sell<double>(const SpinBasis& B) { return B.sell_v64.p; }
 template <>
 const float* pick_sell<float>(const SpinBasis& B) { return B.sell_v32.p; }
 
-template <typename T, int RT, bool FIRST, bool UNIFORM>
-int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, int sms) {
+template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ>
+int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, int sms, int* grid) {
   const size_t smem = size_t(a.dimup + kUpZeroSlots) * RT * sizeof(T);
-  auto kern = k_up_smem<T, RT, FIRST, UNIFORM>;
+  auto kern = k_up_smem<T, RT, FIRST, UNIFORM, LZ>;
   if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
   const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
   kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
+  if (grid) *grid = int(g);
   return EDG_OK;
 }
 
 // VEC-wide loads need every row start aligned: DimUp a multiple of VEC and 2*sizeof(T)
 // aligned vector pointers (always true for our own buffers; checked for callers' pointers).
-template <typename T, bool FIRST>
+// SCALED (Lanczos-fused mode) applies H to v = u / bn[jstep] by scaling the matrix elements.
+template <typename T, bool FIRST, bool SCALED>
 int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms) {
   const bool v2 = (a.dimup % 2 == 0) && (reinterpret_cast<uintptr_t>(a.v) % (2 * sizeof(T)) == 0) &&
                   (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
@@ -528,13 +570,17 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
     // FP32: 4 float2 segments per lane (256 columns per slab); FP64: 2 double2 segments
     constexpr int NSEG = sizeof(T) == 4 ? 4 : 2;
     constexpr int KU = sizeof(T) == 4 ? 3 : 4;
-    auto kern = v2 ? k_dw_grp<T, 2, NSEG, KU, FIRST> : k_dw_grp<T, 1, NSEG, KU, FIRST>;
+    auto kern = v2 ? k_dw_grp<T, 2, NSEG, KU, FIRST, SCALED> : k_dw_grp<T, 1, NSEG, KU, FIRST, SCALED>;
     const size_t smem = size_t(Bdw.group_max) * (kDwHops * (sizeof(T) + 4) + sizeof(T) + 12) + 16;
     if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int64_t nslab = (a.dimup + 32 * vec * NSEG - 1) / (32 * vec * NSEG);
     kern<<<Bdw.groups, 256, smem, st>>>(a, Bdw.group_off.p, Bdw.group_rows.p, nslab);
     EDG_CUDA(cudaGetLastError());
     return EDG_OK;
+  }
+  if (SCALED) {
+    set_error("fused Lanczos H x v needs the grouped down pass");
+    return EDG_ERR_UNSUPPORTED;
   }
   const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
   const int64_t ntiles = nslab * a.dimdw;
@@ -546,10 +592,14 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
   return EDG_OK;
 }
 
-template <typename T, bool FIRST>
-int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms) {
+template <typename T, bool FIRST, bool LZ>
+int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms, int* grid) {
   const int rt = up_rows_per_cta(a.dimup, sizeof(T));
   if (rt == 0) {
+    if (LZ) {
+      set_error("fused Lanczos H x v needs the shared-memory up pass");
+      return EDG_ERR_UNSUPPORTED;
+    }
     const int g = int(a.dimdw < int64_t(sms) * 8 ? a.dimdw : int64_t(sms) * 8);
     k_up_rows<T, FIRST><<<g, 256, 0, st>>>(a);
     EDG_CUDA(cudaGetLastError());
@@ -564,20 +614,19 @@ int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms) {
   }
   sl.val = pick_sell<T>(B);
   sl.h = T(B.sell_h);
+  constexpr int R4 = sizeof(T) == 4 ? 4 : 2;
   if (B.sell_uniform) {
-    if (rt == 4) return launch_up_smem<T, (sizeof(T) == 4 ? 4 : 2), FIRST, true>(a, sl, st, sms);
-    if (rt == 2) return launch_up_smem<T, 2, FIRST, true>(a, sl, st, sms);
-    return launch_up_smem<T, 1, FIRST, true>(a, sl, st, sms);
+    if (rt == 4) return launch_up_smem<T, R4, FIRST, true, LZ>(a, sl, st, sms, grid);
+    if (rt == 2) return launch_up_smem<T, 2, FIRST, true, LZ>(a, sl, st, sms, grid);
+    return launch_up_smem<T, 1, FIRST, true, LZ>(a, sl, st, sms, grid);
   }
-  if (rt == 4) return launch_up_smem<T, (sizeof(T) == 4 ? 4 : 2), FIRST, false>(a, sl, st, sms);
-  if (rt == 2) return launch_up_smem<T, 2, FIRST, false>(a, sl, st, sms);
-  return launch_up_smem<T, 1, FIRST, false>(a, sl, st, sms);
+  if (rt == 4) return launch_up_smem<T, R4, FIRST, false, LZ>(a, sl, st, sms, grid);
+  if (rt == 2) return launch_up_smem<T, 2, FIRST, false, LZ>(a, sl, st, sms, grid);
+  return launch_up_smem<T, 1, FIRST, false, LZ>(a, sl, st, sms, grid);
 }
 
-}  // namespace
-
 template <typename T>
-int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
+HxvArgs<T> make_args(edg_sector_s* s, const T* v, T* hv) {
   HxvArgs<T> a;
   a.v = v;
   a.hv = hv;
@@ -594,11 +643,19 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
   a.map_up = s->up.map.p;
   a.map_dw = s->dw.map.p;
   a.U = T(s->U);
+  return a;
+}
+
+}  // namespace
+
+template <typename T>
+int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
+  HxvArgs<T> a = make_args<T>(s, v, hv);
   const int sms = sm_count();
   cudaStream_t st = s->stream;
   if (s->form == EDG_FORM_STORED) {
-    EDG_CHECK((dw_pass<T, true>(a, s->dw, st, sms)));
-    EDG_CHECK((up_pass<T, false>(a, s->up, st, sms)));
+    EDG_CHECK((dw_pass<T, true, false>(a, s->dw, st, sms)));
+    EDG_CHECK((up_pass<T, false, false>(a, s->up, st, sms, nullptr)));
   } else {
     DirectArgsHdr d;
     d.nb_up = s->bonds[0].nb;
@@ -620,5 +677,34 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
 
 template int hxv_apply<float>(edg_sector_s*, const float*, float*);
 template int hxv_apply<double>(edg_sector_s*, const double*, double*);
+
+// Lanczos-fused H x v (stored form): with v = u / bn[j], writes w = H v - (bn[j]/bn[j-1]) uprev
+// into `w` and per-block partials of <v, w> into `partial` (*nblocks of them). Returns
+// EDG_ERR_UNSUPPORTED when the sector needs one of the general kernels instead.
+template <typename T>
+int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double* bn, int j, double* partial,
+                 int* nblocks) {
+  if (s->form != EDG_FORM_STORED || up_rows_per_cta(s->up.dim, sizeof(T)) == 0 || s->dw.max_row > kDwHops ||
+      s->dw.groups == 0) {
+    set_error("fused Lanczos H x v not available for this sector");
+    return EDG_ERR_UNSUPPORTED;
+  }
+  HxvArgs<T> a = make_args<T>(s, u, w);
+  a.bn = bn;
+  a.jstep = j;
+  a.uprev = uprev;
+  a.partial = partial;
+  const int sms = sm_count();
+  EDG_CHECK((dw_pass<T, true, true>(a, s->dw, s->stream, sms)));
+  EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nblocks)));
+  return EDG_OK;
+}
+bool hxv_lz_available(const edg_sector_s* s, size_t elem) {
+  return s->form == EDG_FORM_STORED && up_rows_per_cta(s->up.dim, elem) > 0 && s->dw.max_row <= kDwHops &&
+         s->dw.groups > 0;
+}
+template int hxv_apply_lz<float>(edg_sector_s*, const float*, const float*, float*, const double*, int, double*, int*);
+template int hxv_apply_lz<double>(edg_sector_s*, const double*, const double*, double*, const double*, int, double*,
+                                  int*);
 
 }  // namespace edg

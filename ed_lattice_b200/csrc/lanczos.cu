@@ -8,9 +8,16 @@
 //   EDG_GS_F32_REFINE FP32 vectors with FP64 scalars until the lowest Ritz value settles at
 //                     FP32 resolution, FP32 Ritz vector accumulated in FP64 from the stored
 //                     FP32 basis, then restarted FP64 Lanczos from it to the requested tol.
-// The sector's work buffers hold v_j, v_{j-1}, w; scalars a_j, b_{j+1} are written by the
-// reduction kernels into device arrays and copied to the host once per step (16 bytes)
-// for the convergence test.
+//
+// The recurrence (w = H v_j - b_j v_{j-1}; a_j = <v_j|w>; u_{j+1} = w - a_j v_j;
+// b_{j+1} = |u_{j+1}|) runs in one of two forms with identical mathematics:
+//  * fused (stored-form sectors whose passes take the shared-memory/grouped kernels): the
+//    vectors are kept unnormalised, u_j = b_j v_j, the scale 1/b_j is folded into the matrix
+//    elements of the H x v, whose second pass also forms w and the partial <v_j|w>; one more
+//    pass forms u_{j+1} and its norm. About 9 vector-lengths of traffic per step.
+//  * general: H x v, then w/a, u/b and v_{j+1} = u/b as three passes (14 vector-lengths).
+// Scalars a_j, b_{j+1} are written by the reduction kernels into device arrays and copied to
+// the host once per step (16 bytes) for the convergence test.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -22,19 +29,26 @@ namespace {
 
 struct Scalars {
   double* partial;  // [kRedBlocks]
-  double* a;        // [cap]
-  double* b;        // [cap+1], b[0] = 0
+  double* a;        // [cap+2]
+  double* b;        // [cap+2], b[0] = 0 (Lanczos b's)
+  double* bn;       // [cap+2], norms of the unnormalised vectors, bn[0] = 1 (fused form)
+  double* tmp;      // [8]
   int cap;
 };
 
 int scalars(edg_sector_s* s, int cap, Scalars* sc) {
-  const size_t need = size_t(kRedBlocks) + 2 * size_t(cap) + 8;
+  const size_t need = size_t(kRedBlocks) + 3 * size_t(cap + 2) + 8;
   EDG_CHECK(s->red.alloc(need, "reduction scratch"));
   sc->partial = s->red.p;
-  sc->a = s->red.p + kRedBlocks;
-  sc->b = sc->a + cap + 1;
+  sc->a = sc->partial + kRedBlocks;
+  sc->b = sc->a + cap + 2;
+  sc->bn = sc->b + cap + 2;
+  sc->tmp = sc->bn + cap + 2;
   sc->cap = cap;
   EDG_CUDA(cudaMemsetAsync(s->red.p, 0, need * sizeof(double), s->stream));
+  const double one = 1.0;
+  EDG_CUDA(cudaMemcpyAsync(sc->bn, &one, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EDG_CUDA(cudaStreamSynchronize(s->stream));  // `one` is a stack value
   return EDG_OK;
 }
 
@@ -45,25 +59,74 @@ DevBuf<double>* work<double>(edg_sector_s* s) { return s->w64; }
 template <>
 DevBuf<float>* work<float>(edg_sector_s* s) { return s->w32; }
 
-// One recurrence step j on (V=v_j, P=v_{j-1}, W): W = H V; a_j; b_{j+1}.
+// The Lanczos recurrence in precision T over the sector's three work vectors.
 template <typename T>
-int step(edg_sector_s* s, const Scalars& sc, int j, const T* V, const T* P, T* W) {
-  const int64_t n = s->dim;
-  EDG_CHECK(hxv_apply<T>(s, V, W));
-  EDG_CHECK(lanczos_step_a<T>(s->stream, W, P, V, sc.b + j, n, sc.partial, sc.a + j));
-  EDG_CHECK(lanczos_step_b<T>(s->stream, W, V, sc.a + j, n, sc.partial, sc.b + j + 1));
-  return EDG_OK;
-}
+struct Recurrence {
+  edg_sector_s* s = nullptr;
+  Scalars sc{};
+  T* U = nullptr;  // current vector: v_j (general) or u_j = b_j v_j (fused)
+  T* P = nullptr;  // previous vector
+  T* W = nullptr;  // output of the step
+  bool fused = false;
+  std::vector<double> bn_host;  // norms of u_j (fused); 1 for the general form
 
-int fetch_ab(edg_sector_s* s, const Scalars& sc, int j, double* a, double* b) {
-  double h[2];
-  EDG_CUDA(cudaMemcpyAsync(&h[0], sc.a + j, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-  EDG_CUDA(cudaMemcpyAsync(&h[1], sc.b + j + 1, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-  EDG_CUDA(cudaStreamSynchronize(s->stream));
-  *a = h[0];
-  *b = h[1];
-  return EDG_OK;
-}
+  // v_0 = dv0 * scale; cap = most steps this run will take
+  int init(edg_sector_s* sec, const double* dv0, double scale, int cap) {
+    s = sec;
+    const int64_t n = s->dim;
+    EDG_CHECK(scalars(s, cap, &sc));
+    DevBuf<T>* wb = work<T>(s);
+    for (int k = 0; k < 3; ++k) EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
+    U = wb[0].p;
+    P = wb[1].p;
+    W = wb[2].p;
+    fused = hxv_lz_available(s, sizeof(T));
+    EDG_CHECK((convert_dev<T, double>(s->stream, U, dv0, n, scale)));
+    EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), s->stream));
+    bn_host.assign(1, 1.0);
+    return EDG_OK;
+  }
+  // scale that turns the current buffer U into v_j
+  double vscale(int j) const { return fused ? 1.0 / bn_host[j] : 1.0; }
+  // step j: W <- the unnormalised u_{j+1}; returns a_j and b_{j+1} on the host
+  int step(int j, double* a, double* b) {
+    const int64_t n = s->dim;
+    cudaStream_t st = s->stream;
+    if (fused) {
+      int nb = 0;
+      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, &nb));
+      EDG_CHECK(finish_dev(st, sc.partial, nb, sc.a + j, 0));
+      EDG_CHECK(lanczos_step_b2<T>(st, W, U, sc.a + j, sc.bn + j, n, sc.partial, sc.bn + j + 1));
+    } else {
+      EDG_CHECK(hxv_apply<T>(s, U, W));
+      EDG_CHECK(lanczos_step_a<T>(st, W, P, U, sc.b + j, n, sc.partial, sc.a + j));
+      EDG_CHECK(lanczos_step_b<T>(st, W, U, sc.a + j, n, sc.partial, sc.b + j + 1));
+    }
+    double h[2];
+    EDG_CUDA(cudaMemcpyAsync(&h[0], sc.a + j, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaMemcpyAsync(&h[1], (fused ? sc.bn : sc.b) + j + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+    *a = h[0];
+    *b = h[1];
+    return EDG_OK;
+  }
+  // after step j with b = b_{j+1} > 0: make U hold (a multiple of) v_{j+1}
+  int advance(int j, double b) {
+    if (fused) {
+      T* t = P;
+      P = U;
+      U = W;
+      W = t;
+      bn_host.push_back(b);
+    } else {
+      EDG_CHECK(scale_into<T>(s->stream, P, W, sc.b + j + 1, s->dim));
+      T* t = P;
+      P = U;
+      U = t;
+    }
+    return EDG_OK;
+  }
+};
 
 // Tridiagonalisation in precision T from the FP64 device start vector dv0.
 template <typename T>
@@ -71,28 +134,21 @@ int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, d
               double* norm2, int* nsteps) {
   const int64_t n = s->dim;
   cudaStream_t st = s->stream;
-  Scalars sc;
-  EDG_CHECK(scalars(s, nlanc + 1, &sc));
   for (int j = 0; j < nlanc; ++j) { alanc[j] = 0.0; blanc[j] = 0.0; }
   *nsteps = 0;
-  EDG_CHECK(dot_dev<double>(st, dv0, dv0, n, sc.partial, sc.b + nlanc + 1));
+  Scalars sc0;
+  EDG_CHECK(scalars(s, 2, &sc0));
+  EDG_CHECK(dot_dev<double>(st, dv0, dv0, n, sc0.partial, sc0.tmp));
   double n2 = 0.0;
-  EDG_CUDA(cudaMemcpyAsync(&n2, sc.b + nlanc + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaMemcpyAsync(&n2, sc0.tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));
   *norm2 = n2;
   if (n2 == 0.0 || nlanc <= 0) return EDG_OK;
-  DevBuf<T>* wb = work<T>(s);
-  for (int k = 0; k < 3; ++k) EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
-  T* V = wb[0].p;
-  T* P = wb[1].p;
-  T* W = wb[2].p;
-  EDG_CHECK((convert_dev<T, double>(st, V, dv0, n, 1.0 / std::sqrt(n2))));
-  EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), st));
-  EDG_CUDA(cudaMemsetAsync(sc.b, 0, sizeof(double), st));
+  Recurrence<T> R;
+  EDG_CHECK(R.init(s, dv0, 1.0 / std::sqrt(n2), nlanc + 1));
   for (int j = 0; j < nlanc; ++j) {
-    EDG_CHECK(step<T>(s, sc, j, V, P, W));
     double a, b;
-    EDG_CHECK(fetch_ab(s, sc, j, &a, &b));
+    EDG_CHECK(R.step(j, &a, &b));
     alanc[j] = a;
     *nsteps = j + 1;
     if (j + 1 < nlanc) blanc[j + 1] = b;
@@ -101,10 +157,7 @@ int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, d
       break;
     }
     if (j + 1 == nlanc) break;
-    EDG_CHECK(scale_into<T>(st, P, W, sc.b + j + 1, n));
-    T* t = P;
-    P = V;
-    V = t;
+    EDG_CHECK(R.advance(j, b));
   }
   return EDG_OK;
 }
@@ -128,30 +181,23 @@ Ritz lowest_ritz(const std::vector<double>& a, const std::vector<double>& b, dou
 }
 
 // Plain Lanczos in precision T from the normalised FP64 device vector dv0 until the lowest
-// Ritz value settles (|dE| <= tol*|E|), b underflows, or maxit. Optionally stores the basis
-// (FP32 only) so the Ritz vector needs no second pass. Returns a, b (b[0] = 0).
+// Ritz value is converged to tol (see lowest_ritz), b underflows, or maxit. Optionally stores
+// the normalised basis vectors in FP32 so the Ritz vector needs no second pass.
 template <typename T>
 int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vector<double>* A,
            std::vector<double>* B, float* basis, int basis_cols, double* e0) {
   const int64_t n = s->dim;
   cudaStream_t st = s->stream;
-  Scalars sc;
-  EDG_CHECK(scalars(s, maxit + 1, &sc));
-  DevBuf<T>* wb = work<T>(s);
-  for (int k = 0; k < 3; ++k) EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
-  T* V = wb[0].p;
-  T* P = wb[1].p;
-  T* W = wb[2].p;
-  EDG_CHECK((convert_dev<T, double>(st, V, dv0, n, 1.0)));
-  EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), st));
+  Recurrence<T> R;
+  EDG_CHECK(R.init(s, dv0, 1.0, maxit + 1));
   A->clear();
   B->assign(1, 0.0);
   double eold = 0.0;
   for (int j = 0; j < maxit; ++j) {
-    if (basis && j < basis_cols) EDG_CHECK((convert_dev<float, T>(st, basis + size_t(j) * n, V, n, 1.0)));
-    EDG_CHECK(step<T>(s, sc, j, V, P, W));
+    if (basis && j < basis_cols)
+      EDG_CHECK((convert_dev<float, T>(st, basis + size_t(j) * n, R.U, n, R.vscale(j))));
     double a, b;
-    EDG_CHECK(fetch_ab(s, sc, j, &a, &b));
+    EDG_CHECK(R.step(j, &a, &b));
     if (!std::isfinite(a) || !std::isfinite(b)) {
       set_error("Lanczos produced a non-finite coefficient at step %d", j);
       return EDG_ERR_NOCONV;
@@ -167,10 +213,7 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
     B->push_back(b);
     *e0 = e;
     if (conv || j + 1 == maxit) break;
-    EDG_CHECK(scale_into<T>(st, P, W, sc.b + j + 1, n));
-    T* t = P;
-    P = V;
-    V = t;
+    EDG_CHECK(R.advance(j, b));
   }
   return EDG_OK;
 }
@@ -194,30 +237,22 @@ int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A
     EDG_CHECK(ritz_dev(st, basis, scz.a, m, n, x));
     EDG_CUDA(cudaStreamSynchronize(st));  // Z (host) must outlive the copy
   } else {
-    Scalars sc;
-    EDG_CHECK(scalars(s, m + 1, &sc));
-    DevBuf<T>* wb = work<T>(s);
-    T* V = wb[0].p;
-    T* P = wb[1].p;
-    T* W = wb[2].p;
-    EDG_CHECK((convert_dev<T, double>(st, V, dv0, n, 1.0)));
-    EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), st));
+    Recurrence<T> R;
+    EDG_CHECK(R.init(s, dv0, 1.0, m + 1));
     for (int j = 0; j < m; ++j) {
-      EDG_CHECK(axpy_accum_dev<T>(st, x, V, Z[j], n));
+      EDG_CHECK(axpy_accum_dev<T>(st, x, R.U, Z[j] * R.vscale(j), n));
       if (j + 1 == m) break;
-      EDG_CHECK(step<T>(s, sc, j, V, P, W));
-      EDG_CHECK(scale_into<T>(st, P, W, sc.b + j + 1, n));
-      T* t = P;
-      P = V;
-      V = t;
+      double a, b;
+      EDG_CHECK(R.step(j, &a, &b));
+      EDG_CHECK(R.advance(j, b));
     }
   }
   // normalise
   Scalars sc2;
   EDG_CHECK(scalars(s, 2, &sc2));
-  EDG_CHECK(dot_dev<double>(st, x, x, n, sc2.partial, sc2.a));
+  EDG_CHECK(dot_dev<double>(st, x, x, n, sc2.partial, sc2.tmp));
   double nn = 0.0;
-  EDG_CUDA(cudaMemcpyAsync(&nn, sc2.a, sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaMemcpyAsync(&nn, sc2.tmp, sizeof(double), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));
   if (!(nn > 0.0)) {
     set_error("Ritz vector vanished");
@@ -231,9 +266,9 @@ int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A
 int normalise(edg_sector_s* s, double* dv) {
   Scalars sc;
   EDG_CHECK(scalars(s, 2, &sc));
-  EDG_CHECK(dot_dev<double>(s->stream, dv, dv, s->dim, sc.partial, sc.a));
+  EDG_CHECK(dot_dev<double>(s->stream, dv, dv, s->dim, sc.partial, sc.tmp));
   double nn = 0.0;
-  EDG_CUDA(cudaMemcpyAsync(&nn, sc.a, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EDG_CUDA(cudaMemcpyAsync(&nn, sc.tmp, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   EDG_CUDA(cudaStreamSynchronize(s->stream));
   if (!(nn > 0.0)) {
     set_error("start vector has zero norm");

@@ -78,6 +78,23 @@ __global__ void __launch_bounds__(kRedThreads) k_step_b(T* __restrict__ w, const
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// Fused recurrence, second half: u_{j+1} = w - (a_j / bn_j) u_j in place on w, and the
+// partial sums of |u_{j+1}|^2 (bn_{j+1} after the finish pass).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_step_b2(T* __restrict__ w, const T* __restrict__ u,
+                                                         const double* __restrict__ a, const double* __restrict__ bn,
+                                                         int64_t n, double* __restrict__ partial) {
+  const double coef = *a / *bn;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const T wt = T(double(w[i]) - coef * double(u[i]));
+    w[i] = wt;
+    s = __fma_rn(double(wt), double(wt), s);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
 template <typename T>
 __global__ void k_scale_into(T* __restrict__ dst, const T* __restrict__ src, const double* __restrict__ b, int64_t n) {
   const double bb = *b;
@@ -161,6 +178,21 @@ int lanczos_step_b(cudaStream_t st, T* w, const T* v, const double* a, int64_t n
 }
 
 template <typename T>
+int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
+                    double* bn_next) {
+  k_step_b2<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n, partial);
+  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, bn_next, 1);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, int do_sqrt) {
+  k_finish<<<1, kRedThreads, 0, st>>>(partial, nblk, out, do_sqrt);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
 int scale_into(cudaStream_t st, T* dst, const T* src, const double* b, int64_t n) {
   k_scale_into<T><<<grid_for(n), 256, 0, st>>>(dst, src, b, n);
   EDG_CUDA(cudaGetLastError());
@@ -204,6 +236,8 @@ int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed) {
                                  double*);                                                                 \
   template int lanczos_step_b<T>(cudaStream_t, T*, const T*, const double*, int64_t, double*, double*);   \
   template int scale_into<T>(cudaStream_t, T*, const T*, const double*, int64_t);                         \
+  template int lanczos_step_b2<T>(cudaStream_t, T*, const T*, const double*, const double*, int64_t,      \
+                                  double*, double*);                                                      \
   template int axpy_accum_dev<T>(cudaStream_t, double*, const T*, double, int64_t);
 EDG_INST(float)
 EDG_INST(double)
