@@ -376,6 +376,7 @@ static void build_schedule(int64_t dim, int rt, const std::vector<uint32_t>& off
       width = std::max(width, D);
     }
     const size_t base = ent.size();
+    width = (width + kSellBatch - 1) / kSellBatch * kSellBatch;  // whole batches: no bounds checks
     soff[sl + 1] = soff[sl] + 32u * uint32_t(width);
     ent.resize(base + size_t(32) * width, 0u);
     std::vector<char> used(size_t(width) * M);
@@ -459,6 +460,7 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
   for (int64_t sl = 0; sl < nsl; ++sl) {
     uint32_t w = 0;
     for (int64_t r = sl * 32; r < std::min<int64_t>(dim, sl * 32 + 32); ++r) w = std::max(w, off[r + 1] - off[r]);
+    w = (w + kSellBatch - 1) / kSellBatch * kSellBatch;
     soff[sl + 1] = soff[sl] + 32 * w;
   }
   double h0 = B.nnz ? std::fabs(val[0]) : 0.0;

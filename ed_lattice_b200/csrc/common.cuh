@@ -156,6 +156,7 @@ namespace edg {
 constexpr size_t kUpSmemTwoPerSM = 113 * 1024;
 constexpr size_t kUpSmemOnePerSM = 227 * 1024;
 constexpr int kUpZeroSlots = 32;
+constexpr int kSellBatch = 8;  // SELL slice widths are multiples of this (entries loaded per batch)
 inline int up_rows_per_cta(int64_t dimup, size_t elem) {
   const size_t row = size_t(dimup + kUpZeroSlots) * elem;
   if (elem == 4 && 4 * row <= kUpSmemTwoPerSM) return 4;

@@ -179,17 +179,16 @@ __global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> s
 #pragma unroll
         for (int r = 0; r < RT; ++r) acc[r] = (r0 + r < a.dimdw) ? a.hv[(r0 + r) * dimup + iup] : T(0);
       }
-      // entries in batches of independent loads; slots past the slice end read the zero slot
-      constexpr int kUpBatch = 8;
-      const uint32_t pad = uint32_t(dimup);
+      // entries in batches of independent loads (slice widths are whole batches; padding
+      // entries read a zero column)
+      constexpr int kUpBatch = kSellBatch;
       for (uint32_t p0 = o + lane; p0 < o1; p0 += 32 * kUpBatch) {
         uint32_t e[kUpBatch];
         T hv_[kUpBatch];
 #pragma unroll
         for (int u = 0; u < kUpBatch; ++u) {
-          const uint32_t p = p0 + 32u * u;
-          e[u] = p < o1 ? __ldg(sl.ent + p) : pad;
-          if (!UNIFORM) hv_[u] = p < o1 ? __ldg(sl.val + p) : T(0);
+          e[u] = __ldg(sl.ent + p0 + 32u * u);
+          if (!UNIFORM) hv_[u] = __ldg(sl.val + p0 + 32u * u);
         }
 #pragma unroll
         for (int u = 0; u < kUpBatch; ++u) {
