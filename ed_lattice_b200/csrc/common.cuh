@@ -159,7 +159,7 @@ constexpr int kUpZeroSlots = 32;
 constexpr int kSellBatch = 8;  // SELL slice widths are multiples of this (entries loaded per batch)
 inline int up_rows_per_cta(int64_t dimup, size_t elem) {
   const size_t row = size_t(dimup + kUpZeroSlots) * elem;
-  if (elem == 4 && 4 * row <= kUpSmemTwoPerSM) return 4;
+  if (elem == 4 && 4 * row <= kUpSmemTwoPerSM) return 4;  // (4 rows with 1 CTA/SM measured slower)
   if (2 * row <= kUpSmemTwoPerSM) return 2;
   if (row <= kUpSmemOnePerSM) return 1;
   return 0;
