@@ -66,6 +66,9 @@ SIGNATURES = {
     "edg_ground_state": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pd, _pi]),
     "edg_ground_state_keep": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pi]),
     "edg_ground_state_stats": (_i, [_p, _pi, _pi]),
+    "edg_lowest_k": (_i, [_p, _i, _pd, _u64, _i, _d, _pd, _pd, _pd, _pi]),
+    "edg_sector_dense": (_i, [_p, _pd]),
+    "edg_sector_dense_dev": (_i, [_p, _p]),
     "edg_state_get": (_i, [_p, _pd]),
     "edg_state_set": (_i, [_p, _pd]),
     "edg_random_vector": (_i, [_u64, _i64, _pd]),

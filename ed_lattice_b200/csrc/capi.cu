@@ -334,6 +334,31 @@ int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, 
   return EDG_OK;
 }
 
+int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol, double* evals,
+                 double* evecs, double* resid, int* niter) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(evals && niter, "edg_lowest_k: NULL output");
+  EDG_ARG(k >= 1 && k <= 16, "edg_lowest_k: k=%d outside 1..16", k);
+  EDG_ARG(maxit >= 1, "edg_lowest_k: maxit=%d", maxit);
+  EDG_ARG(tol > 0.0 && std::isfinite(tol), "edg_lowest_k: tol must be > 0");
+  EDG_CHECK(ensure_device(s));
+  return lowest_k(s, k, v0, seed, maxit, tol, evals, evecs, resid, niter);
+}
+
+int edg_sector_dense(edg_sector* s, double* h) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(h, "edg_sector_dense: NULL");
+  EDG_CHECK(ensure_device(s));
+  return sector_dense(s, h);
+}
+
+int edg_sector_dense_dev(edg_sector* s, double* dh) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(dh, "edg_sector_dense_dev: NULL");
+  EDG_CHECK(ensure_device(s));
+  return sector_dense_dev(s, dh);
+}
+
 int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64) {
   EDG_CHECK(check_sector(s));
   if (n_f32) *n_f32 = s->last_n32;

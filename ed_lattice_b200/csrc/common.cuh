@@ -208,6 +208,12 @@ int tridiag_dev(edg_sector_s* s, const double* dv0, int nlanc, double threshold,
 int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
                  double* e0, int* niter);
 
+// ---- lowest.cu
+int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, double* evals,
+             double* evecs_host, double* resid, int* niter);
+int sector_dense(edg_sector_s* s, double* H_host);
+int sector_dense_dev(edg_sector_s* s, double* dH);
+
 // ---- tridiag_host.cpp
 // zn (optional): last components of the eigenvectors (Ritz residual estimates b*|zn|).
 int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull,

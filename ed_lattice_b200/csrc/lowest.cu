@@ -1,0 +1,265 @@
+// lowest.cu -- the lowest k eigenpairs of a sector, and the dense sector matrix.
+//
+// edg_lowest_k stands in for the sp_eigh (ARPACK) call of ed_diag_d
+// (src/DIAG/DIAG.f90:144-146,191-202): Neigen = min(dim, lanc_nstates_sector) lowest states
+// of a sector for the finite-temperature state list. Method: FP64 Lanczos with full
+// reorthogonalisation (classical Gram-Schmidt applied twice) against the basis kept on the
+// device, stopped when the k lowest Ritz pairs have residual b_{m+1}|z_m,i| below
+// tol*max(1,|theta_i|); the Ritz vectors are then formed in one pass over the basis.
+// Single-vector Lanczos resolves one vector per eigenspace, so exactly degenerate levels
+// inside one sector are found only through round-off; the dense path covers small sectors.
+//
+// edg_sector_dense fills the dense sector Hamiltonian the way ed_buildh(Hmat) assembles it
+// (src/DIAG/HAMILTONIAN_STORED_HxV.f90:81-117): diag + kron(Hdw,1) + kron(1,Hup), for the
+// lapack branch of ed_diag_d (src/DIAG/DIAG.f90:229-254).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace edg {
+namespace {
+
+constexpr int kMaxBasis = 1024;   // Lanczos basis columns (multi-dot coefficients in shared memory)
+constexpr int kMaxK = 16;         // eigenpairs per call
+constexpr int kLkThreads = 256;
+constexpr int kDenseMaxDim = 16384;  // 2 GB dense matrix
+
+// partial[j * nblk + blk] = sum over this block's elements of Q[j][i] * w[i], j < m
+__global__ void __launch_bounds__(kLkThreads) k_multidot(const double* __restrict__ Q, int m, int64_t n,
+                                                         const double* __restrict__ w, double* __restrict__ partial) {
+  __shared__ double sh[kLkThreads / 32];
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = blockIdx.x * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
+  for (int j = 0; j < m; ++j) {
+    const double* q = Q + int64_t(j) * n;
+    double s = 0.0;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) s = __fma_rn(q[i], w[i], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int q2 = 0; q2 < kLkThreads / 32; ++q2) t += sh[q2];
+      partial[int64_t(j) * gridDim.x + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// c[j] = sum_blk partial[j * nblk + blk], fixed order
+__global__ void k_multifinish(const double* __restrict__ partial, int nblk, int m, double* __restrict__ c) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  double t = 0.0;
+  for (int b = 0; b < nblk; ++b) t += partial[int64_t(j) * nblk + b];
+  c[j] = t;
+}
+
+// w[i] -= sum_j c[j] Q[j][i]
+__global__ void __launch_bounds__(kLkThreads) k_multiaxpy(const double* __restrict__ Q, const double* __restrict__ c,
+                                                          int m, int64_t n, double* __restrict__ w) {
+  __shared__ double sc[kMaxBasis];
+  for (int j = threadIdx.x; j < m; j += blockDim.x) sc[j] = c[j];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double t = w[i];
+    for (int j = 0; j < m; ++j) t = __fma_rn(-sc[j], Q[int64_t(j) * n + i], t);
+    w[i] = t;
+  }
+}
+
+// X[r][i] = sum_j Z[j*m + r] Q[j][i], r < k (Z column-major m x m, first k columns)
+__global__ void __launch_bounds__(kLkThreads) k_ritz_k(const double* __restrict__ Q, const double* __restrict__ Z,
+                                                       int m, int k, int64_t n, double* __restrict__ X) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double acc[kMaxK];
+#pragma unroll
+    for (int r = 0; r < kMaxK; ++r) acc[r] = 0.0;
+    for (int j = 0; j < m; ++j) {
+      const double q = Q[int64_t(j) * n + i];
+#pragma unroll
+      for (int r = 0; r < kMaxK; ++r)
+        if (r < k) acc[r] = __fma_rn(Z[j + int64_t(r) * m], q, acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < kMaxK; ++r)
+      if (r < k) X[int64_t(r) * n + i] = acc[r];
+  }
+}
+
+// Dense sector matrix, column-major H[i + j*D]: one thread per row i = iup + idw*DimUp.
+__global__ void k_dense(const uint32_t* __restrict__ off_up, const uint32_t* __restrict__ src_up,
+                        const double* __restrict__ val_up, const uint32_t* __restrict__ off_dw,
+                        const uint32_t* __restrict__ src_dw, const double* __restrict__ val_dw,
+                        const double* __restrict__ e_up, const double* __restrict__ e_dw,
+                        const uint32_t* __restrict__ map_up, const uint32_t* __restrict__ map_dw, double U,
+                        int64_t dimup, int64_t dimdw, double* __restrict__ H) {
+  const int64_t D = dimup * dimdw;
+  const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  if (i >= D) return;
+  const int64_t idw = i / dimup, iup = i - idw * dimup;
+  H[i + i * D] += e_up[iup] + e_dw[idw] + U * double(__popc(map_up[iup] & map_dw[idw]));
+  for (uint32_t k = off_up[iup]; k < off_up[iup + 1]; ++k) {
+    const int64_t j = int64_t(src_up[k]) + idw * dimup;
+    H[i + j * D] += val_up[k];
+  }
+  for (uint32_t k = off_dw[idw]; k < off_dw[idw + 1]; ++k) {
+    const int64_t j = iup + int64_t(src_dw[k]) * dimup;
+    H[i + j * D] += val_dw[k];
+  }
+}
+
+int grid_n(int64_t n) {
+  int64_t g = (n + kLkThreads - 1) / kLkThreads;
+  return int(g < 148 * 8 ? (g < 1 ? 1 : g) : 148 * 8);
+}
+
+}  // namespace
+
+int sector_dense_dev(edg_sector_s* s, double* dH) {
+  const int64_t D = s->dim;
+  if (D > kDenseMaxDim) {
+    set_error("edg_sector_dense: dimension %lld above %d", (long long)D, kDenseMaxDim);
+    return EDG_ERR_ARG;
+  }
+  if (s->form != EDG_FORM_STORED) {
+    set_error("edg_sector_dense: needs the stored form (hop tables)");
+    return EDG_ERR_STATE;
+  }
+  cudaStream_t st = s->stream;
+  EDG_CUDA(cudaMemsetAsync(dH, 0, size_t(D) * D * sizeof(double), st));
+  k_dense<<<int((D + 255) / 256), 256, 0, st>>>(s->up.off.p, s->up.src.p, s->up.val64.p, s->dw.off.p, s->dw.src.p,
+                                                s->dw.val64.p, s->up.e64.p, s->dw.e64.p, s->up.map.p, s->dw.map.p,
+                                                s->U, s->up.dim, s->dw.dim, dH);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+int sector_dense(edg_sector_s* s, double* H_host) {
+  const int64_t D = s->dim;
+  if (D > kDenseMaxDim) {
+    set_error("edg_sector_dense: dimension %lld above %d", (long long)D, kDenseMaxDim);
+    return EDG_ERR_ARG;
+  }
+  DevBuf<double> Hd;
+  EDG_CHECK(Hd.alloc(size_t(D) * D, "dense sector matrix"));
+  EDG_CHECK(sector_dense_dev(s, Hd.p));
+  cudaStream_t st = s->stream;
+  EDG_CUDA(cudaMemcpyAsync(H_host, Hd.p, size_t(D) * D * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  return EDG_OK;
+}
+
+int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, double* evals,
+             double* evecs_host, double* resid, int* niter) {
+  const int64_t n = s->dim;
+  cudaStream_t st = s->stream;
+  if (k < 1 || k > kMaxK) {
+    set_error("edg_lowest_k: k=%d outside 1..%d", k, kMaxK);
+    return EDG_ERR_ARG;
+  }
+  if (k > n) k = int(n);
+  int mmax = std::min<int64_t>(std::min(maxit, kMaxBasis), n);
+  if (mmax < k) mmax = k;
+  {  // the basis takes what HBM allows beyond a 2 GB reserve
+    size_t fr = 0, tot = 0;
+    EDG_CUDA(cudaMemGetInfo(&fr, &tot));
+    const size_t reserve = size_t(2) << 30, per = size_t(n) * sizeof(double);
+    const int64_t fit = fr > reserve + 4 * per ? int64_t((fr - reserve) / per) - 4 : 0;
+    if (fit < mmax) mmax = int(fit);
+    if (mmax < k || mmax < 1) {
+      set_error("edg_lowest_k: %lld-element basis vectors: no room for %d of them", (long long)n, k);
+      return EDG_ERR_NOMEM;
+    }
+  }
+  // device: basis Q[mmax][n], w, scratch
+  DevBuf<double> Q, w, part, coef, Zd, X;
+  EDG_CHECK(Q.alloc(size_t(mmax) * n, "Lanczos basis (lowest-k)"));
+  EDG_CHECK(w.alloc(n, "Lanczos vector"));
+  const int nblk = std::min<int64_t>(592, (n + kLkThreads - 1) / kLkThreads);
+  EDG_CHECK(part.alloc(size_t(std::max(mmax, 2)) * nblk + kRedBlocks, "multi-dot partials"));
+  EDG_CHECK(coef.alloc(size_t(mmax) + 8, "multi-dot coefficients"));
+  // start vector
+  if (v0_host) {
+    EDG_CUDA(cudaMemcpyAsync(Q.p, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  } else {
+    EDG_CHECK(random_dev(st, Q.p, n, seed));
+  }
+  auto norm_of = [&](const double* x, double* out) -> int {
+    EDG_CHECK(dot_dev<double>(st, x, x, n, part.p, coef.p + mmax));
+    double h = 0.0;
+    EDG_CUDA(cudaMemcpyAsync(&h, coef.p + mmax, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+    *out = std::sqrt(h);
+    return EDG_OK;
+  };
+  double nrm = 0.0;
+  EDG_CHECK(norm_of(Q.p, &nrm));
+  if (!(nrm > 0.0)) {
+    set_error("edg_lowest_k: start vector has zero norm");
+    return EDG_ERR_ARG;
+  }
+  EDG_CHECK((convert_dev<double, double>(st, Q.p, Q.p, n, 1.0 / nrm)));
+  std::vector<double> A, B(1, 0.0), cvec(mmax), zlast;
+  double blast = 0.0;
+  int m = 0;
+  bool done = false;
+  for (int j = 0; j < mmax && !done; ++j) {
+    double* qj = Q.p + size_t(j) * n;
+    EDG_CHECK(hxv_apply<double>(s, qj, w.p));
+    // a_j = <q_j, w>; then full reorthogonalisation against q_0..q_j (twice)
+    for (int pass = 0; pass < 2; ++pass) {
+      k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, part.p);
+      k_multifinish<<<(j + 1 + 127) / 128, 128, 0, st>>>(part.p, nblk, j + 1, coef.p);
+      if (pass == 0) {
+        EDG_CUDA(cudaMemcpyAsync(cvec.data(), coef.p, size_t(j + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+      }
+      k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
+    }
+    EDG_CUDA(cudaGetLastError());
+    EDG_CUDA(cudaStreamSynchronize(st));
+    A.push_back(cvec[j]);
+    double b = 0.0;
+    EDG_CHECK(norm_of(w.p, &b));
+    m = j + 1;
+    // Ritz values and residual estimates of the lowest k
+    std::vector<double> th(m), zl(m);
+    EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
+    zlast = zl;
+    blast = b;
+    if (m >= k) {
+      bool conv = true;
+      for (int i = 0; i < k; ++i)
+        if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) conv = false;
+      if (conv) done = true;
+    }
+    if (b < 1e-12 || m == n) done = true;  // invariant subspace reached
+    if (done || m == mmax) break;
+    B.push_back(b);
+    EDG_CHECK((convert_dev<double, double>(st, Q.p + size_t(m) * n, w.p, n, 1.0 / b)));
+  }
+  if (niter) *niter = m;
+  std::vector<double> th(m), Z(size_t(m) * m);
+  EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, Z.data()));
+  const int kk = std::min(k, m);
+  for (int i = 0; i < kk; ++i) evals[i] = th[i];
+  for (int i = kk; i < k; ++i) evals[i] = NAN;
+  if (resid) {
+    for (int i = 0; i < kk; ++i) resid[i] = blast * std::fabs(zlast[i]);
+    for (int i = kk; i < k; ++i) resid[i] = NAN;
+  }
+  if (evecs_host) {
+    EDG_CHECK(Zd.alloc(size_t(m) * m, "Ritz coefficients"));
+    EDG_CHECK(X.alloc(size_t(kk) * n, "Ritz vectors"));
+    EDG_CUDA(cudaMemcpyAsync(Zd.p, Z.data(), size_t(m) * m * sizeof(double), cudaMemcpyHostToDevice, st));
+    k_ritz_k<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p, m, kk, n, X.p);
+    EDG_CUDA(cudaGetLastError());
+    EDG_CUDA(cudaMemcpyAsync(evecs_host, X.p, size_t(kk) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+  }
+  return EDG_OK;
+}
+
+}  // namespace edg

@@ -212,6 +212,36 @@ class Sector:
         L.check(L.lib().edg_hxv_d(self.handle, v.size, _pd(v), _pd(hv)), "spHtimesV")
         return hv
 
+    def set_stream(self, stream: int | None) -> None:
+        """Run the sector's device work on `stream` (a cudaStream_t as an int; None = own stream)."""
+        L.check(L.lib().edg_sector_set_stream(self.handle, C.c_void_p(stream)), "edg_sector_set_stream")
+
+    def lowest_k(self, k: int, v0: np.ndarray | None = None, seed: int = 1234, maxit: int = 512,
+                 tol: float = 1e-10, want_vectors: bool = True):
+        """Lowest k eigenpairs (the sp_eigh branch of ed_diag_d, src/DIAG/DIAG.f90:191-202).
+        Returns (evals[k'], evecs[k', dim] or None, resid[k'], basis size), k' = min(k, dim)."""
+        kk = min(k, self.dim)
+        ev = np.zeros(k)
+        rs = np.zeros(k)
+        vecs = np.empty((kk, self.dim)) if want_vectors else None
+        it = C.c_int()
+        v0a = _f64(v0) if v0 is not None else None
+        if v0a is not None and v0a.size != self.dim:
+            raise ValueError("v0 size != sector dimension")
+        L.check(L.lib().edg_lowest_k(self.handle, k, _pd(v0a), C.c_uint64(seed), maxit, tol, _pd(ev), _pd(vecs),
+                                     _pd(rs), C.byref(it)), "sp_eigh")
+        return ev[:kk], vecs, rs[:kk], it.value
+
+    def dense(self) -> np.ndarray:
+        """Dense sector matrix of ed_buildh(Hmat) (src/DIAG/HAMILTONIAN_STORED_HxV.f90:81-117)."""
+        h = np.empty((self.dim, self.dim))
+        L.check(L.lib().edg_sector_dense(self.handle, _pd(h)), "ed_buildh")
+        return h  # symmetric: row- and column-major read the same
+
+    def dense_dev(self, dh_ptr: int) -> None:
+        """Dense sector matrix into device memory (dim*dim doubles) on the sector's stream."""
+        L.check(L.lib().edg_sector_dense_dev(self.handle, C.c_void_p(dh_ptr)), "ed_buildh")
+
     # ---- state buffer (the eigenvector kept on the device)
     def get_state(self) -> np.ndarray:
         x = np.empty(self.dim)

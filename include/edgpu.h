@@ -150,6 +150,26 @@ int edg_ground_state_keep(edg_sector* s, const double* v0, uint64_t seed, int ma
 /* H x v applications of the last ground-state run, split by vector precision (FP32 phase,
  * FP64 phase). No counterpart in the reference (sp_lanc_eigh reports no statistics). */
 int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64);
+/* Lowest k (1..16) eigenpairs of a sector: the sp_eigh (ARPACK) branch of ed_diag_d,
+ * Neigen = min(dim, lanc_nstates_sector) states per sector for the finite-temperature state
+ * list (src/DIAG/DIAG.f90:144-146,191-202). FP64 Lanczos with full reorthogonalisation
+ * (Gram-Schmidt twice per step) against a basis of at most min(maxit, 1024) device
+ * vectors (fewer if HBM is short); stops when every one of the k lowest Ritz pairs has
+ * residual b_{m+1}|z_{m,i}| <= tol*max(1,|theta_i|), or the Krylov space becomes invariant,
+ * or the basis is full. evals[k] ascending (NaN beyond dim); evecs (host, may be NULL):
+ * k normalised vectors, vector r at evecs + r*dim; resid (may be NULL): the k residual
+ * estimates at exit (the caller checks them against tol); *niter = basis size. v0 and
+ * seed as in edg_ground_state. One vector per eigenspace: exactly degenerate levels
+ * inside a sector appear once (use edg_sector_dense for small sectors with symmetries). */
+int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol,
+                 double* evals, double* evecs, double* resid, int* niter);
+/* Dense sector Hamiltonian, column-major dim x dim (the matrix ed_buildh(Hmat) assembles for
+ * the LAPACK branch of ed_diag_d, src/DIAG/HAMILTONIAN_STORED_HxV.f90:81-117 and
+ * src/DIAG/DIAG.f90:229-235): diag + kron(H_dw, 1) + kron(1, H_up). Stored form only;
+ * dim <= 16384. h: host array of dim*dim doubles; the _dev variant writes device memory
+ * on the sector's stream without synchronising. */
+int edg_sector_dense(edg_sector* s, double* h);
+int edg_sector_dense_dev(edg_sector* s, double* dh);
 int edg_state_get(const edg_sector* s, double* evec);
 int edg_state_set(edg_sector* s, const double* evec);
 

@@ -83,9 +83,61 @@ def disorder3x4():
                         gf_norm2=n2)
 
 
+def thermal3x4():
+    """The disorder3x4 lattice over all 169 (Nup,Ndw) sectors: the lowest 4 levels of each
+    sector, then the finite-temperature state list at beta=20 (T=0.05, cutoff 1e-9) with Z and
+    the thermal n_i, n_i,up, n_i,dw, d_i, m_i. Sectors with D <= 4000 are diagonalised densely
+    (scipy.linalg.eigh on the oracle's dense matrix); larger ones with ARPACK (scipy's eigsh,
+    the library behind the reference's sp_eigh) over the oracle's stored H x v."""
+    import math
+
+    import scipy.linalg as sla
+    import scipy.sparse.linalg as spla
+
+    rng = np.random.default_rng(7)
+    eps = np.round(rng.uniform(-1, 1, 12) * 65536) / 65536
+    H = square(3, 4)
+    H[np.diag_indices(12)] = eps
+    m = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    ns, k, temp, cutoff = 12, 4, 0.05, 1e-9
+    energies = np.full(((ns + 1) ** 2, k), np.nan)
+    dims = np.zeros((ns + 1) ** 2, dtype=np.int64)
+    states = []
+    for isector in range(1, (ns + 1) ** 2 + 1):
+        nup, ndw = O.lib().orc_get_nup(ns, isector), O.lib().orc_get_ndw(ns, isector)
+        D = O.binomial(ns, nup) * O.binomial(ns, ndw)
+        dims[isector - 1] = D
+        kk = min(k, D)
+        if D <= 4000:
+            w, z = sla.eigh(O.dense_h(m, nup, ndw), subset_by_index=[0, kk - 1])
+        else:
+            st = O.Stored(m, nup, ndw)
+            op = spla.LinearOperator((D, D), matvec=lambda v, st=st: st.matvec_d(np.ascontiguousarray(v)),
+                                     dtype=np.float64)
+            w, z = spla.eigsh(op, k=kk, which="SA", tol=1e-13, ncv=40, v0=O.random_vector(5, D), maxiter=5000)
+            order = np.argsort(w)
+            w, z = w[order], z[:, order]
+        energies[isector - 1, :kk] = w
+        states += [(w[i], isector, nup, ndw, z[:, i]) for i in range(kk)]
+        print(f"sector ({nup},{ndw}) D={D} E={w}", flush=True)
+    states.sort(key=lambda s: s[0])
+    egs = states[0][0]
+    kept = [s for s in states if math.exp(-(s[0] - egs) / temp) > cutoff]
+    zeta = sum(math.exp(-(s[0] - egs) / temp) for s in kept)
+    acc = {q: np.zeros(ns) for q in ("dens", "dens_up", "dens_dw", "docc", "magz")}
+    for e, _, nup, ndw, v in kept:
+        o = O.observables(ns, nup, ndw, v, math.exp(-(e - egs) / temp) / zeta)
+        for q in acc:
+            acc[q] += o[q]
+    np.savez_compressed(os.path.join(HERE, "thermal3x4.npz"), eps=eps, dims=dims, energies=energies, egs=egs,
+                        zeta=zeta, nkept=len(kept), kept_sectors=np.array([s[1] for s in kept]),
+                        kept_energies=np.array([s[0] for s in kept]), **acc)
+
+
 if __name__ == "__main__":
-    config1()
-    disorder3x4()
+    which = sys.argv[1:] or ["config1", "disorder3x4", "thermal3x4"]
+    for name in which:
+        globals()[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

@@ -1,0 +1,146 @@
+"""Host logic of the sector-diagonalisation driver (no GPU): the state list (es_*), the
+finite-T bookkeeping of ed_diag_d, partition_function_lattice and lanc_observables. The
+per-sector eigensolver and the observables of one state are injected from the CPU oracle
+(dense diagonalisation), and the thermal averages are checked against a brute-force sum over
+every eigenstate of every sector."""
+import math
+
+import numpy as np
+import pytest
+
+import ed_lattice_b200 as E
+from ed_lattice_b200.diag import DiagParams, StateList, diagonalize_lattice, lanc_observables, partition_function
+from oracle import oracle as O
+
+
+def test_state_list_order_cap_and_pop():
+    sl = StateList()
+    for e, sec in ((0.5, 1), (-1.0, 2), (0.5, 3), (2.0, 4)):
+        sl.add_state(e, None, sec)
+    # equal energies: the newcomer goes before the older entry (es_insert_state)
+    assert [s.sector for s in sl.states] == [2, 3, 1, 4]
+    assert sl.emin == -1.0 and sl.emax == 2.0
+    sl.pop_state()
+    assert sl.energy() == 0.5 and sl.emax == 2.0  # pop keeps the running maximum
+    # capped insert: a full list only takes states below its last entry
+    sl.add_state(1.0, None, 5, size=3)
+    assert sl.size == 3 and 5 not in [s.sector for s in sl.states]
+    sl.add_state(0.0, None, 6, size=3)
+    assert [s.e for s in sl.states] == [-1.0, 0.0, 0.5]
+    sl.pop_state(1)
+    assert sl.energy(1) == 0.0
+    sl.free()
+    assert sl.size == 0 and sl.emin == math.inf
+    with pytest.raises(E.EdgError):
+        sl.pop_state()
+
+
+def test_state_list_trim_and_degeneracy():
+    sl = StateList()
+    for e in (0.0, 1e-10, 0.3, 0.6, 5.0):
+        sl.add_state(e, None, 1)
+    assert sl.gs_degeneracy(1e-9) == 2
+    # T=0.1, cutoff 1e-9: exp(-E/T) > 1e-9 for E < 2.07
+    assert sl.trim_size(0.1, 1e-9, True) == 4
+    assert sl.trim_size(0.1, 1e-9, False) == 5
+
+
+def test_setup_state_counts():
+    p = DiagParams(finite_temp=True, lanc_nstates_sector=3).setup(169)
+    assert p.lanc_nstates_sector == 4 and p.lanc_nstates_total == 4 * 169 + 10
+    p = DiagParams(finite_temp=True, lanc_nstates_sector=2).setup(25)
+    assert p.lanc_nstates_total == 60
+    with pytest.raises(E.EdgError):
+        DiagParams(lanc_method="nope").setup(4)
+
+
+def _chain4(seed=3):
+    rng = np.random.default_rng(seed)
+    H = E.ring(4).astype(float)
+    H[np.diag_indices(4)] = np.round(rng.uniform(-1, 1, 4) * 2**16) / 2**16
+    return H
+
+
+def _oracle_solver(om):
+    def solve(model, nup, ndw, neigen, lanc_solve, params, seed):
+        w, z = np.linalg.eigh(O.dense_h(om, nup, ndw))
+        return w[:neigen], z[:, :neigen].T.copy()
+    return solve
+
+
+def _oracle_observer(model, isector, vec, bw):
+    return O.observables(model.ns, model.get_nup(isector), model.get_ndw(isector), vec, bw)
+
+
+def _brute_force(om, ns, temp, cutoff):
+    """Every eigenstate of every sector: Z and weighted observables with the reference cutoff."""
+    states = []
+    for nup in range(ns + 1):
+        for ndw in range(ns + 1):
+            w, z = np.linalg.eigh(O.dense_h(om, nup, ndw))
+            states += [(w[i], nup, ndw, z[:, i]) for i in range(w.size)]
+    egs = min(s[0] for s in states)
+    kept = [s for s in states if math.exp(-(s[0] - egs) / temp) > cutoff]
+    zeta = sum(math.exp(-(s[0] - egs) / temp) for s in kept)
+    acc = {k: np.zeros(ns) for k in ("dens", "dens_up", "dens_dw", "docc", "magz")}
+    for e, nup, ndw, v in kept:
+        o = O.observables(ns, nup, ndw, v, math.exp(-(e - egs) / temp) / zeta)
+        for k in acc:
+            acc[k] += o[k]
+    return egs, zeta, acc
+
+
+@pytest.mark.parametrize("temp", [0.05, 0.5])
+def test_finite_temperature_against_brute_force(temp):
+    H = _chain4()
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    # 36 states per sector = every state of the 4-site sectors: the list is exact up to the cutoff
+    p = DiagParams(finite_temp=True, temp=temp, lanc_nstates_sector=36)
+    sl, eigs = diagonalize_lattice(m, p, solver=_oracle_solver(om))
+    assert len(eigs) == 25
+    zeta = partition_function(sl, p)
+    obs = lanc_observables(m, sl, zeta, p, observer=_oracle_observer)
+    egs, zref, ref = _brute_force(om, 4, temp, p.cutoff)
+    assert sl.emin == pytest.approx(egs, abs=1e-13)
+    assert zeta == pytest.approx(zref, rel=1e-12)
+    for k in ref:
+        assert np.allclose(obs[k], ref[k], atol=1e-12), k
+    assert np.allclose(obs["mag"], obs["dens_up"] - obs["dens_dw"])
+
+
+def test_cutoff_condition_not_met_raises():
+    H = _chain4()
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    p = DiagParams(finite_temp=True, temp=5.0, lanc_nstates_sector=2)
+    with pytest.raises(E.EdgError, match="Cutoff"):
+        diagonalize_lattice(m, p, solver=_oracle_solver(om))
+
+
+def test_zero_temperature_ground_manifold():
+    H = _chain4(seed=11)
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    p = DiagParams(finite_temp=False, lanc_nstates_sector=2)
+    sl, _ = diagonalize_lattice(m, p, solver=_oracle_solver(om))
+    # brute force: lowest level over all sectors and its multiplet (spin degeneracy across Sz)
+    lev = sorted((np.linalg.eigvalsh(O.dense_h(om, a, b))[0], a, b) for a in range(5) for b in range(5))
+    e0 = lev[0][0]
+    manifold = [(a, b) for (e, a, b) in lev if abs(e - e0) <= 1e-9]
+    assert sl.size == len(manifold) == sl.gs_degeneracy()
+    assert sorted((m.get_nup(s.sector), m.get_ndw(s.sector)) for s in sl.states) == sorted(manifold)
+    zeta = partition_function(sl, p)
+    assert zeta == float(len(manifold))
+    obs = lanc_observables(m, sl, zeta, p, observer=_oracle_observer)
+    assert obs["dens"].sum() == pytest.approx(sum(a + b for a, b in manifold) / len(manifold), abs=1e-10)
+
+
+def test_filling_restricts_sectors():
+    H = _chain4()
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False, ed_filling=4)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False, ed_filling=4)
+    p = DiagParams(finite_temp=True, temp=0.2, lanc_nstates_sector=36)
+    sl, eigs = diagonalize_lattice(m, p, solver=_oracle_solver(om))
+    assert len(eigs) == 5  # (0,4) (1,3) (2,2) (3,1) (4,0)
+    assert all(m.get_nup(s.sector) + m.get_ndw(s.sector) == 4 for s in sl.states)

@@ -1,0 +1,116 @@
+"""The 6x3 periodic lattice at half filling, sector (9,9): D = 48,620^2 = 2,363,904,400 > 2^31,
+beyond the reference's int32 Dim. Checks of the 64-bit indexing at full size: exact columns
+H e_i for indices past 2^31 (integer matrix elements, so FP32 is exact), FP32 against FP64,
+and the symmetry <x|H z> = <H x|z>."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import ed_lattice_b200 as E
+from ed_lattice_b200 import _edgpu_lib as L
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+NS, N, U, XMU = 18, 9, 4.0, 2.0
+
+
+@pytest.fixture(scope="module")
+def big():
+    import torch
+    model = E.Model(E.square_lattice(6, 3), uloc=U, xmu=XMU, hfmode=False)
+    s = E.Sector(model, N, N)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    assert s.dim == 2_363_904_400 and s.dim > 2**31
+    yield s
+    s.delete()
+    torch.cuda.empty_cache()
+
+
+def hxv(s, x, y):
+    import torch
+    fn = L.lib().edg_hxv_dev_f64 if x.dtype == torch.float64 else L.lib().edg_hxv_dev_f32
+    L.check(fn(s.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "hxv")
+    torch.cuda.synchronize()
+
+
+def chunked_dot(a, b, chunk=1 << 28):
+    tot = 0.0
+    for i in range(0, a.numel(), chunk):
+        tot += float((a[i:i + chunk].double() * b[i:i + chunk].double()).sum().item())
+    return tot
+
+
+def expected_column(i, maps, tabs, dimup):
+    """H e_i from the oracle's hop tables: diagonal -XMU*(2N) + U*popcount(up & dw) (eps = 0,
+    HFMODE=F), up hops along the row of idw, down hops along the column of iup."""
+    iup, idw = i % dimup, i // dimup
+    mu, md = int(maps[iup]), int(maps[idw])
+    cols = {i: -XMU * 2 * N + U * bin(mu & md).count("1")}
+    rp, c, v = tabs
+    for k in range(rp[iup], rp[iup + 1]):
+        cols[int(c[k]) + idw * dimup] = float(v[k])
+    for k in range(rp[idw], rp[idw + 1]):
+        cols[iup + int(c[k]) * dimup] = float(v[k])
+    return cols
+
+
+def test_diag_formula_small_sector():
+    """The diagonal used below, checked against the oracle's stored H x v on sector (2,2)."""
+    om = O.Model(E.square_lattice(6, 3), uloc=U, xmu=XMU, hfmode=False)
+    st = O.Stored(om, 2, 2)
+    maps = O.build_map(NS, 2)
+    for i in (0, 77, st.dim - 1):
+        e = np.zeros(st.dim)
+        e[i] = 1.0
+        iup, idw = i % maps.size, i // maps.size
+        assert st.matvec_d(e)[i] == -XMU * 4 + U * bin(int(maps[iup]) & int(maps[idw])).count("1")
+
+
+def test_columns_past_int32(big):
+    import torch
+    om = O.Model(E.square_lattice(6, 3), uloc=U, xmu=XMU, hfmode=False)
+    maps = O.build_map(NS, N)
+    tabs = O.hop_csr(om, 1, N)  # same table for both spins (same N, spin-independent Hij)
+    x = torch.zeros(big.dim, dtype=torch.float32, device="cuda")
+    y = torch.empty_like(x)
+    for i in (0, 2**31 - 5, 2**31 + 12_345, big.dim - big.dimup + 17, big.dim - 1):
+        x[i] = 1.0
+        hxv(big, x, y)
+        x[i] = 0.0
+        exp = expected_column(i, maps, tabs, big.dimup)
+        idx = torch.tensor(sorted(exp), dtype=torch.int64, device="cuda")
+        got = y[idx].double().cpu().numpy()
+        want = np.array([exp[j] for j in sorted(exp)])
+        assert np.array_equal(got, want), i
+        assert int((y != 0).sum().item()) == len(exp), i
+    del x, y
+    torch.cuda.empty_cache()
+
+
+def test_f32_f64_and_symmetry(big):
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x64 = torch.rand(big.dim, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    y64 = torch.empty_like(x64)
+    hxv(big, x64, y64)
+    x32 = x64.float()
+    y32 = torch.empty_like(x32)
+    hxv(big, x32, y32)
+    err = 0.0
+    chunk = 1 << 28
+    for i in range(0, big.dim, chunk):
+        err = max(err, (y32[i:i + chunk].double() - y64[i:i + chunk]).abs().max().item())
+    scale = y64[: 1 << 26].abs().max().item()
+    assert err <= 2e-6 * scale
+    del y64, x64
+    torch.cuda.empty_cache()
+    z32 = torch.rand(big.dim, dtype=torch.float32, device="cuda", generator=g) * 2 - 1
+    hz = torch.empty_like(z32)
+    hxv(big, z32, hz)
+    a = chunked_dot(x32, hz)
+    b = chunked_dot(y32, z32)
+    assert abs(a - b) <= 1e-5 * max(abs(a), 1.0)
+    del x32, y32, z32, hz
+    torch.cuda.empty_cache()
