@@ -149,18 +149,21 @@ struct edg_sector_s {
 
 namespace edg {
 
-// Rows per CTA of the shared-memory up pass for element size `elem` (4 or 8 bytes): the most
-// that fit two CTAs per SM (113 KB each), else one row with one CTA per SM (227 KB), else 0
-// (the row does not fit; the L1-gather kernel takes over). The staged rows carry 32 zero
-// columns after DimUp (padding targets).
+// Rows per CTA of the shared-memory up pass for element size `elem` (4 or 8 bytes): four FP32
+// rows if they fit two CTAs per SM (113 KB each), else two rows (two CTAs per SM if they fit,
+// else one CTA of up to 227 KB), else one row with one CTA per SM, else 0 (the row does not
+// fit; the L1-gather kernel takes over). On the 4x4 half-filled sector (DimUp 12870): FP32
+// two rows with two CTAs per SM (four rows in one CTA measured 2.17 against 1.87 ms per
+// H x v); FP64 two rows in one CTA (4.30 against 4.46 ms for one row with two CTAs). The
+// staged rows carry 32 zero columns after DimUp (padding targets).
 constexpr size_t kUpSmemTwoPerSM = 113 * 1024;
 constexpr size_t kUpSmemOnePerSM = 227 * 1024;
 constexpr int kUpZeroSlots = 32;
 constexpr int kSellBatch = 8;  // SELL slice widths are multiples of this (entries loaded per batch)
 inline int up_rows_per_cta(int64_t dimup, size_t elem) {
   const size_t row = size_t(dimup + kUpZeroSlots) * elem;
-  if (elem == 4 && 4 * row <= kUpSmemTwoPerSM) return 4;  // (4 rows with 1 CTA/SM measured slower)
-  if (2 * row <= kUpSmemTwoPerSM) return 2;
+  if (elem == 4 && 4 * row <= kUpSmemTwoPerSM) return 4;
+  if (2 * row <= kUpSmemOnePerSM) return 2;
   if (row <= kUpSmemOnePerSM) return 1;
   return 0;
 }

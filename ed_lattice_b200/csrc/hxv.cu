@@ -131,8 +131,11 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 
 // SELL entry: bit 31 = sign of the uniform value, bits 0..30 = source column (DimUp for
 // padding: a zero slot after the staged rows, so padding needs no branch).
-template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ>
-__global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+// ONE: one CTA per SM (the staged rows take more than half of shared memory); the 64
+// registers per thread this allows carry the next batch of entries while the current one is
+// applied.
+template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE>
+__global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
@@ -182,19 +185,43 @@ __global__ void __launch_bounds__(1024, 2) k_up_smem(HxvArgs<T> a, SellArgs<T> s
       // entries in batches of independent loads (slice widths are whole batches; padding
       // entries read a zero column)
       constexpr int kUpBatch = kSellBatch;
-      for (uint32_t p0 = o + lane; p0 < o1; p0 += 32 * kUpBatch) {
+      if (ONE && UNIFORM) {
         uint32_t e[kUpBatch];
-        T hv_[kUpBatch];
+        uint32_t p0 = o + lane;
+        if (p0 < o1) {
 #pragma unroll
-        for (int u = 0; u < kUpBatch; ++u) {
-          e[u] = __ldg(sl.ent + p0 + 32u * u);
-          if (!UNIFORM) hv_[u] = __ldg(sl.val + p0 + 32u * u);
+          for (int u = 0; u < kUpBatch; ++u) e[u] = __ldg(sl.ent + p0 + 32u * u);
         }
+        for (; p0 < o1; p0 += 32 * kUpBatch) {
+          uint32_t en[kUpBatch];
+          const uint32_t pn = p0 + 32 * kUpBatch;
+          if (pn < o1) {
 #pragma unroll
-        for (int u = 0; u < kUpBatch; ++u) {
-          const T h = UNIFORM ? flip_sign(hs, e[u]) : (LZ ? T(double(hv_[u]) * sc) : hv_[u]);
-          const V x = S[e[u] & 0x7fffffffu];
-          Fma<T, RT>::run(h, reinterpret_cast<const T*>(&x), acc);
+            for (int u = 0; u < kUpBatch; ++u) en[u] = __ldg(sl.ent + pn + 32u * u);
+          }
+#pragma unroll
+          for (int u = 0; u < kUpBatch; ++u) {
+            const V x = S[e[u] & 0x7fffffffu];
+            Fma<T, RT>::run(flip_sign(hs, e[u]), reinterpret_cast<const T*>(&x), acc);
+          }
+#pragma unroll
+          for (int u = 0; u < kUpBatch; ++u) e[u] = en[u];
+        }
+      } else {
+        for (uint32_t p0 = o + lane; p0 < o1; p0 += 32 * kUpBatch) {
+          uint32_t e[kUpBatch];
+          T hv_[kUpBatch];
+#pragma unroll
+          for (int u = 0; u < kUpBatch; ++u) {
+            e[u] = __ldg(sl.ent + p0 + 32u * u);
+            if (!UNIFORM) hv_[u] = __ldg(sl.val + p0 + 32u * u);
+          }
+#pragma unroll
+          for (int u = 0; u < kUpBatch; ++u) {
+            const T h = UNIFORM ? flip_sign(hs, e[u]) : (LZ ? T(double(hv_[u]) * sc) : hv_[u]);
+            const V x = S[e[u] & 0x7fffffffu];
+            Fma<T, RT>::run(h, reinterpret_cast<const T*>(&x), acc);
+          }
         }
       }
       if (LZ) {
@@ -546,10 +573,10 @@ const float* pick_sell<float>(const SpinBasis& B) { return B.sell_v32.p; }
 template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ>
 int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, int sms, int* grid) {
   const size_t smem = size_t(a.dimup + kUpZeroSlots) * RT * sizeof(T);
-  auto kern = k_up_smem<T, RT, FIRST, UNIFORM, LZ>;
+  const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
+  auto kern = per_sm == 2 ? k_up_smem<T, RT, FIRST, UNIFORM, LZ, false> : k_up_smem<T, RT, FIRST, UNIFORM, LZ, true>;
   if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
-  const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
   const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
   kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());

@@ -26,35 +26,53 @@ constexpr int kMaxK = 16;         // eigenpairs per call
 constexpr int kLkThreads = 256;
 constexpr int kDenseMaxDim = 16384;  // 2 GB dense matrix
 
-// partial[j * nblk + blk] = sum over this block's elements of Q[j][i] * w[i], j < m
+// partial[j * nblk + blk] = sum over this block's chunk of Q[j][i] * w[i] for j < m, and with
+// `self` also column m = <w, w>. Each warp takes groups of kColGrp columns, its lanes stride
+// over the chunk with one load of w and kColGrp loads of Q in flight per step; no block
+// barrier. Fixed summation order (deterministic).
+constexpr int kColGrp = 8;
 __global__ void __launch_bounds__(kLkThreads) k_multidot(const double* __restrict__ Q, int m, int64_t n,
-                                                         const double* __restrict__ w, double* __restrict__ partial) {
-  __shared__ double sh[kLkThreads / 32];
-  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+                                                         const double* __restrict__ w, int self,
+                                                         double* __restrict__ partial) {
+  int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  chunk = (chunk + 31) & ~int64_t(31);
   const int64_t i0 = blockIdx.x * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
-  for (int j = 0; j < m; ++j) {
-    const double* q = Q + int64_t(j) * n;
-    double s = 0.0;
-    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) s = __fma_rn(q[i], w[i], s);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int q2 = 0; q2 < kLkThreads / 32; ++q2) t += sh[q2];
-      partial[int64_t(j) * gridDim.x + blockIdx.x] = t;
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int mt = m + (self ? 1 : 0);
+  const int ngrp = (mt + kColGrp - 1) / kColGrp;
+  for (int g = threadIdx.x >> 5; g < ngrp; g += nw) {
+    const int j0 = g * kColGrp;
+    const double* __restrict__ q[kColGrp];
+#pragma unroll
+    for (int c = 0; c < kColGrp; ++c) {
+      const int j = j0 + c < mt ? j0 + c : mt - 1;  // tail columns repeat the last one
+      q[c] = j < m ? Q + int64_t(j) * n : w;
     }
-    __syncthreads();
+    double acc[kColGrp];
+#pragma unroll
+    for (int c = 0; c < kColGrp; ++c) acc[c] = 0.0;
+    for (int64_t i = i0 + lane; i < i1; i += 32) {
+      const double wi = w[i];
+#pragma unroll
+      for (int c = 0; c < kColGrp; ++c) acc[c] = __fma_rn(q[c][i], wi, acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < kColGrp; ++c) {
+      double t = acc[c];
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (lane == 0 && j0 + c < mt) partial[int64_t(j0 + c) * gridDim.x + blockIdx.x] = t;
+    }
   }
 }
 
-// c[j] = sum_blk partial[j * nblk + blk], fixed order
+// c[j] = sum_blk partial[j * nblk + blk], one warp per column, fixed order
 __global__ void k_multifinish(const double* __restrict__ partial, int nblk, int m, double* __restrict__ c) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (j >= m) return;
   double t = 0.0;
-  for (int b = 0; b < nblk; ++b) t += partial[int64_t(j) * nblk + b];
-  c[j] = t;
+  for (int b = lane; b < nblk; b += 32) t += partial[int64_t(j) * nblk + b];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if (lane == 0) c[j] = t;
 }
 
 // w[i] -= sum_j c[j] Q[j][i]
@@ -65,6 +83,7 @@ __global__ void __launch_bounds__(kLkThreads) k_multiaxpy(const double* __restri
   __syncthreads();
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     double t = w[i];
+#pragma unroll 8
     for (int j = 0; j < m; ++j) t = __fma_rn(-sc[j], Q[int64_t(j) * n + i], t);
     w[i] = t;
   }
@@ -179,7 +198,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   EDG_CHECK(Q.alloc(size_t(mmax) * n, "Lanczos basis (lowest-k)"));
   EDG_CHECK(w.alloc(n, "Lanczos vector"));
   const int nblk = std::min<int64_t>(592, (n + kLkThreads - 1) / kLkThreads);
-  EDG_CHECK(part.alloc(size_t(std::max(mmax, 2)) * nblk + kRedBlocks, "multi-dot partials"));
+  EDG_CHECK(part.alloc(size_t(mmax + 1) * nblk + kRedBlocks, "multi-dot partials"));
   EDG_CHECK(coef.alloc(size_t(mmax) + 8, "multi-dot coefficients"));
   // start vector
   if (v0_host) {
@@ -188,9 +207,9 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     EDG_CHECK(random_dev(st, Q.p, n, seed));
   }
   auto norm_of = [&](const double* x, double* out) -> int {
-    EDG_CHECK(dot_dev<double>(st, x, x, n, part.p, coef.p + mmax));
+    EDG_CHECK(dot_dev<double>(st, x, x, n, part.p, coef.p + mmax + 4));
     double h = 0.0;
-    EDG_CUDA(cudaMemcpyAsync(&h, coef.p + mmax, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaMemcpyAsync(&h, coef.p + mmax + 4, sizeof(double), cudaMemcpyDeviceToHost, st));
     EDG_CUDA(cudaStreamSynchronize(st));
     *out = std::sqrt(h);
     return EDG_OK;
@@ -202,41 +221,55 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     return EDG_ERR_ARG;
   }
   EDG_CHECK((convert_dev<double, double>(st, Q.p, Q.p, n, 1.0 / nrm)));
-  std::vector<double> A, B(1, 0.0), cvec(mmax), zlast;
+  std::vector<double> A, B(1, 0.0), cvec(size_t(mmax) + 1), zlast;
+  int npass2 = 0;
   double blast = 0.0;
   int m = 0;
   bool done = false;
   for (int j = 0; j < mmax && !done; ++j) {
     double* qj = Q.p + size_t(j) * n;
     EDG_CHECK(hxv_apply<double>(s, qj, w.p));
-    // a_j = <q_j, w>; then full reorthogonalisation against q_0..q_j (twice)
-    for (int pass = 0; pass < 2; ++pass) {
-      k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, part.p);
-      k_multifinish<<<(j + 1 + 127) / 128, 128, 0, st>>>(part.p, nblk, j + 1, coef.p);
-      if (pass == 0) {
-        EDG_CUDA(cudaMemcpyAsync(cvec.data(), coef.p, size_t(j + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
-      }
-      k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
-    }
+    // a_j = <q_j, w>; full reorthogonalisation against q_0..q_j by classical Gram-Schmidt,
+    // repeated when the projection removed more than half of |w|^2 (Daniel, Gragg, Kaufman &
+    // Stewart, Math. Comp. 30 (1976) 772). With |a_j| well above b_j, as for the shifted
+    // spectra of Hubbard sectors, that is nearly every step; one pass alone lost
+    // orthogonality entirely on small sectors.
+    k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, 1, part.p);
+    k_multifinish<<<(j + 2 + 7) / 8, 256, 0, st>>>(part.p, nblk, j + 2, coef.p);
+    EDG_CUDA(cudaMemcpyAsync(cvec.data(), coef.p, size_t(j + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
     EDG_CUDA(cudaGetLastError());
     EDG_CUDA(cudaStreamSynchronize(st));
+    const double wnorm0 = std::sqrt(std::max(cvec[j + 1], 0.0));  // |H q_j|
     A.push_back(cvec[j]);
     double b = 0.0;
     EDG_CHECK(norm_of(w.p, &b));
-    m = j + 1;
-    // Ritz values and residual estimates of the lowest k
-    std::vector<double> th(m), zl(m);
-    EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
-    zlast = zl;
-    blast = b;
-    if (m >= k) {
-      bool conv = true;
-      for (int i = 0; i < k; ++i)
-        if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) conv = false;
-      if (conv) done = true;
+    if (b < 0.7071067811865476 * wnorm0) {
+      k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, 0, part.p);
+      k_multifinish<<<(j + 1 + 7) / 8, 256, 0, st>>>(part.p, nblk, j + 1, coef.p);
+      k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
+      EDG_CUDA(cudaGetLastError());
+      EDG_CHECK(norm_of(w.p, &b));
+      ++npass2;
     }
-    if (b < 1e-12 || m == n) done = true;  // invariant subspace reached
-    if (done || m == mmax) break;
+    m = j + 1;
+    const bool last = b < 1e-12 || m == n || m == mmax;  // invariant subspace reached, or full
+    // Ritz values and residual estimates of the lowest k: the host eigensolve costs O(m^2), so
+    // it runs every max(1, m/32) steps (at most m/32 extra H x v past convergence)
+    if ((m >= k && (m - k) % std::max(1, m / 32) == 0) || last) {
+      std::vector<double> th(m), zl(m);
+      EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
+      zlast = zl;
+      blast = b;
+      if (m >= k) {
+        bool conv = true;
+        for (int i = 0; i < k; ++i)
+          if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) conv = false;
+        if (conv) done = true;
+      }
+    }
+    if (last) done = true;
+    if (done) break;
     B.push_back(b);
     EDG_CHECK((convert_dev<double, double>(st, Q.p + size_t(m) * n, w.p, n, 1.0 / b)));
   }
