@@ -230,6 +230,48 @@ def thermal_3x4(E):
             "docc_mean": float(obs["docc"].mean())}
 
 
+def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150):
+    """Green's function chains on the 4x4 lattice at U=4 (t=1, XMU=2): ground state of the
+    half-filled sector (8,8) (FP32+refine, vector kept on the device), then c^+_{i,up} into
+    (9,8) and c_{i,up} into (7,8) (D = 147,232,800 each) for the 16 sites: 32 chains of 150
+    steps with FP32 vectors, G_ii(iw_n) on 4096 Matsubara frequencies at beta=50 and on the
+    real axis (eta=0.05). Also the first `nchains_f64` chains with FP64 vectors for the ratio."""
+    import torch
+    model = E.Model(E.square_lattice(4, 4), uloc=4.0, xmu=2.0, hfmode=False)
+    gs = E.Sector(model, 8, 8)
+    part, hole = E.Sector(model, 9, 8), E.Sector(model, 7, 8)
+    e0, it = C.c_double(), C.c_int()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.check(L.lib().edg_ground_state_keep(gs.handle, None, C.c_uint64(2024), 600, 1e-10, E.EDG_GS_F32_REFINE,
+                                          C.byref(e0), C.byref(it)), "gs")
+    torch.cuda.synchronize()
+    t_gs = time.perf_counter() - t0
+    out = {"e0": e0.value, "gs_seconds": t_gs, "gs_hxv": it.value, "dim_gs": gs.dim, "dim_excited": part.dim}
+    for prec, name, nch in ((E.EDG_PREC_F32, "f32", 32), (E.EDG_PREC_F64, "f64", nchains_f64)):
+        chans = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for c in range(nch):
+            site = c // 2 + 1
+            # particle chains (op=+1) and hole chains (op=-1, poles already -(theta-E0))
+            to, op = (part, +1) if c % 2 == 0 else (hole, -1)
+            chans.append(E.gf_chain(gs, to, op, site, 1, nlanc, e0.value, precision=prec))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        steps = sum(len(ch.poles) for ch in chans)
+        out[name] = {"chains": nch, "seconds": dt, "lanczos_steps": steps, "ms_per_step": 1e3 * dt / steps,
+                     "sum_rule_site1": chans[0].norm2 + chans[1].norm2}
+        if name == "f32":
+            wm, _, wr, _, _ = E.grids(1.0 / 50.0, lmats=4096, lreal=5000)
+            gm, gr = E.eval_gf(chans[:2], wm, wr, 0.05)
+            out[name]["G11_iw0"] = [gm[0].real, gm[0].imag]
+    out["f32_speedup_per_step"] = out["f64"]["ms_per_step"] / out["f32"]["ms_per_step"]
+    for sct in (gs, part, hole):
+        sct.delete()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -333,6 +375,10 @@ def run_ours(args):
         extra["e0_time_to_1e-8"] = e0_time_to_solution(E, L, sector)
     if rank == 0 and not args.no_thermal and ws == 1:
         extra["thermal_3x4_beta20"] = thermal_3x4(E)
+    if rank == 0 and not args.no_gf and ws == 1:
+        sector.delete()
+        torch.cuda.empty_cache()
+        extra["gf_chains_4x4_U4"] = gf_4x4_chains(E, L)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         val, info = cpu_baseline_sample()
@@ -377,6 +423,7 @@ def main():
     ap.add_argument("--no-e0", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-thermal", action="store_true")
+    ap.add_argument("--no-gf", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -505,6 +505,64 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
       B.sched_rt = rt32;
     }
   }
+  // column-split copy for rows that do not fit shared memory whole (FP64 rows above 227 KB)
+  B.split_parts = 0;
+  if (up_rows_per_cta(dim, sizeof(double)) == 0 && B.nnz > 0) {
+    const int64_t cap = int64_t(kUpSmemOnePerSM / sizeof(double)) - kUpZeroSlots;
+    const int P = int((dim + cap - 1) / cap);
+    if (P <= SpinBasis::kMaxSplit) {
+      const int64_t wpart = (dim + P - 1) / P;
+      for (int p = 0; p <= P; ++p) B.split_col[p] = std::min<int64_t>(dim, p * wpart);
+      std::vector<uint32_t> poff(size_t(P) * (nsl + 1), 0), pent;
+      std::vector<double> pval;
+      std::vector<uint32_t> lo(32), hi(32);
+      size_t base = 0;
+      for (int p = 0; p < P; ++p) {
+        const uint32_t c0 = uint32_t(B.split_col[p]), c1 = uint32_t(B.split_col[p + 1]);
+        for (int64_t sl = 0; sl < nsl; ++sl) {
+          poff[size_t(p) * (nsl + 1) + sl] = uint32_t(base);
+          uint32_t w = 0;
+          for (int l = 0; l < 32; ++l) {
+            const int64_t r = sl * 32 + l;
+            lo[l] = hi[l] = 0;
+            if (r >= dim) continue;
+            const uint32_t* b0 = src.data() + off[r];
+            const uint32_t* b1 = src.data() + off[r + 1];
+            lo[l] = uint32_t(std::lower_bound(b0, b1, c0) - src.data());
+            hi[l] = uint32_t(std::lower_bound(b0, b1, c1) - src.data());
+            w = std::max(w, hi[l] - lo[l]);
+          }
+          w = (w + kSellBatch - 1) / kSellBatch * kSellBatch;
+          pent.resize(base + size_t(32) * w, c1 - c0);
+          if (!uniform) pval.resize(base + size_t(32) * w, 0.0);
+          for (int l = 0; l < 32; ++l)
+            for (uint32_t k = lo[l]; k < hi[l]; ++k) {
+              const size_t pos = base + size_t(k - lo[l]) * 32 + l;
+              const uint32_t sign = uniform ? ((val[k] == hsgn) ? 0u : 1u) : 0u;
+              pent[pos] = (src[k] - c0) | (sign << 31);
+              if (!uniform) pval[pos] = val[k];
+            }
+          base += size_t(32) * w;
+        }
+        poff[size_t(p) * (nsl + 1) + nsl] = uint32_t(base);
+      }
+      pent.push_back(0u);
+      EDG_CHECK(B.split_off.alloc(poff.size(), "split SELL offsets"));
+      EDG_CHECK(B.split_ent.alloc(pent.size(), "split SELL entries"));
+      EDG_CUDA(cudaMemcpyAsync(B.split_off.p, poff.data(), poff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      EDG_CUDA(cudaMemcpyAsync(B.split_ent.p, pent.data(), pent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      if (!uniform) {
+        pval.push_back(0.0);
+        std::vector<float> pv32(pval.begin(), pval.end());
+        EDG_CHECK(B.split_v64.alloc(pval.size(), "split SELL values"));
+        EDG_CHECK(B.split_v32.alloc(pv32.size(), "split SELL values"));
+        EDG_CUDA(cudaMemcpyAsync(B.split_v64.p, pval.data(), pval.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        EDG_CUDA(cudaMemcpyAsync(B.split_v32.p, pv32.data(), pv32.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+      }
+      EDG_CUDA(cudaStreamSynchronize(st));  // host staging vectors go out of scope
+      B.split_parts = P;
+    }
+  }
   EDG_CHECK(B.sell_off.alloc(nsl + 1, "SELL offsets"));
   EDG_CHECK(B.sell_ent.alloc(ent.size(), "SELL entries"));
   EDG_CUDA(cudaMemcpyAsync(B.sell_off.p, soff.data(), soff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));

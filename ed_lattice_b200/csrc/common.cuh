@@ -95,6 +95,18 @@ struct SpinBasis {
   DevBuf<uint32_t> sched_ent;
   DevBuf<uint32_t> sched_off;
   int sched_rt = 0;             // rows-per-CTA of the FP32 up pass the schedule was built for
+  // Column-split copy of the SELL table for rows too long to stage whole in shared memory
+  // (FP64 rows above 227 KB): part p lists, per slice, the entries whose source lies in
+  // columns [split_col[p], split_col[p+1]), stored as source - split_col[p] (padding: the
+  // part's width, a zero slot after the staged part). Concatenating the parts keeps each
+  // row's sources ascending, so the summation order is that of the whole table.
+  static constexpr int kMaxSplit = 8;
+  int split_parts = 0;
+  int64_t split_col[kMaxSplit + 1] = {};
+  DevBuf<uint32_t> split_ent;   // parts concatenated
+  DevBuf<uint32_t> split_off;   // [parts * (nslices + 1)]: part p's slice starts, then its end
+  DevBuf<double> split_v64;     // only when !sell_uniform
+  DevBuf<float> split_v32;
   int max_row = 0;              // longest hop list of any configuration
   // Down-spin pass work split: rows grouped into `groups` CTAs with near-equal total hop
   // counts (longest-processing-time-first assignment), CSR: group_off[groups+1], group_rows.

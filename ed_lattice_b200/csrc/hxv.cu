@@ -11,6 +11,8 @@
 //  STORED (spMatVec, src/DIAG/HAMILTONIAN_STORED_HxV.f90:159-220): diag, DW, UP;
 //  DIRECT (directMatVec, src/DIAG/HAMILTONIAN_DIRECT_HxV.f90:19-59): diag, UP, DW;
 // inside each spin part sources are added in ascending rank, as the reference's loops do.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace edg {
@@ -257,6 +259,65 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, Sel
   }
 }
 
+// Up pass for rows too long to stage whole (FP64 rows above 227 KB): one CTA per row (grid-
+// stride) stages the row one column part at a time and applies that part's entries; between
+// parts the running sums of the row live in hv (the CTA's own row, just written, so L2).
+// Each target column is always handled by the same thread, and the parts' entries come in
+// ascending source order, so the sums are those of the whole-row kernels.
+template <typename T>
+struct SplitArgs {
+  const uint32_t* __restrict__ ent;
+  const uint32_t* __restrict__ off;
+  const T* __restrict__ val;  // non-uniform tables only
+  T h;
+  int parts;
+  int64_t nsl;
+  int64_t col[SpinBasis::kMaxSplit + 1];
+};
+
+template <typename T, bool FIRST, bool UNIFORM>
+__global__ void __launch_bounds__(1024, 1) k_up_split(HxvArgs<T> a, SplitArgs<T> sp) {
+  extern __shared__ __align__(16) unsigned char smem_split[];
+  T* S = reinterpret_cast<T*>(smem_split);
+  const int64_t dimup = a.dimup;
+  for (int64_t idw = blockIdx.x; idw < a.dimdw; idw += gridDim.x) {
+    const T* __restrict__ vrow = a.v + idw * dimup;
+    T* __restrict__ hrow = a.hv + idw * dimup;
+    for (int p = 0; p < sp.parts; ++p) {
+      const int64_t c0 = sp.col[p], w = sp.col[p + 1] - c0;
+      for (int64_t j = threadIdx.x; j < w + kUpZeroSlots; j += blockDim.x) S[j] = j < w ? vrow[c0 + j] : T(0);
+      __syncthreads();
+      const uint32_t* __restrict__ offp = sp.off + int64_t(p) * (sp.nsl + 1);
+      for (int64_t iup = threadIdx.x; iup < dimup; iup += blockDim.x) {
+        T acc;
+        if (FIRST && p == 0) {
+          const T d = a.e_up[iup] + a.e_dw[idw] + a.U * T(__popc(a.map_up[iup] & a.map_dw[idw]));
+          acc = d * vrow[iup];
+        } else {
+          acc = hrow[iup];
+        }
+        const uint32_t o = offp[iup >> 5], o1 = offp[(iup >> 5) + 1];
+        for (uint32_t q = o + uint32_t(iup & 31); q < o1; q += 32 * kSellBatch) {
+          uint32_t e[kSellBatch];
+          T hv_[kSellBatch];
+#pragma unroll
+          for (int u = 0; u < kSellBatch; ++u) {
+            e[u] = __ldg(sp.ent + q + 32u * u);
+            if (!UNIFORM) hv_[u] = __ldg(sp.val + q + 32u * u);
+          }
+#pragma unroll
+          for (int u = 0; u < kSellBatch; ++u) {
+            const T h = UNIFORM ? flip_sign(sp.h, e[u]) : hv_[u];
+            acc = fmaT<T>(h, S[e[u] & 0x7fffffffu], acc);
+          }
+        }
+        hrow[iup] = acc;
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // Down-spin pass, one warp per (row idw', segment of 32*VEC consecutive iup). The row's hop
 // list is uniform across the warp: lanes load up to 32 (source, value) pairs in one
 // coalesced read and hand them out with shuffles; the source rows are then read as
@@ -456,30 +517,6 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
   }
 }
 
-// Column-slab pass: a tile is 32 consecutive iup x 8 rows; tiles are visited slab-major so
-// that the slab of V being combined (DimDw rows x 32 columns) stays resident in L2 while
-// every row of it is read ~(hops per row) times. FIRST: hv = diag*v + dw-part.
-template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256) k_dw_slab(HxvArgs<T> a, int64_t nrb, int64_t ntiles) {
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t slab = tile / nrb, rb = tile - slab * nrb;
-    const int64_t iup = slab * 32 + threadIdx.x;
-    const int64_t idw = rb * 8 + threadIdx.y;
-    if (iup >= a.dimup || idw >= a.dimdw) continue;
-    const int64_t e = idw * a.dimup + iup;
-    T acc;
-    if (FIRST) {
-      const T d = a.e_up[iup] + a.e_dw[idw] + a.U * T(__popc(a.map_up[iup] & a.map_dw[idw]));
-      acc = d * a.v[e];
-    } else {
-      acc = a.hv[e];
-    }
-    const uint32_t k0 = a.off_dw[idw], k1 = a.off_dw[idw + 1];
-    for (uint32_t k = k0; k < k1; ++k) acc = fmaT<T>(a.val_dw[k], a.v[int64_t(a.src_dw[k]) * a.dimup + iup], acc);
-    a.hv[e] = acc;
-  }
-}
-
 // ---------------------------------------------------------------- direct (on-the-fly) form
 // No tables: each thread derives its hops from the bitstrings, as directMatVec does, with
 // ranks from the combinatorial number system instead of binary_search. Bonds arrive
@@ -625,6 +662,25 @@ int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms, i
     if (LZ) {
       set_error("fused Lanczos H x v needs the shared-memory up pass");
       return EDG_ERR_UNSUPPORTED;
+    }
+    if (B.split_parts > 0) {
+      SplitArgs<T> sp;
+      sp.ent = B.split_ent.p;
+      sp.off = B.split_off.p;
+      sp.val = sizeof(T) == 8 ? reinterpret_cast<const T*>(B.split_v64.p) : reinterpret_cast<const T*>(B.split_v32.p);
+      sp.h = T(B.sell_h);
+      sp.parts = B.split_parts;
+      sp.nsl = (a.dimup + 31) / 32;
+      int64_t wmax = 0;
+      for (int p = 0; p <= SpinBasis::kMaxSplit; ++p) sp.col[p] = p <= B.split_parts ? B.split_col[p] : 0;
+      for (int p = 0; p < B.split_parts; ++p) wmax = std::max<int64_t>(wmax, sp.col[p + 1] - sp.col[p]);
+      const size_t smem = size_t(wmax + kUpZeroSlots) * sizeof(T);
+      auto kern = B.sell_uniform ? k_up_split<T, FIRST, true> : k_up_split<T, FIRST, false>;
+      EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      const int g = int(a.dimdw < int64_t(sms) ? a.dimdw : int64_t(sms));
+      kern<<<g, 1024, smem, st>>>(a, sp);
+      EDG_CUDA(cudaGetLastError());
+      return EDG_OK;
     }
     const int g = int(a.dimdw < int64_t(sms) * 8 ? a.dimdw : int64_t(sms) * 8);
     k_up_rows<T, FIRST><<<g, 256, 0, st>>>(a);

@@ -168,14 +168,19 @@ int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, d
 struct Ritz {
   double e0, err;
 };
-Ritz lowest_ritz(const std::vector<double>& a, const std::vector<double>& b, double b_next) {
+// `window` (relative to |theta_1|): Ritz values that close to the lowest one are taken as its
+// copies (the duplicates that plain Lanczos produces once orthogonality is lost, which FP32
+// vectors reach early) and skipped when the gap is measured; 0 takes the next Ritz value.
+Ritz lowest_ritz(const std::vector<double>& a, const std::vector<double>& b, double b_next, double window) {
   const int m = int(a.size());
   std::vector<double> w(m), zl(m);
   tridiag_eigh_host(m, a.data(), b.data(), w.data(), nullptr, nullptr, zl.data());
   Ritz r;
   r.e0 = w[0];
   const double res = b_next * std::fabs(zl[0]);
-  const double gap = m > 1 ? w[1] - w[0] : 0.0;
+  int i = 1;
+  while (i < m && w[i] - w[0] <= window * std::fabs(w[0])) ++i;
+  const double gap = i < m ? w[i] - w[0] : 0.0;
   r.err = gap > 1e-12 ? res * res / gap : res;
   return r;
 }
@@ -203,7 +208,8 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
       return EDG_ERR_NOCONV;
     }
     A->push_back(a);
-    const Ritz rz = lowest_ritz(*A, *B, b);
+    // FP32 vectors lose orthogonality within tens of steps: skip the copies of E0 that follow
+    const Ritz rz = lowest_ritz(*A, *B, b, sizeof(T) == 4 ? 10.0 * tol : 0.0);
     const double e = rz.e0;
     // converged when the error estimate is 10x below tol*|E0| (or, as a fallback for a
     // degenerate lowest level, when E0 stops moving), or the Krylov space is exhausted

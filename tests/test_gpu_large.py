@@ -71,3 +71,31 @@ def test_large_stored_vs_direct(sector):
     # parts differs (stored: diag, DW, UP; direct: diag, UP, DW)
     assert (ys - yd).abs().max().item() <= 1e-12 * ys.abs().max().item()
     sd.delete()
+
+
+def test_gf_chains_config3_size():
+    """4x4 lattice at U=4: ground state of (8,8), then c^+_{1,up} into (9,8) and c_{1,up} into
+    (7,8) (D = 147,232,800 each). The particle and hole norms add up to 1 (the anticommutator
+    {c, c^+} = 1 on a normalised state), their difference is 1 - 2 n_{1,up} from the state's
+    observables, and the FP32 chains reproduce the FP64 G(iw_n) at beta=50."""
+    model = E.Model(E.square_lattice(4, 4), uloc=4.0, xmu=2.0, hfmode=False)
+    gs = E.Sector(model, 8, 8)
+    part, hole = E.Sector(model, 9, 8), E.Sector(model, 7, 8)
+    e0, it = C.c_double(), C.c_int()
+    L.check(L.lib().edg_ground_state_keep(gs.handle, None, C.c_uint64(2024), 600, 1e-10, E.EDG_GS_F32_REFINE,
+                                          C.byref(e0), C.byref(it)), "gs")
+    n_up = gs.observables()["dens_up"][0]
+    sp = {}
+    for prec in (E.EDG_PREC_F64, E.EDG_PREC_F32):
+        sp[prec] = (E.gf_chain(gs, part, +1, 1, 1, 150, e0.value, precision=prec),
+                    E.gf_chain(gs, hole, -1, 1, 1, 150, e0.value, precision=prec))
+    p64, h64 = sp[E.EDG_PREC_F64]
+    assert abs(p64.norm2 + h64.norm2 - 1.0) < 1e-12
+    assert abs((p64.norm2 - h64.norm2) - (1.0 - 2.0 * n_up)) < 1e-12
+    wm = np.pi / 50.0 * (2 * np.arange(1, 65) - 1)
+    g = {}
+    for prec, (pa, ho) in sp.items():
+        g[prec] = sum((ch.weight[None, :] / (1j * wm[:, None] - ch.poles[None, :])).sum(1) for ch in (pa, ho))
+    assert np.abs(g[E.EDG_PREC_F32] - g[E.EDG_PREC_F64]).max() <= 1e-5 * np.abs(g[E.EDG_PREC_F64]).max()
+    for s in (gs, part, hole):
+        s.delete()
