@@ -209,8 +209,11 @@ template <typename T>
 int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
                     double* bn_next);
 int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, int do_sqrt);
+// dst = TD(src * scale); dst and src must not overlap (scale_inplace_dev scales in place)
 template <typename TD, typename TS>
 int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale);
+template <typename T>
+int scale_inplace_dev(cudaStream_t st, T* x, int64_t n, double scale);
 template <typename TD>
 int axpy_accum_dev(cudaStream_t st, double* dst, const TD* x, double coef, int64_t n);
 int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed);

@@ -264,7 +264,7 @@ int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A
     set_error("Ritz vector vanished");
     return EDG_ERR_NOCONV;
   }
-  EDG_CHECK((convert_dev<double, double>(st, x, x, n, 1.0 / std::sqrt(nn))));
+  EDG_CHECK((scale_inplace_dev<double>(st, x, n, 1.0 / std::sqrt(nn))));
   return EDG_OK;
 }
 
@@ -280,7 +280,7 @@ int normalise(edg_sector_s* s, double* dv) {
     set_error("start vector has zero norm");
     return EDG_ERR_ARG;
   }
-  return convert_dev<double, double>(s->stream, dv, dv, s->dim, 1.0 / std::sqrt(nn));
+  return scale_inplace_dev<double>(s->stream, dv, s->dim, 1.0 / std::sqrt(nn));
 }
 
 }  // namespace

@@ -220,7 +220,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     set_error("edg_lowest_k: start vector has zero norm");
     return EDG_ERR_ARG;
   }
-  EDG_CHECK((convert_dev<double, double>(st, Q.p, Q.p, n, 1.0 / nrm)));
+  EDG_CHECK((scale_inplace_dev<double>(st, Q.p, n, 1.0 / nrm)));
   std::vector<double> A, B(1, 0.0), cvec(size_t(mmax) + 1), zlast;
   int npass2 = 0;
   double blast = 0.0;

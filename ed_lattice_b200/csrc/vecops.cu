@@ -29,12 +29,28 @@ __device__ __forceinline__ double block_sum(double v) {
   return r;  // valid in thread 0
 }
 
+// Grid-stride loops below take kUnr elements per thread per trip (indices i + u*stride, each
+// coalesced across the warp) with all loads issued before the arithmetic, so that every
+// thread keeps several HBM requests in flight; the order of the partial sums is fixed.
+constexpr int kUnr = 4;
+
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ x, const T* __restrict__ y, int64_t n,
                                                      double* __restrict__ partial) {
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   double s = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    s = __fma_rn(double(x[i]), double(y[i]), s);
+  for (; i + (kUnr - 1) * st < n; i += kUnr * st) {
+    T xa[kUnr], ya[kUnr];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) {
+      xa[u] = x[i + u * st];
+      ya[u] = y[i + u * st];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) s = __fma_rn(double(xa[u]), double(ya[u]), s);
+  }
+  for (; i < n; i += st) s = __fma_rn(double(x[i]), double(y[i]), s);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
@@ -53,8 +69,25 @@ __global__ void __launch_bounds__(kRedThreads) k_step_a(T* __restrict__ w, const
                                                         const T* __restrict__ v, const double* __restrict__ bprev,
                                                         int64_t n, double* __restrict__ partial) {
   const double b = *bprev;
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   double s = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+  for (; i + (kUnr - 1) * st < n; i += kUnr * st) {
+    T wa[kUnr], pa[kUnr], va[kUnr];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) {
+      wa[u] = w[i + u * st];
+      pa[u] = vprev[i + u * st];
+      va[u] = v[i + u * st];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) {
+      const T wt = T(double(wa[u]) - b * double(pa[u]));
+      w[i + u * st] = wt;
+      s = __fma_rn(double(va[u]), double(wt), s);
+    }
+  }
+  for (; i < n; i += st) {
     const T wt = T(double(w[i]) - b * double(vprev[i]));
     w[i] = wt;
     s = __fma_rn(double(v[i]), double(wt), s);
@@ -63,17 +96,39 @@ __global__ void __launch_bounds__(kRedThreads) k_step_a(T* __restrict__ w, const
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// w <- w - coef * x, returning this thread's partial sum of |w|^2
+template <typename T>
+__device__ __forceinline__ double axpy_norm(T* __restrict__ w, const T* __restrict__ x, double coef, int64_t n) {
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  double s = 0.0;
+  for (; i + (kUnr - 1) * st < n; i += kUnr * st) {
+    T wa[kUnr], xa[kUnr];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) {
+      wa[u] = w[i + u * st];
+      xa[u] = x[i + u * st];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) {
+      const T wt = T(double(wa[u]) - coef * double(xa[u]));
+      w[i + u * st] = wt;
+      s = __fma_rn(double(wt), double(wt), s);
+    }
+  }
+  for (; i < n; i += st) {
+    const T wt = T(double(w[i]) - coef * double(x[i]));
+    w[i] = wt;
+    s = __fma_rn(double(wt), double(wt), s);
+  }
+  return s;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_step_b(T* __restrict__ w, const T* __restrict__ v,
                                                         const double* __restrict__ a, int64_t n,
                                                         double* __restrict__ partial) {
-  const double al = *a;
-  double s = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const T wt = T(double(w[i]) - al * double(v[i]));
-    w[i] = wt;
-    s = __fma_rn(double(wt), double(wt), s);
-  }
+  double s = axpy_norm<T>(w, v, *a, n);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
@@ -84,35 +139,68 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_step_b2(T* __restrict__ w, const T* __restrict__ u,
                                                          const double* __restrict__ a, const double* __restrict__ bn,
                                                          int64_t n, double* __restrict__ partial) {
-  const double coef = *a / *bn;
-  double s = 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const T wt = T(double(w[i]) - coef * double(u[i]));
-    w[i] = wt;
-    s = __fma_rn(double(wt), double(wt), s);
-  }
+  double s = axpy_norm<T>(w, u, *a / *bn, n);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// dst[i] = T(src[i] * scale); dst and src do not overlap
+template <typename TD, typename TS>
+__device__ __forceinline__ void scale_copy(TD* __restrict__ dst, const TS* __restrict__ src, int64_t n, double scale) {
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  for (; i + (kUnr - 1) * st < n; i += kUnr * st) {
+    TS xa[kUnr];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) xa[u] = src[i + u * st];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) dst[i + u * st] = TD(double(xa[u]) * scale);
+  }
+  for (; i < n; i += st) dst[i] = TD(double(src[i]) * scale);
 }
 
 template <typename T>
 __global__ void k_scale_into(T* __restrict__ dst, const T* __restrict__ src, const double* __restrict__ b, int64_t n) {
   const double bb = *b;
-  const double inv = bb != 0.0 ? 1.0 / bb : 0.0;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    dst[i] = T(double(src[i]) * inv);
+  scale_copy<T, T>(dst, src, n, bb != 0.0 ? 1.0 / bb : 0.0);
 }
 
 template <typename TD, typename TS>
 __global__ void k_convert(TD* __restrict__ dst, const TS* __restrict__ src, int64_t n, double scale) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    dst[i] = TD(double(src[i]) * scale);
+  scale_copy<TD, TS>(dst, src, n, scale);
+}
+
+// x[i] *= scale in place
+template <typename T>
+__global__ void k_scale_inplace(T* __restrict__ x, int64_t n, double scale) {
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  for (; i + (kUnr - 1) * st < n; i += kUnr * st) {
+    T xa[kUnr];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) xa[u] = x[i + u * st];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) x[i + u * st] = T(double(xa[u]) * scale);
+  }
+  for (; i < n; i += st) x[i] = T(double(x[i]) * scale);
 }
 
 template <typename TS>
 __global__ void k_axpy_accum(double* __restrict__ dst, const TS* __restrict__ x, double coef, int64_t n) {
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    dst[i] = __fma_rn(coef, double(x[i]), dst[i]);
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
+  for (; i + (kUnr - 1) * st < n; i += kUnr * st) {
+    double da[kUnr];
+    TS xa[kUnr];
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) {
+      da[u] = dst[i + u * st];
+      xa[u] = x[i + u * st];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnr; ++u) dst[i + u * st] = __fma_rn(coef, double(xa[u]), da[u]);
+  }
+  for (; i < n; i += st) dst[i] = __fma_rn(coef, double(x[i]), dst[i]);
 }
 
 // x[i] = sum_j z[j] * basis[j][i] in one pass over the stored FP32 Lanczos basis (z in FP64,
@@ -205,6 +293,15 @@ int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
+
+template <typename T>
+int scale_inplace_dev(cudaStream_t st, T* x, int64_t n, double scale) {
+  k_scale_inplace<T><<<grid_for(n), 256, 0, st>>>(x, n, scale);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+template int scale_inplace_dev<double>(cudaStream_t, double*, int64_t, double);
+template int scale_inplace_dev<float>(cudaStream_t, float*, int64_t, double);
 
 template <typename TS>
 int axpy_accum_dev(cudaStream_t st, double* dst, const TS* x, double coef, int64_t n) {

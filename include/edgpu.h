@@ -217,9 +217,11 @@ int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qc
 int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* poles,
                  double* weights, double* norm2, int* nout);
 
-/* Batched chains: k start vectors in one sector run as block H x V in a single recurrence
- * (one alpha/beta pair per column). dvinit: k device vectors, column c at dvinit + c*dim.
- * alanc/blanc/norm2: [k][nlanc] row-major per column; nsteps[k]. */
+/* Batched chains: k start vectors of one sector in one call, each tridiagonalised as by
+ * edg_tridiag_dev_f64 (one alpha/beta sequence per column). The chains run one after
+ * another, each H x v using the whole GPU; a block H x V over several vectors would gather
+ * the same bytes per vector, so it is not used. dvinit: k device vectors, column c at
+ * dvinit + c*dim. alanc/blanc/norm2: [k][nlanc] row-major per column; nsteps[k]. */
 int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc, double threshold,
                           int precision, double* alanc, double* blanc, double* norm2, int* nsteps);
 
