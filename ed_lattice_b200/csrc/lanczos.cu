@@ -20,6 +20,7 @@
 // the host once per step (16 bytes) for the convergence test.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -69,18 +70,34 @@ struct Recurrence {
   T* W = nullptr;  // output of the step
   bool fused = false;
   std::vector<double> bn_host;  // norms of u_j (fused); 1 for the general form
+  // Basis columns used as the recurrence's own vectors (fused form): u_j is written straight
+  // into column j, so keeping the basis costs no copy. Column j then holds u_j, i.e.
+  // v_j / vscale(j). Past the last column the three work vectors take over.
+  T* ext = nullptr;
+  int ext_cols = 0;
+  T* wbuf[3] = {nullptr, nullptr, nullptr};
 
-  // v_0 = dv0 * scale; cap = most steps this run will take
-  int init(edg_sector_s* sec, const double* dv0, double scale, int cap) {
+  // v_0 = dv0 * scale; cap = most steps this run will take; basis (optional): ncols device
+  // columns of dim elements that receive u_0, u_1, ... (fused form only)
+  int init(edg_sector_s* sec, const double* dv0, double scale, int cap, T* basis = nullptr, int ncols = 0) {
     s = sec;
     const int64_t n = s->dim;
     EDG_CHECK(scalars(s, cap, &sc));
     DevBuf<T>* wb = work<T>(s);
-    for (int k = 0; k < 3; ++k) EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
+    for (int k = 0; k < 3; ++k) {
+      EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
+      wbuf[k] = wb[k].p;
+    }
     U = wb[0].p;
     P = wb[1].p;
     W = wb[2].p;
     fused = hxv_lz_available(s, sizeof(T));
+    if (fused && basis && ncols >= 2) {
+      ext = basis;
+      ext_cols = ncols;
+      U = ext;
+      W = ext + n;
+    }
     EDG_CHECK((convert_dev<T, double>(s->stream, U, dv0, n, scale)));
     EDG_CUDA(cudaMemsetAsync(P, 0, n * sizeof(T), s->stream));
     bn_host.assign(1, 1.0);
@@ -116,7 +133,13 @@ struct Recurrence {
       T* t = P;
       P = U;
       U = W;
-      W = t;
+      if (ext && j + 2 < ext_cols) {
+        W = ext + size_t(j + 2) * s->dim;
+      } else if (ext) {  // out of basis columns: a work vector that is neither P nor U
+        W = wbuf[0] != P && wbuf[0] != U ? wbuf[0] : (wbuf[1] != P && wbuf[1] != U ? wbuf[1] : wbuf[2]);
+      } else {
+        W = t;
+      }
       bn_host.push_back(b);
     } else {
       EDG_CHECK(scale_into<T>(s->stream, P, W, sc.b + j + 1, s->dim));
@@ -190,17 +213,25 @@ Ritz lowest_ritz(const std::vector<double>& a, const std::vector<double>& b, dou
 // the normalised basis vectors in FP32 so the Ritz vector needs no second pass.
 template <typename T>
 int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vector<double>* A,
-           std::vector<double>* B, float* basis, int basis_cols, double* e0) {
+           std::vector<double>* B, float* basis, int basis_cols, std::vector<double>* colscale, double* e0) {
   const int64_t n = s->dim;
   cudaStream_t st = s->stream;
   Recurrence<T> R;
-  EDG_CHECK(R.init(s, dv0, 1.0, maxit + 1));
+  T* own = std::is_same<T, float>::value ? reinterpret_cast<T*>(basis) : nullptr;
+  EDG_CHECK(R.init(s, dv0, 1.0, maxit + 1, own, own ? basis_cols : 0));
   A->clear();
   B->assign(1, 0.0);
+  colscale->clear();
   double eold = 0.0;
   for (int j = 0; j < maxit; ++j) {
-    if (basis && j < basis_cols)
-      EDG_CHECK((convert_dev<float, T>(st, basis + size_t(j) * n, R.U, n, R.vscale(j))));
+    if (basis && j < basis_cols) {
+      if (R.ext) {
+        colscale->push_back(R.vscale(j));  // column j holds u_j = v_j / vscale(j)
+      } else {
+        EDG_CHECK((convert_dev<float, T>(st, basis + size_t(j) * n, R.U, n, R.vscale(j))));
+        colscale->push_back(1.0);
+      }
+    }
     double a, b;
     EDG_CHECK(R.step(j, &a, &b));
     if (!std::isfinite(a) || !std::isfinite(b)) {
@@ -228,15 +259,17 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
 // from the stored FP32 basis when present, else by replaying the recurrence from dv0.
 template <typename T>
 int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A, const std::vector<double>& B,
-                const float* basis, int basis_cols, double* x) {
+                const float* basis, int basis_cols, const std::vector<double>& colscale, double* x) {
   const int64_t n = s->dim;
   cudaStream_t st = s->stream;
   const int m = int(A.size());
   std::vector<double> w(m), Z(size_t(m) * m);
   EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), w.data(), nullptr, Z.data()));
   EDG_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), st));
-  if (basis && basis_cols >= m) {
-    // one pass over the stored columns (same FMA order as m successive axpys)
+  if (basis && basis_cols >= m && int(colscale.size()) >= m) {
+    // one pass over the stored columns (same FMA order as m successive axpys); column j
+    // holds v_j / colscale[j]
+    for (int j = 0; j < m; ++j) Z[j] *= colscale[j];
     Scalars scz;
     EDG_CHECK(scalars(s, m + 1, &scz));
     EDG_CUDA(cudaMemcpyAsync(scz.a, Z.data(), size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -306,17 +339,17 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
     EDG_CHECK(random_dev(st, x0, n, seed));
   }
   EDG_CHECK(normalise(s, x0));
-  std::vector<double> A, B;
+  std::vector<double> A, B, cs;
   *niter = 0;
   s->last_n32 = s->last_n64 = 0;
   s->has_state = false;
   const bool want_vec = !(mode & EDG_GS_E0_ONLY);
   mode &= 0xff;
   if (mode == EDG_GS_F64) {
-    EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, e0));
+    EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, &cs, e0));
     s->last_n64 += int(A.size());
     if (want_vec) {
-      EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, s->state.p));
+      EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, cs, s->state.p));
       s->last_n64 += int(A.size()) - 1;
     }
   } else {
@@ -342,16 +375,16 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
     // FP32 phase: stop once the lowest Ritz value settles at FP32 resolution
     const double tol32 = tol > 2e-7 ? tol : 2e-7;
     double e32 = 0.0;
-    EDG_CHECK(gs_run<float>(s, x0, maxit, tol32, &A, &B, s->basis32.p, cols, &e32));
+    EDG_CHECK(gs_run<float>(s, x0, maxit, tol32, &A, &B, s->basis32.p, cols, &cs, &e32));
     s->last_n32 += int(A.size());
-    EDG_CHECK(ritz_vector<float>(s, x0, A, B, s->basis32.p, cols, s->state.p));
+    EDG_CHECK(ritz_vector<float>(s, x0, A, B, s->basis32.p, cols, cs, s->state.p));
     if (cols < int(A.size())) s->last_n32 += int(A.size()) - 1;
     // phase 2: restarted FP64 Lanczos from the FP32 Ritz vector
     EDG_CUDA(cudaMemcpyAsync(x0, s->state.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-    EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, e0));
+    EDG_CHECK(gs_run<double>(s, x0, maxit, tol, &A, &B, nullptr, 0, &cs, e0));
     s->last_n64 += int(A.size());
     if (want_vec) {
-      EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, s->state.p));
+      EDG_CHECK(ritz_vector<double>(s, x0, A, B, nullptr, 0, cs, s->state.p));
       s->last_n64 += int(A.size()) - 1;
     }
   }

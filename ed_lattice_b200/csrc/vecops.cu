@@ -10,6 +10,8 @@
 // one-block pass in fixed order, so results are bit-reproducible run to run.
 // Scalars (a, b) live in device memory and are read by the next kernel: no host round trip
 // is needed between the passes.
+#include <cstdint>
+
 #include "common.cuh"
 
 namespace edg {
@@ -122,6 +124,106 @@ __device__ __forceinline__ double axpy_norm(T* __restrict__ w, const T* __restri
     s = __fma_rn(double(wt), double(wt), s);
   }
   return s;
+}
+
+// 16-byte vector forms (float4 / double2) for arrays whose length is a multiple of K and
+// whose pointers are 16-byte aligned: four times the bytes in flight per load instruction.
+template <typename T>
+struct V16;
+template <>
+struct V16<float> {
+  using type = float4;
+  static constexpr int K = 4;
+};
+template <>
+struct V16<double> {
+  using type = double2;
+  static constexpr int K = 2;
+};
+
+template <typename T>
+__device__ __forceinline__ double axpy_norm_v(T* __restrict__ w, const T* __restrict__ x, double coef, int64_t nv) {
+  using V = typename V16<T>::type;
+  constexpr int K = V16<T>::K;
+  V* __restrict__ wv = reinterpret_cast<V*>(w);
+  const V* __restrict__ xv = reinterpret_cast<const V*>(x);
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += 2 * st) {
+    V wa[2], xa[2];
+    const bool two = i + st < nv;
+    wa[0] = wv[i];
+    xa[0] = xv[i];
+    if (two) {
+      wa[1] = wv[i + st];
+      xa[1] = xv[i + st];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (u == 1 && !two) break;
+      T* pw = reinterpret_cast<T*>(&wa[u]);
+      const T* px = reinterpret_cast<const T*>(&xa[u]);
+#pragma unroll
+      for (int c = 0; c < K; ++c) {
+        pw[c] = T(double(pw[c]) - coef * double(px[c]));
+        s = __fma_rn(double(pw[c]), double(pw[c]), s);
+      }
+      wv[i + u * st] = wa[u];
+    }
+  }
+  return s;
+}
+
+template <typename T>
+__device__ __forceinline__ double dot_v(const T* __restrict__ x, const T* __restrict__ y, int64_t nv) {
+  using V = typename V16<T>::type;
+  constexpr int K = V16<T>::K;
+  const V* __restrict__ xv = reinterpret_cast<const V*>(x);
+  const V* __restrict__ yv = reinterpret_cast<const V*>(y);
+  const int64_t st = int64_t(gridDim.x) * blockDim.x;
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < nv; i += 2 * st) {
+    V xa[2], ya[2];
+    const bool two = i + st < nv;
+    xa[0] = xv[i];
+    ya[0] = yv[i];
+    if (two) {
+      xa[1] = xv[i + st];
+      ya[1] = yv[i + st];
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (u == 1 && !two) break;
+      const T* px = reinterpret_cast<const T*>(&xa[u]);
+      const T* py = reinterpret_cast<const T*>(&ya[u]);
+#pragma unroll
+      for (int c = 0; c < K; ++c) s = __fma_rn(double(px[c]), double(py[c]), s);
+    }
+  }
+  return s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dot_v(const T* __restrict__ x, const T* __restrict__ y, int64_t nv,
+                                                       double* __restrict__ partial) {
+  double s = dot_v<T>(x, y, nv);
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_step_b2_v(T* __restrict__ w, const T* __restrict__ u,
+                                                           const double* __restrict__ a,
+                                                           const double* __restrict__ bn, int64_t nv,
+                                                           double* __restrict__ partial) {
+  double s = axpy_norm_v<T>(w, u, *a / *bn, nv);
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+template <typename T>
+bool vec16_ok(int64_t n, const void* p, const void* q) {
+  return n % V16<T>::K == 0 && (reinterpret_cast<uintptr_t>(p) % 16) == 0 && (reinterpret_cast<uintptr_t>(q) % 16) == 0;
 }
 
 template <typename T>
@@ -242,7 +344,10 @@ uint64_t splitmix64(uint64_t x) { return splitmix64_d(x); }
 
 template <typename T>
 int dot_dev(cudaStream_t st, const T* x, const T* y, int64_t n, double* partial, double* out) {
-  k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n, partial);
+  if (vec16_ok<T>(n, x, y))
+    k_dot_v<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n / V16<T>::K, partial);
+  else
+    k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n, partial);
   k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, out, 0);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
@@ -268,7 +373,10 @@ int lanczos_step_b(cudaStream_t st, T* w, const T* v, const double* a, int64_t n
 template <typename T>
 int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
                     double* bn_next) {
-  k_step_b2<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n, partial);
+  if (vec16_ok<T>(n, w, u))
+    k_step_b2_v<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n / V16<T>::K, partial);
+  else
+    k_step_b2<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n, partial);
   k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, bn_next, 1);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
