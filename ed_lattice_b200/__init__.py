@@ -10,13 +10,13 @@ from .edlat import (Hij, Model, Sector, Spectrum, chi_chain, drude_weight, eval_
                     grids, oc_chain, poles_weights, random_vector, read_gfmatrix, ring, sp_lanc_eigh, square_lattice,
                     tridiag_eigh, tridiag_Hv_sector, write_gfmatrix)
 
-from .diag import DiagParams, StateList, diagonalize_lattice, lanc_observables, partition_function
+from .diag import DiagParams, StateList, diagonalize_lattice, lanc_energy, lanc_observables, partition_function
 
 lib()  # load now: a missing or broken libedgpu.so fails the import
 
 __all__ = [
     "EDG_FORM_DIRECT", "EDG_FORM_STORED", "EDG_GS_E0_ONLY", "EDG_GS_F32_REFINE", "EDG_GS_F64", "EDG_PREC_F32",
-    "EDG_PREC_F64", "DiagParams", "EdgError", "Hij", "StateList", "diagonalize_lattice", "lanc_observables",
+    "EDG_PREC_F64", "DiagParams", "EdgError", "Hij", "StateList", "diagonalize_lattice", "lanc_energy", "lanc_observables",
     "partition_function", "Model", "Sector", "Spectrum", "chi_chain", "drude_weight", "eval_chi",
     "eval_gf", "eval_oc", "gf_chain", "grids", "oc_chain", "poles_weights", "random_vector", "read_gfmatrix", "ring",
     "sp_lanc_eigh", "square_lattice", "tridiag_eigh", "tridiag_Hv_sector", "write_gfmatrix",

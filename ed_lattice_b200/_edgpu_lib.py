@@ -76,6 +76,7 @@ SIGNATURES = {
     "edg_apply_diagop_dev_f64": (_i, [_p, _i, _i, _i, _pd, _p, _p]),
     "edg_apply_current_dev_f64": (_i, [_p, _p, _p]),
     "edg_observables": (_i, [_p, _d, _pd, _pd, _pd, _pd, _pd]),
+    "edg_energy": (_i, [_p, _d, _pd, _pd, _pd, _pd]),
     "edg_gf_chain": (_i, [_p, _p, _i, _i, _i, _i, _i, _i, _d, _pd, _pd, _pd, _pi]),
     "edg_chi_chain": (_i, [_p, _i, _i, _i, _pd, _i, _i, _d, _pd, _pd, _pd, _pi]),
     "edg_oc_chain": (_i, [_p, _i, _i, _d, _pd, _pd, _pd, _pi]),

@@ -16,6 +16,8 @@ int apply_cop(const edg_sector_s* from, const edg_sector_s* to, int op, int site
 int apply_diagop(const edg_sector_s* s, int kind, const double* wsite, const double* din, double* dout,
                  cudaStream_t st);
 int apply_current(const edg_sector_s* s, const double* din, double* dout, cudaStream_t st);
+int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, double* epot, double* eknot,
+           double* ehartree);
 int observables(const edg_sector_s* s, const double* psi, double weight, double* dens, double* dens_up,
                 double* dens_dw, double* docc, double* magz, cudaStream_t st);
 }  // namespace edg
@@ -437,6 +439,17 @@ int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* do
   EDG_ARG(din && dout && din != dout, "edg_apply_current: bad vectors");
   EDG_CHECK(ensure_device(s));
   return apply_current(s, din, dout, s->stream);
+}
+
+int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double* eknot, double* ehartree) {
+  EDG_CHECK(check_sector(s));
+  if (!s->has_state) {
+    set_error("edg_energy: the sector holds no state");
+    return EDG_ERR_STATE;
+  }
+  EDG_ARG(std::isfinite(weight), "edg_energy: weight is not finite");
+  EDG_CHECK(ensure_device(s));
+  return energy(s, s->state.p, weight, ekin, epot, eknot, ehartree);
 }
 
 int edg_observables(const edg_sector* s, double weight, double* dens, double* dens_up, double* dens_dw, double* docc,

@@ -198,6 +198,30 @@ __global__ void __launch_bounds__(256) k_obs_rows(const double* __restrict__ psi
 
 int grid_rows(int64_t rows) { return int(rows < 148 * 8 ? (rows < 1 ? 1 : rows) : 148 * 8); }
 
+// Partial sums of psi_i^2 diag(H)_i with diag(H)_i = E_up[iup] + E_dw[idw] + U popc(up & dw),
+// the diagonal the H x v applies; fixed grid and order (deterministic).
+constexpr int kDiagBlocks = 592;
+__global__ void __launch_bounds__(256) k_diag_dot(const double* __restrict__ psi, int64_t dup, int64_t n,
+                                                  const double* __restrict__ eup, const double* __restrict__ edw,
+                                                  const uint32_t* __restrict__ mup, const uint32_t* __restrict__ mdw,
+                                                  double U, double* __restrict__ partial) {
+  __shared__ double sh[8];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t idw = i / dup, iup = i - idw * dup;
+    const double d = eup[iup] + edw[idw] + U * double(__popc(mup[iup] & mdw[idw]));
+    s = __fma_rn(psi[i] * psi[i], d, s);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += sh[w];
+    partial[blockIdx.x] = t;
+  }
+}
+
 }  // namespace
 
 int apply_cop(const edg_sector_s* from, const edg_sector_s* to, int op, int site, int spin, double coef,
@@ -289,6 +313,46 @@ int observables(const edg_sector_s* s, const double* psi, double weight, double*
     if (docc) docc[i] += weight * dd;
     if (magz) magz[i] += weight * (u - d);
   }
+  return EDG_OK;
+}
+
+// lanc_energy (src/ENERGY.f90:118-226, Norb=1 terms) for one state:
+//  ekin = <psi|H|psi> - <psi|diag(H)|psi> (the off-diagonal part is exactly the hopping),
+//  eknot from the Hij diagonal and the site densities, epot = U sum_i docc_i plus the Hartree
+//  term -U/2 sum_i n_i when HFMODE (reported also on its own, as ENERGY.f90:343 adds it).
+int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, double* epot, double* eknot,
+           double* ehartree) {
+  const int ns = s->model.ns;
+  const int64_t n = s->dim;
+  cudaStream_t st = s->stream;
+  std::vector<double> dens(ns, 0.0), nup(ns, 0.0), ndw(ns, 0.0), docc(ns, 0.0);
+  EDG_CHECK(observables(s, psi, 1.0, dens.data(), nup.data(), ndw.data(), docc.data(), nullptr, st));
+  EDG_CHECK(s->w64[0].alloc(n, "energy work vector"));
+  double* hv = s->w64[0].p;
+  EDG_CHECK(hxv_apply<double>(s, psi, hv));
+  DevBuf<double> part;
+  EDG_CHECK(part.alloc(size_t(kRedBlocks) + kDiagBlocks + 4, "energy partials"));
+  double* out = part.p + kRedBlocks + kDiagBlocks;
+  EDG_CHECK(dot_dev<double>(st, psi, hv, n, part.p, out));
+  k_diag_dot<<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, n, s->up.e64.p, s->dw.e64.p, s->up.map.p, s->dw.map.p,
+                                          s->U, part.p + kRedBlocks);
+  EDG_CUDA(cudaGetLastError());
+  EDG_CHECK(finish_dev(st, part.p + kRedBlocks, kDiagBlocks, out + 1, 0));
+  double h[2] = {0.0, 0.0};
+  EDG_CUDA(cudaMemcpyAsync(h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  const std::vector<double>& h1 = s->model.hre[0];
+  const std::vector<double>& h2 = s->model.nspin == 2 ? s->model.hre[1] : s->model.hre[0];
+  double kn = 0.0, ep = 0.0, eh = 0.0;
+  for (int i = 0; i < ns; ++i) {
+    kn += h1[size_t(i) * ns + i] * nup[i] + h2[size_t(i) * ns + i] * ndw[i];
+    ep += s->model.uloc * docc[i];
+    if (s->model.hfmode) eh -= 0.5 * s->model.uloc * dens[i];
+  }
+  if (ekin) *ekin += weight * (h[0] - h[1]);
+  if (eknot) *eknot += weight * kn;
+  if (epot) *epot += weight * (ep + eh);
+  if (ehartree) *ehartree += weight * eh;
   return EDG_OK;
 }
 

@@ -6,6 +6,7 @@
     diagonalize_lattice  ed_diag_d (src/DIAG/DIAG.f90:103-332)
     partition_function   partition_function_lattice (src/DIAG/DIAG.f90:52-92)
     lanc_observables     lanc_observables (src/OBSERVABLES.f90:78-192)
+    lanc_energy          lanc_energy (src/ENERGY.f90:76-356), Norb=1 terms
 
 The eigenpairs of each sector come from the device: edg_lowest_k for the sp_eigh (ARPACK)
 branch, edg_ground_state for lanc_method="lanczos", and for dim <= lanc_dim_threshold the dense
@@ -361,3 +362,42 @@ def lanc_observables(model: Model, state_list: StateList, zeta: float, params: D
     out = _allreduce_sum(out, comm)
     out["mag"] = out["dens_up"] - out["dens_dw"]
     return out
+
+
+def lanc_energy(model: Model, state_list: StateList, zeta: float, params: DiagParams, energy_fn=None,
+                comm=None) -> dict:
+    """Thermal ed_Ekin, ed_Epot (Hartree term included, as src/ENERGY.f90:343), ed_Eknot and
+    ed_Ehartree over the trimmed list with weights exp(-(E-Egs)/T)/Z (1/Z at T=0)
+    (src/ENERGY.f90:76-356, Norb=1 terms). `energy_fn(model, isector, vec, weight)` returns the
+    weighted dict of one state; the default loads the state into the device sector and runs
+    edg_energy. With `comm`, each rank adds the states it owns and the sums are all-reduced."""
+    rank, _ = _rank_world(comm)
+    egs = state_list.emin
+    n = state_list.trim_size(params.temp, params.cutoff, params.finite_temp)
+    out = {k: np.zeros(1) for k in ("ekin", "epot", "eknot", "ehartree")}
+    sectors: dict[int, Sector] = {}
+    try:
+        for istate in range(1, n + 1):
+            st = state_list.states[istate - 1]
+            if st.owner != rank:
+                continue
+            bw = math.exp(-(st.e - egs) / params.temp) if params.finite_temp else 1.0
+            bw /= zeta
+            if st.vec is None:
+                raise L.EdgError(L.EDG_ERR_STATE, "lanc_energy", "state list holds no vectors")
+            if energy_fn is not None:
+                en = energy_fn(model, st.sector, st.vec, bw)
+            else:
+                sec = sectors.get(st.sector)
+                if sec is None:
+                    sec = sectors[st.sector] = Sector.from_index(model, st.sector)
+                sec.set_state(np.real(st.vec))
+                en = sec.energy(bw)
+            for k in out:
+                out[k] += en[k]
+    finally:
+        for sec in sectors.values():
+            sec.delete()
+    out = _allreduce_sum(out, comm)
+    return {k: float(v[0]) for k, v in out.items()}
+

@@ -263,6 +263,14 @@ class Sector:
         return out
 
 
+    def energy(self, weight: float = 1.0) -> dict:
+        """lanc_energy's Norb=1 terms for the stored state (src/ENERGY.f90:118-226):
+        ekin, epot (Hartree term included), eknot, ehartree, each times weight."""
+        out = [C.c_double(0.0) for _ in range(4)]
+        L.check(L.lib().edg_energy(self.handle, weight, *[C.byref(x) for x in out]), "lanc_energy")
+        return dict(zip(("ekin", "epot", "eknot", "ehartree"), (x.value for x in out)))
+
+
 # ----------------------------------------------------------------------------- Lanczos
 def random_vector(seed: int, n: int) -> np.ndarray:
     out = np.empty(n)

@@ -199,6 +199,16 @@ int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* do
 int edg_observables(const edg_sector* s, double weight, double* dens, double* dens_up,
                     double* dens_dw, double* docc, double* magz);
 
+/* Energies of the state buffer: the Norb=1 terms of lanc_energy (src/ENERGY.f90:118-226).
+ * ekin = <psi|hopping|psi> (off-diagonal Hij of both spins), eknot = sum_i Hij(i,i) <n_i>
+ * per spin, epot = U sum_i <n_i,up n_i,dw> + ehartree, ehartree = -U/2 sum_i <n_i> when
+ * HFMODE (else 0; ENERGY.f90:343 folds it into ed_Epot the same way). Each is scaled by
+ * weight and ADDED to its output (NULL outputs are skipped), as edg_observables does, so a
+ * caller sums Boltzmann-weighted states. One FP64 H x v of the state. The OC Drude weight
+ * (src/OC/OC_FUNCTIONS.f90:65) takes ekin from here. */
+int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double* eknot,
+               double* ehartree);
+
 /* ------------------------------------------------------------------ response functions
  * One Lanczos chain per excitation, as built by the GF/CHI/OC builders:
  *  edg_gf_chain: c^+ (op=+1) or c (op=-1) on the state buffer of `from`, tridiagonalised in

@@ -833,6 +833,51 @@ void orc_observables_d(int ns, int nup, int ndw, const double* psi, double bw, d
   }
 }
 
+// lanc_energy inner loop (src/ENERGY.f90:118-180 and :196-226, Norb=1 terms) for one real
+// state with boltzman_weight/zeta folded into bw, accumulated into the outputs:
+//  eknot    += sum_io Hdiag(spin,io) n_io           (ENERGY.f90:142-145)
+//  ekin     += Hij(io,jo) sg1 sg2 psi(i) psi(j)      (up and down hops, :147-180)
+//  epot     += Uloc n_up n_dw per site               (:182-188)
+//  ehartree -= 0.5 Uloc (n_up + n_dw) when HFMODE    (:213-219)
+// The caller adds ehartree to epot as ENERGY.f90:343 does.
+void orc_energy_d(const orc_model* m, int nup, int ndw, const double* psi, double bw, double* ekin, double* epot,
+                  double* eknot, double* ehartree) {
+  const int ns = m->ns;
+  Sector S; make_sector(ns, nup, ndw, &S);
+  for (int64_t i = 0; i < S.dim; ++i) {
+    const int64_t iup = i % S.dimup, idw = i / S.dimup;
+    const int64_t mup = S.mup[iup], mdw = S.mdw[idw];
+    const double sw = psi[i] * psi[i];
+    for (int io = 0; io < ns; ++io) {
+      *eknot += hij(m, 1, io, io).real() * btest(mup, io) * bw * sw;
+      *eknot += hij(m, 2, io, io).real() * btest(mdw, io) * bw * sw;
+    }
+    for (int io = 0; io < ns; ++io)
+      for (int jo = 0; jo < ns; ++jo) {
+        if (hij(m, 1, io, jo) == zc(0.0) || !btest(mup, jo) || btest(mup, io)) continue;
+        int64_t k1, k2; double sg1, sg2;
+        op_c(jo, mup, &k1, &sg1);
+        op_cdg(io, k1, &k2, &sg2);
+        const int64_t jup = bsearch_rec(S.mup.data(), S.dimup, k2);
+        const int64_t j = (jup - 1) + idw * S.dimup;
+        *ekin += hij(m, 1, io, jo).real() * sg1 * sg2 * psi[i] * psi[j] * bw;
+      }
+    for (int io = 0; io < ns; ++io)
+      for (int jo = 0; jo < ns; ++jo) {
+        if (hij(m, 2, io, jo) == zc(0.0) || !btest(mdw, jo) || btest(mdw, io)) continue;
+        int64_t k1, k2; double sg1, sg2;
+        op_c(jo, mdw, &k1, &sg1);
+        op_cdg(io, k1, &k2, &sg2);
+        const int64_t jdw = bsearch_rec(S.mdw.data(), S.dimdw, k2);
+        const int64_t j = iup + (jdw - 1) * S.dimup;
+        *ekin += hij(m, 2, io, jo).real() * sg1 * sg2 * psi[i] * psi[j] * bw;
+      }
+    for (int io = 0; io < ns; ++io) *epot += m->uloc * btest(mup, io) * btest(mdw, io) * bw * sw;
+    if (m->hfmode)
+      for (int io = 0; io < ns; ++io) *ehartree -= 0.5 * m->uloc * (btest(mup, io) + btest(mdw, io)) * bw * sw;
+  }
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

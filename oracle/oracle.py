@@ -60,6 +60,7 @@ _SIG = {
     "orc_apply_current_d": (None, [_p, _i, _i, _p, _p]),
     "orc_poles_weights": (None, [_i, _p, _p, _d, _d, _i, _p, _p]),
     "orc_observables_d": (None, [_i, _i, _i, _p, _d, _p, _p, _p, _p, _p]),
+    "orc_energy_d": (None, [_p, _i, _i, _p, _d, _p, _p, _p, _p]),
     "orc_num_threads": (_i, []),
 }
 
@@ -262,6 +263,15 @@ def observables(ns, nup, ndw, psi, bw=1.0):
     lib().orc_observables_d(ns, nup, ndw, _ptr(psi), bw, _ptr(out["dens"]), _ptr(out["dens_up"]),
                             _ptr(out["dens_dw"]), _ptr(out["docc"]), _ptr(out["magz"]))
     return out
+
+
+def energy(m: Model, nup, ndw, psi, bw=1.0):
+    """lanc_energy's Norb=1 terms for one real state: (ekin, epot incl. ehartree, eknot, ehartree)."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    out = [C.c_double(0.0) for _ in range(4)]
+    lib().orc_energy_d(m.ref, nup, ndw, _ptr(psi), bw, *[C.byref(x) for x in out])
+    ekin, epot, eknot, ehartree = (x.value for x in out)
+    return ekin, epot + ehartree, eknot, ehartree
 
 
 def num_threads() -> int:

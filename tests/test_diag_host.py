@@ -144,3 +144,27 @@ def test_filling_restricts_sectors():
     sl, eigs = diagonalize_lattice(m, p, solver=_oracle_solver(om))
     assert len(eigs) == 5  # (0,4) (1,3) (2,2) (3,1) (4,0)
     assert all(m.get_nup(s.sector) + m.get_ndw(s.sector) == 4 for s in sl.states)
+
+
+def test_thermal_energy_identity():
+    """lanc_energy over the state list with the oracle's per-state energies: the thermal
+    <H> = Ekin + Epot + Eknot - xmu <N> equals sum_i p_i E_i."""
+    from ed_lattice_b200.diag import lanc_energy
+    H = _chain4()
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=True)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=True)
+    p = DiagParams(finite_temp=True, temp=0.5, lanc_nstates_sector=36)
+    sl, _ = diagonalize_lattice(m, p, solver=_oracle_solver(om))
+    zeta = partition_function(sl, p)
+
+    def energy_fn(model, isector, vec, bw):
+        ek, ep, ekn, eh = O.energy(om, model.get_nup(isector), model.get_ndw(isector), vec, bw)
+        return {"ekin": ek, "epot": ep, "eknot": ekn, "ehartree": eh}
+
+    en = lanc_energy(m, sl, zeta, p, energy_fn=energy_fn)
+    obs = lanc_observables(m, sl, zeta, p, observer=_oracle_observer)
+    egs = sl.emin
+    n = sl.trimd_size
+    h_avg = sum(math.exp(-(sl.energy(i) - egs) / p.temp) * sl.energy(i) for i in range(1, n + 1)) / zeta
+    assert en["ekin"] + en["epot"] + en["eknot"] - 2.0 * obs["dens"].sum() == pytest.approx(h_avg, abs=1e-12)
+    assert en["ehartree"] == pytest.approx(-0.5 * 4.0 * obs["dens"].sum(), abs=1e-12)

@@ -85,6 +85,8 @@ def test_gf_chains_config3_size():
     L.check(L.lib().edg_ground_state_keep(gs.handle, None, C.c_uint64(2024), 600, 1e-10, E.EDG_GS_F32_REFINE,
                                           C.byref(e0), C.byref(it)), "gs")
     n_up = gs.observables()["dens_up"][0]
+    en = gs.energy()  # E0 = Ekin + Epot + Eknot - xmu N at full size (16 electrons, XMU=2)
+    assert abs(en["ekin"] + en["epot"] + en["eknot"] - 2.0 * 16 - e0.value) <= 1e-9 * abs(e0.value)
     sp = {}
     for prec in (E.EDG_PREC_F64, E.EDG_PREC_F32):
         sp[prec] = (E.gf_chain(gs, part, +1, 1, 1, 150, e0.value, precision=prec),

@@ -372,3 +372,26 @@ def test_observables_vs_oracle():
     ref = O.observables(12, 5, 4, psi, 0.5)
     for k in ("dens", "dens_up", "dens_dw", "docc", "magz"):
         assert np.allclose(obs[k], ref[k], atol=1e-13), k
+
+
+@pytest.mark.parametrize("hfmode", [False, True])
+@pytest.mark.parametrize("form", [E.EDG_FORM_STORED, E.EDG_FORM_DIRECT])
+def test_energy_vs_oracle(hfmode, form):
+    """edg_energy against the oracle's restatement of lanc_energy's loops, on a normalised
+    random state of the disordered 3x4 sector (5,3) with weight 0.7 (1e-12 relative), and the
+    terms of the device ground state adding up to E0."""
+    h = square_lattice(3, 4)
+    h[np.diag_indices(12)] = disorder(12, 3)
+    gm, om = models(h, uloc=4.0, xmu=2.0, hfmode=hfmode)
+    s = E.Sector(gm, 5, 3, form)
+    v = O.random_vector(31, s.dim)
+    v /= np.linalg.norm(v)
+    s.set_state(v)
+    en = s.energy(0.7)
+    ekin, epot, eknot, eh = O.energy(om, 5, 3, v, 0.7)
+    for got, ref in ((en["ekin"], ekin), (en["epot"], epot), (en["eknot"], eknot), (en["ehartree"], eh)):
+        assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref))
+    e0, _, _ = E.sp_lanc_eigh(s, seed=5, maxit=400, tol=1e-13)
+    en = s.energy()
+    assert abs(en["ekin"] + en["epot"] + en["eknot"] - 2.0 * 8 - e0) <= 1e-10 * abs(e0)
+    s.delete()

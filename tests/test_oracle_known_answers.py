@@ -226,3 +226,21 @@ def test_golden_fixtures_reproduce():
     rp, c, v = O.hop_csr(m2, 1, 3)
     assert np.array_equal(rp, g2["rp_up"]) and np.array_equal(c, g2["c_up"]) and np.array_equal(v, g2["v_up"])
     assert np.array_equal(O.Stored(m2, 3, 2).matvec_d(g2["v0"]), g2["hv"])
+
+
+@pytest.mark.parametrize("hfmode", [False, True])
+def test_energy_terms_add_up_to_e0(hfmode):
+    """lanc_energy's terms of an eigenstate rebuild its energy: E = Ekin + Epot + Eknot - xmu N
+    (Epot includes the Hartree term), on a disordered 6-ring; U=0 gives Epot = Ehartree."""
+    rng = np.random.default_rng(1)
+    H = ring(6).astype(float)
+    H[np.diag_indices(6)] = rng.uniform(-1, 1, 6)
+    for u in (3.0, 0.0):
+        m = O.Model(H, uloc=u, xmu=1.2, hfmode=hfmode)
+        w, z = np.linalg.eigh(O.dense_h(m, 3, 2))
+        for k in (0, 3):
+            ekin, epot, eknot, eh = O.energy(m, 3, 2, z[:, k])
+            assert abs(ekin + epot + eknot - 1.2 * 5 - w[k]) < 1e-12
+            assert abs(eh - (-0.5 * u * 5 if hfmode else 0.0)) < 1e-12
+            if u == 0.0:
+                assert epot == eh
