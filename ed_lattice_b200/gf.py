@@ -1,0 +1,261 @@
+"""Response functions over the state list: the build and evaluation loops of the GF, CHI
+and OC modules.
+
+    build_gf_electrons  build_gf_electrons + lanc_build_gf_electrons_diag/_mix
+                        (src/GF/GF_ELECTRONS.f90:33-98,202-405)
+    eval_gf_electrons   eval_gf_electrons + lanc_eval_gf_electrons
+                        (src/GF/GF_ELECTRONS.f90:100-185,472-512)
+    build_chi           build_chi_spin_electrons + lanc_build_spinChi_diag
+                        (src/CHI/CHI_SPIN_ELECTRONS.f90:33-95,189-240); kind 1 = charge
+    eval_chi_electrons  eval_chi_spin_electrons + lanc_eval_spinChi_electrons (:97-188,380-468)
+    build_oc            build_oc_electrons + lanc_ed_build_oc (src/OC/OC_ELECTRONS.f90:36-214)
+    eval_oc_electrons   lanc_ed_eval_oc + eval_oc_lattice's Drude weight
+                        (src/OC/OC_ELECTRONS.f90:270-319, src/OC/OC_FUNCTIONS.f90:50-70)
+
+GF: for every state of the list, site (pair) and spin, one particle chain (c^+ into the
+sector with one more electron of that spin) and one hole chain (c into the sector with one
+less) run on the device through edg_gf_chain; a sector without such a neighbour gives an
+empty channel (Nexc=0). CHI and OC: one same-sector chain per state (and site) on
+O|state>. Weights and poles are those of the add_to_lanczos_* routines. Chains of a state
+run on the rank that holds its vector; the spectra are all-gathered.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _edgpu_lib as L
+from .diag import StateList, _allgather, _rank_world
+from .edlat import Model, Sector, Spectrum, chi_chain, drude_weight, eval_chi, eval_oc, gf_chain, oc_chain
+
+LANC_NGFITER = 200  # LANC_NGFITER default (src/INPUT_VARS.f90:161)
+
+
+def get_cdg_sector(model: Model, ispin: int, isector: int) -> int:
+    """getCDGsector(1,ispin,isector): the sector with one more electron of spin ispin, 0 if none."""
+    nup, ndw = model.get_nup(isector), model.get_ndw(isector)
+    nup, ndw = (nup + 1, ndw) if ispin == 1 else (nup, ndw + 1)
+    return model.get_sector(nup, ndw) if nup <= model.ns and ndw <= model.ns else 0
+
+
+def get_c_sector(model: Model, ispin: int, isector: int) -> int:
+    """getCsector(1,ispin,isector): the sector with one less electron of spin ispin, 0 if none."""
+    nup, ndw = model.get_nup(isector), model.get_ndw(isector)
+    nup, ndw = (nup - 1, ndw) if ispin == 1 else (nup, ndw - 1)
+    return model.get_sector(nup, ndw) if nup >= 0 and ndw >= 0 else 0
+
+
+class _DeviceChains:
+    """Default chain runner: sectors built once and kept for the whole build."""
+
+    def __init__(self, model: Model, precision: int):
+        self.model, self.precision = model, precision
+        self.sectors: dict[int, Sector] = {}
+        self.loaded = None
+
+    def sector(self, isector: int) -> Sector:
+        s = self.sectors.get(isector)
+        if s is None:
+            s = self.sectors[isector] = Sector.from_index(self.model, isector)
+        return s
+
+    def load(self, isector: int, vec) -> Sector:
+        src = self.sector(isector)
+        if self.loaded is not vec:
+            src.set_state(np.real(vec))
+            self.loaded = vec
+        return src
+
+    def __call__(self, isector, vec, jsector, op, io, jo, ispin, nlanc, ei) -> Spectrum:
+        src = self.load(isector, vec)
+        dst = self.sector(jsector)
+        return gf_chain(src, dst, op, io, ispin, min(nlanc, dst.dim), ei, site2=jo, precision=self.precision)
+
+    def close(self):
+        for s in self.sectors.values():
+            s.delete()
+        self.sectors.clear()
+
+
+def build_gf_electrons(model: Model, state_list: StateList, nlanc: int = LANC_NGFITER, offdiag: bool = False,
+                       precision: int = L.EDG_PREC_F64, chain_fn=None, comm=None) -> dict:
+    """impGmatrix: {(ispin, io, jo): [[particle, hole] per state]} with 1-based sites, for
+    io == jo (the diagonal) and, with `offdiag`, every ordered pair io != jo built from
+    (c_io + c_jo) chains. `chain_fn(isector, vec, jsector, op, io, jo, ispin, nlanc, ei)`
+    returns one channel (jo = 0 for a single site); the default runs on the device."""
+    rank, _ = _rank_world(comm)
+    runner = chain_fn or _DeviceChains(model, precision)
+    ns = model.ns
+    pairs = [(io, io) for io in range(1, ns + 1)]
+    if offdiag:
+        pairs += [(io, jo) for io in range(1, ns + 1) for jo in range(1, ns + 1) if io != jo]
+    mine = {}
+    try:
+        for istate in range(1, state_list.size + 1):
+            st = state_list.states[istate - 1]
+            if st.owner != rank:
+                continue
+            if st.vec is None:
+                raise L.EdgError(L.EDG_ERR_STATE, "build_gf_electrons", "state list holds no vectors")
+            for ispin in range(1, model.nspin + 1):
+                jp, jh = get_cdg_sector(model, ispin, st.sector), get_c_sector(model, ispin, st.sector)
+                for io, jo in pairs:
+                    chans = []
+                    for jsec, op in ((jp, +1), (jh, -1)):
+                        if jsec == 0:
+                            chans.append(Spectrum(np.zeros(0), np.zeros(0), 0.0))
+                        else:
+                            chans.append(runner(st.sector, st.vec, jsec, op, io, 0 if io == jo else jo, ispin,
+                                                nlanc, st.e))
+                    mine[(ispin, io, jo, istate)] = chans
+    finally:
+        if chain_fn is None:
+            runner.close()
+    gm: dict = {}
+    for part in _allgather(mine, comm):
+        for (ispin, io, jo, istate), chans in part.items():
+            gm.setdefault((ispin, io, jo), [None] * state_list.size)[istate - 1] = chans
+    return gm
+
+
+def eval_gf_electrons(gmatrix: dict, state_list: StateList, zeta: float, temp: float, finite_temp: bool,
+                      cutoff: float, wm: np.ndarray, wr: np.ndarray, eps: float, nspin: int, ns: int):
+    """impGmats[nspin, ns, ns, Lmats] and impGreal[nspin, ns, ns, Lreal] (0-based site axes):
+    lanc_eval_gf_electrons' sum over the trimmed list with pesoBZ = exp(-(Ei-Egs)/T)/Z (1/Z
+    at T=0), then G_ij = (G~_ij - G_ii - G_jj)/2 for the off-diagonal pairs (:168-176)."""
+    gmats = np.zeros((nspin, ns, ns, wm.size), dtype=np.complex128)
+    greal = np.zeros((nspin, ns, ns, wr.size), dtype=np.complex128)
+    egs = state_list.emin
+    n = state_list.trim_size(temp, cutoff, finite_temp)
+    zm, zr = 1j * wm, wr + 1j * eps
+    for (ispin, io, jo), states in gmatrix.items():
+        for istate in range(1, n + 1):
+            chans = states[istate - 1]
+            if chans is None:
+                continue
+            ei = state_list.energy(istate)
+            peso_bz = (np.exp(-(ei - egs) / temp) if finite_temp else 1.0) / zeta
+            for ch in chans:
+                if ch.poles.size == 0:
+                    continue
+                w = peso_bz * ch.weight
+                gmats[ispin - 1, io - 1, jo - 1] += (w[None, :] / (zm[:, None] - ch.poles[None, :])).sum(1)
+                greal[ispin - 1, io - 1, jo - 1] += (w[None, :] / (zr[:, None] - ch.poles[None, :])).sum(1)
+    for (ispin, io, jo) in gmatrix:
+        if io == jo:
+            continue
+        s, i, j = ispin - 1, io - 1, jo - 1
+        gmats[s, i, j] = 0.5 * (gmats[s, i, j] - gmats[s, i, i] - gmats[s, j, j])
+        greal[s, i, j] = 0.5 * (greal[s, i, j] - greal[s, i, i] - greal[s, j, j])
+    return gmats, greal
+
+
+def _per_state(state_list: StateList, comm, what: str, fn) -> list:
+    """fn(istate, state) on the rank that owns each state; results gathered in list order."""
+    rank, _ = _rank_world(comm)
+    mine = {}
+    for istate in range(1, state_list.size + 1):
+        st = state_list.states[istate - 1]
+        if st.owner != rank:
+            continue
+        if st.vec is None:
+            raise L.EdgError(L.EDG_ERR_STATE, what, "state list holds no vectors")
+        mine[istate] = fn(istate, st)
+    out = [None] * state_list.size
+    for part in _allgather(mine, comm):
+        for istate, res in part.items():
+            out[istate - 1] = res
+    return out
+
+
+def build_chi(model: Model, state_list: StateList, kind: int = 0, nlanc: int = LANC_NGFITER,
+              precision: int = L.EDG_PREC_F64, chain_fn=None, comm=None) -> dict:
+    """SpinChiMatrix (kind 0: S^z_i) or the charge analogue (kind 1: n_i): {io: [[chain] per
+    state]} for every site (1-based), a same-sector chain on O_io|state> per state. Norb=1
+    has no mixed spin-chi (the reference builds those only for Norb > 1).
+    `chain_fn(isector, vec, io, nlanc, ei)` returns one channel; the default runs on the device."""
+    dev = None if chain_fn else _DeviceChains(model, precision)
+
+    def run(istate, st):
+        res = {}
+        for io in range(1, model.ns + 1):
+            if chain_fn:
+                res[io] = [chain_fn(st.sector, st.vec, io, nlanc, st.e)]
+            else:
+                sec = dev.load(st.sector, st.vec)
+                res[io] = [chi_chain(sec, io, min(nlanc, sec.dim), st.e, kind=kind, precision=precision)]
+        return res
+
+    try:
+        per = _per_state(state_list, comm, "build_chi", run)
+    finally:
+        if dev:
+            dev.close()
+    return {io: [per[k][io] for k in range(state_list.size)] for io in range(1, model.ns + 1)}
+
+
+def _peso_bz(state_list: StateList, istate: int, zeta: float, temp: float, finite_temp: bool) -> float:
+    ei, egs = state_list.energy(istate), state_list.emin
+    return (np.exp(-(ei - egs) / temp) if finite_temp else 1.0) / zeta
+
+
+def eval_chi_electrons(chimatrix: dict, state_list: StateList, zeta: float, temp: float, finite_temp: bool,
+                       cutoff: float, tau: np.ndarray, vr: np.ndarray, eps: float, ns: int, vm=None):
+    """spinChi_tau[ns, ns, Ltau+1], spinChi_w[ns, ns, Lreal] (and spinChi_iv when vm is given,
+    the formula the reference keeps commented out) summed over the trimmed list with pesoBZ
+    as in lanc_eval_spinChi_electrons; beta = 1/temp (temp is the IR cut-off at T=0)."""
+    beta = 1.0 / temp
+    ct = np.zeros((ns, ns, tau.size))
+    cw = np.zeros((ns, ns, vr.size), dtype=np.complex128)
+    civ = np.zeros((ns, ns, vm.size), dtype=np.complex128) if vm is not None else None
+    n = state_list.trim_size(temp, cutoff, finite_temp)
+    for io, states in chimatrix.items():
+        for istate in range(1, n + 1):
+            chans = states[istate - 1]
+            if not chans:
+                continue
+            t, w, v = eval_chi(chans, beta, tau, vr, eps, vm=vm,
+                               pesoBZ=_peso_bz(state_list, istate, zeta, temp, finite_temp))
+            ct[io - 1, io - 1] += t
+            cw[io - 1, io - 1] += w
+            if civ is not None:
+                civ[io - 1, io - 1] += v
+    return ct, cw, civ
+
+
+def build_oc(model: Model, state_list: StateList, nlanc: int = LANC_NGFITER, precision: int = L.EDG_PREC_F64,
+             chain_fn=None, comm=None) -> list:
+    """OcMatrix: [[chain] per state], the chain of the current J (hop i+1 -> i minus h.c.
+    along the ring of sites) on each state, in its own sector. `chain_fn(isector, vec, nlanc,
+    ei)` returns one channel; the default runs on the device."""
+    dev = None if chain_fn else _DeviceChains(model, precision)
+
+    def run(istate, st):
+        if chain_fn:
+            return [chain_fn(st.sector, st.vec, nlanc, st.e)]
+        sec = dev.load(st.sector, st.vec)
+        return [oc_chain(sec, min(nlanc, sec.dim), st.e, precision=precision)]
+
+    try:
+        return _per_state(state_list, comm, "build_oc", run)
+    finally:
+        if dev:
+            dev.close()
+
+
+def eval_oc_electrons(ocmatrix: list, state_list: StateList, zeta: float, temp: float, finite_temp: bool,
+                      cutoff: float, vr: np.ndarray, eps: float, ekin: float, nsites: int):
+    """(Drude weight, OptCond_w[Lreal]): lanc_ed_eval_oc's sums over the trimmed list with
+    pesoBZ, then Drude_weight = -pi/Nsites (Ekin + 2 D) (src/OC/OC_FUNCTIONS.f90:65) with
+    Ekin from lanc_energy."""
+    d_tot = 0.0
+    oc = np.zeros(vr.size)
+    n = state_list.trim_size(temp, cutoff, finite_temp)
+    for istate in range(1, n + 1):
+        chans = ocmatrix[istate - 1]
+        if not chans:
+            continue
+        d, o = eval_oc(chans, vr, eps, cutoff=cutoff, pesoBZ=_peso_bz(state_list, istate, zeta, temp, finite_temp))
+        d_tot += d
+        oc += o
+    return drude_weight(d_tot, ekin, nsites), oc
+
