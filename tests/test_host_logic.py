@@ -82,3 +82,35 @@ def test_gfmatrix_restart_roundtrip():
     assert np.array_equal(back[1][0].weight, states[1][0].weight)
     assert back[0][1].poles.size == 0
     assert E.read_gfmatrix(f) is None
+
+
+def test_read_input_file(tmp_path):
+    """ed_read_input's key file: case-insensitive keys, comments, Fortran reals and logicals,
+    per-orbital lists, defaults for absent keys, and the objects built from it."""
+    from ed_lattice_b200.inputvars import DEFAULTS, diag_params, model_from_input, read_input, sector_form
+    p = tmp_path / "inputED.conf"
+    p.write_text("ULOC=4.d0          ! local interaction\n"
+                 "xmu=2D0\n"
+                 "HFMODE=F\n"
+                 "ED_FINITE_TEMP=.true.\n"
+                 "TEMP=0.05\n"
+                 "LANC_NSTATES_SECTOR=4\n"
+                 "LANC_TOLERANCE=1.d-18\n"
+                 "ED_SPARSE_H=F\n"
+                 "GF_FLAG=T\n"
+                 "   \n"
+                 "! a comment line\n"
+                 "MY_KEY=something\n")
+    cfg = read_input(str(p))
+    assert cfg["ULOC"] == [4.0] and cfg["XMU"] == 2.0 and cfg["HFMODE"] is False
+    assert cfg["ED_FINITE_TEMP"] is True and cfg["TEMP"] == 0.05 and cfg["GF_FLAG"] == [True]
+    assert cfg["LMATS"] == DEFAULTS["LMATS"] and cfg["MY_KEY"] == "something"
+    dp = diag_params(cfg)
+    assert dp.finite_temp and dp.temp == 0.05 and dp.lanc_nstates_sector == 4 and dp.lanc_tolerance == 1e-12
+    assert sector_form(cfg) == E.EDG_FORM_DIRECT
+    m = model_from_input(cfg, E.ring(4))
+    assert m.uloc == 4.0 and m.xmu == 2.0 and not m.hfmode
+    bad = tmp_path / "bad.conf"
+    bad.write_text("HFMODE=maybe\n")
+    with pytest.raises(E.EdgError):
+        read_input(str(bad))
