@@ -369,6 +369,26 @@ def run_ours(args):
         ms64 = s0.elapsed_time(s1) / k64
         extra["hxv_f64"] = {"ms": ms64, "algorithmic_GBps": 2 * D * 8 / (ms64 * 1e-3) / 1e9,
                             "f32_speedup": ms64 / avg_launch_ms}
+        # arithmetic rate: 2 flops per stored nonzero (diagonal + both spins' hops per element)
+        nnz_el = 1.0
+        for spin, dsp in ((1, sector.dimup), (2, sector.dimdw)):
+            nz = C.c_int64()
+            L.check(lib.edg_sector_get_hops(sector.handle, spin, None, None, None, C.byref(nz)), "hops")
+            nnz_el += nz.value / dsp
+        extra["hxv_gflops"] = {"nonzeros_per_element": nnz_el, "f32": 2 * nnz_el * D / (avg_launch_ms * 1e-3) / 1e9,
+                               "f64": 2 * nnz_el * D / (ms64 * 1e-3) / 1e9}
+        # the direct (on-the-fly) form of the same H x v, a few applications
+        sd = E.Sector(model, NUP, NDW, E.EDG_FORM_DIRECT)
+        L.check(lib.edg_sector_set_stream(sd.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
+        L.check(lib.edg_hxv_dev_f64(sd.handle, p64, q64), "direct")
+        s0.record()
+        for _ in range(3):
+            L.check(lib.edg_hxv_dev_f64(sd.handle, p64, q64), "direct")
+        s1.record()
+        torch.cuda.synchronize()
+        msd = s0.elapsed_time(s1) / 3
+        sd.delete()
+        extra["hxv_direct_f64"] = {"ms": msd, "algorithmic_GBps": 2 * D * 8 / (msd * 1e-3) / 1e9}
         del v64, h64
         torch.cuda.empty_cache()
     if rank == 0 and not args.no_e0 and ws == 1:

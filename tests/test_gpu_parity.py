@@ -395,3 +395,19 @@ def test_energy_vs_oracle(hfmode, form):
     en = s.energy()
     assert abs(en["ekin"] + en["epot"] + en["eknot"] - 2.0 * 8 - e0) <= 1e-10 * abs(e0)
     s.delete()
+
+
+def test_half_filling_mapping_identical_hamiltonians():
+    """The model mapping used by every workload: "mu = U/2" is HFMODE=F with XMU=U/2, or
+    HFMODE=T with XMU=0 (src/INPUT_VARS.f90:123,144); both give the same H x v, bit for bit
+    on an integer-valued model, and the same H x v as the oracle."""
+    h = square_lattice(3, 4)
+    a = E.Sector(E.Model(h, uloc=4.0, xmu=2.0, hfmode=False), 6, 6)
+    b = E.Sector(E.Model(h, uloc=4.0, xmu=0.0, hfmode=True), 6, 6)
+    v = O.random_vector(3, a.dim)
+    ha, hb = a.hxv_real(v), b.hxv_real(v)
+    assert np.array_equal(ha, hb)
+    om = O.Model(h, uloc=4.0, xmu=0.0, hfmode=True)
+    assert np.array_equal(ha, O.Stored(om, 6, 6).matvec_d(v))
+    a.delete()
+    b.delete()
