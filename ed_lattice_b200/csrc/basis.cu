@@ -70,6 +70,60 @@ void dev_free(void* p) {
   if (p) cudaFree(p);
 }
 
+// Stream-ordered allocations from a library-owned pool per device that keeps up to
+// kPoolKeepBytes of freed memory for reuse. Freeing a multi-GB buffer with cudaFree after
+// every solve cost up to a second at random in sector loops; returning it to this pool does
+// not. Admission is as in dev_alloc (memory held by the pool counts as used).
+namespace {
+constexpr int kPoolDevices = 64;
+constexpr uint64_t kPoolKeepBytes = uint64_t(8) << 30;
+cudaMemPool_t g_pool[kPoolDevices] = {};
+std::mutex g_pool_mu;
+}  // namespace
+
+int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
+  *p = nullptr;
+  if (bytes == 0) return EDG_OK;
+  int dev = 0;
+  EDG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kPoolDevices) return dev_alloc(p, bytes, what);
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pool[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      EDG_CUDA(cudaMemPoolCreate(&g_pool[dev], &props));
+      uint64_t keep = kPoolKeepBytes;
+      EDG_CUDA(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    pool = g_pool[dev];
+  }
+  size_t freeb = 0, totalb = 0, held = 0, used = 0;
+  EDG_CUDA(cudaMemGetInfo(&freeb, &totalb));
+  EDG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held));
+  EDG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+  const size_t idle = held > used ? held - used : 0;  // reusable without new device memory
+  if (bytes + kReserveBytes > freeb + idle) {
+    set_error("HBM admission refused for %s: %zu bytes requested, %zu free", what, bytes, freeb + idle);
+    return EDG_ERR_NOMEM;
+  }
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_error("cudaMallocFromPoolAsync(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
+    *p = nullptr;
+    return EDG_ERR_NOMEM;
+  }
+  return EDG_OK;
+}
+
+void pool_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
 uint64_t binom_host(int n, int k) {
   if (k < 0 || k > n || n < 0) return 0;
   uint64_t r = 1;

@@ -5,6 +5,7 @@
 // src/GRAPH_MATRIX.f90:325) become EDG_ERR_ARG with a message in edg_last_error().
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -52,6 +53,30 @@ __global__ void k_interleave(double* __restrict__ z, const double* __restrict__ 
 int grid1(int64_t n) {
   int64_t g = (n + 255) / 256;
   return int(g < 148 * 16 ? (g < 1 ? 1 : g) : 148 * 16);
+}
+
+// Sectors draw their stream from a per-device pool created on first use and kept until
+// exit. Creating and destroying a stream per sector (hundreds in a finite-temperature run)
+// stalled the process for up to a second at random; with the pool, up to kStreamPool sectors
+// still run concurrently on separate streams.
+constexpr int kStreamPool = 16;
+constexpr int kMaxDevices = 64;
+cudaError_t pooled_stream(int dev, cudaStream_t* out) {
+  static std::mutex mu;
+  static cudaStream_t pool[kMaxDevices][kStreamPool] = {};
+  static unsigned next[kMaxDevices] = {};
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  const unsigned slot = next[dev]++ % kStreamPool;
+  if (!pool[dev][slot]) {
+    const cudaError_t e = cudaStreamCreateWithFlags(&pool[dev][slot], cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      pool[dev][slot] = nullptr;
+      return e;
+    }
+  }
+  *out = pool[dev][slot];
+  return cudaSuccess;
 }
 
 int check_sector(const edg_sector_s* s) {
@@ -174,13 +199,13 @@ int edg_sector_create(const edg_model* m, int nup, int ndw, int form, edg_sector
   s->ndw = ndw;
   s->form = form;
   cudaError_t e = cudaGetDevice(&s->device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = pooled_stream(s->device, &s->stream);
   if (e != cudaSuccess) {
     set_error("edg_sector_create: %s", cudaGetErrorString(e));
     delete s;
     return EDG_ERR_CUDA;
   }
-  s->own_stream = true;
+  s->own_stream = false;  // pooled: never destroyed with the sector
   int st = sector_build(s);
   if (st != EDG_OK) {
     edg_sector_destroy(s);

@@ -39,6 +39,27 @@ const char* get_error();
 int dev_alloc(void** p, size_t bytes, const char* what);
 void dev_free(void* p);
 
+// Stream-ordered buffers from a per-device pool that keeps freed memory for reuse (large,
+// short-lived solver work space); freed on the same stream when the owner goes out of scope.
+int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what);
+void pool_free(void* p, cudaStream_t st);
+
+template <typename T>
+struct PoolBuf {
+  T* p = nullptr;
+  cudaStream_t st = nullptr;
+  PoolBuf() = default;
+  PoolBuf(const PoolBuf&) = delete;
+  PoolBuf& operator=(const PoolBuf&) = delete;
+  ~PoolBuf() { pool_free(p, st); }
+  int alloc(size_t count, cudaStream_t stream, const char* what) {
+    pool_free(p, st);
+    p = nullptr;
+    st = stream;
+    return pool_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), stream, what);
+  }
+};
+
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
@@ -209,6 +230,8 @@ template <typename T>
 int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
                     double* bn_next);
 int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, int do_sqrt);
+// *out = |x| (FP64, fixed reduction grid; partial holds kRedBlocks values)
+int norm_dev(cudaStream_t st, const double* x, int64_t n, double* partial, double* out);
 // dst = TD(src * scale); dst and src must not overlap (scale_inplace_dev scales in place)
 template <typename TD, typename TS>
 int convert_dev(cudaStream_t st, TD* dst, const TS* src, int64_t n, double scale);

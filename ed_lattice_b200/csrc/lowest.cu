@@ -65,6 +65,8 @@ __global__ void __launch_bounds__(kLkThreads) k_multidot(const double* __restric
   }
 }
 
+__global__ void k_copy1(double* __restrict__ dst, const double* __restrict__ src) { *dst = *src; }
+
 // c[j] = sum_blk partial[j * nblk + blk], one warp per column, fixed order
 __global__ void k_multifinish(const double* __restrict__ partial, int nblk, int m, double* __restrict__ c) {
   const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -194,8 +196,9 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     }
   }
   // device: basis Q[mmax][n], w, scratch
-  DevBuf<double> Q, w, part, coef, Zd, X;
-  EDG_CHECK(Q.alloc(size_t(mmax) * n, "Lanczos basis (lowest-k)"));
+  PoolBuf<double> Q, X;
+  DevBuf<double> w, part, coef, Zd;
+  EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
   EDG_CHECK(w.alloc(n, "Lanczos vector"));
   const int nblk = std::min<int64_t>(592, (n + kLkThreads - 1) / kLkThreads);
   EDG_CHECK(part.alloc(size_t(mmax + 1) * nblk + kRedBlocks, "multi-dot partials"));
@@ -206,72 +209,67 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   } else {
     EDG_CHECK(random_dev(st, Q.p, n, seed));
   }
-  auto norm_of = [&](const double* x, double* out) -> int {
-    EDG_CHECK(dot_dev<double>(st, x, x, n, part.p, coef.p + mmax + 4));
-    double h = 0.0;
-    EDG_CUDA(cudaMemcpyAsync(&h, coef.p + mmax + 4, sizeof(double), cudaMemcpyDeviceToHost, st));
-    EDG_CUDA(cudaStreamSynchronize(st));
-    *out = std::sqrt(h);
-    return EDG_OK;
-  };
+  DevBuf<double> dab;  // a_j at [j], b_{j+1} at [mmax + 1 + j + 1]
+  EDG_CHECK(dab.alloc(2 * size_t(mmax) + 4, "Lanczos scalars"));
+  double* dA = dab.p;
+  double* dB = dab.p + mmax + 1;
+  EDG_CHECK(norm_dev(st, Q.p, n, part.p, dB));
   double nrm = 0.0;
-  EDG_CHECK(norm_of(Q.p, &nrm));
+  EDG_CUDA(cudaMemcpyAsync(&nrm, dB, sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
   if (!(nrm > 0.0)) {
     set_error("edg_lowest_k: start vector has zero norm");
     return EDG_ERR_ARG;
   }
   EDG_CHECK((scale_inplace_dev<double>(st, Q.p, n, 1.0 / nrm)));
-  std::vector<double> A, B(1, 0.0), cvec(size_t(mmax) + 1), zlast;
-  int npass2 = 0;
+  // Steps are queued without waiting on the host: the scalars stay on the device (v_{j+1} =
+  // w / b_{j+1} reads b from there) and the host reads them only when it tests convergence,
+  // every max(1, m/32) steps past the first k. Each step reorthogonalises against the whole
+  // basis by classical Gram-Schmidt applied twice: one pass lost orthogonality entirely on
+  // small sectors, and the test of Daniel, Gragg, Kaufman & Stewart (Math. Comp. 30 (1976)
+  // 772) asked for the second pass at nearly every step (|a_j| is well above b_j for the
+  // shifted spectra of Hubbard sectors).
+  std::vector<double> A, B, hA(size_t(mmax) + 1), hB(size_t(mmax) + 2), zlast;
   double blast = 0.0;
-  int m = 0;
-  bool done = false;
-  for (int j = 0; j < mmax && !done; ++j) {
+  int m = 0, next_check = k;
+  for (int j = 0; j < mmax; ++j) {
     double* qj = Q.p + size_t(j) * n;
     EDG_CHECK(hxv_apply<double>(s, qj, w.p));
-    // a_j = <q_j, w>; full reorthogonalisation against q_0..q_j by classical Gram-Schmidt,
-    // repeated when the projection removed more than half of |w|^2 (Daniel, Gragg, Kaufman &
-    // Stewart, Math. Comp. 30 (1976) 772). With |a_j| well above b_j, as for the shifted
-    // spectra of Hubbard sectors, that is nearly every step; one pass alone lost
-    // orthogonality entirely on small sectors.
-    k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, 1, part.p);
-    k_multifinish<<<(j + 2 + 7) / 8, 256, 0, st>>>(part.p, nblk, j + 2, coef.p);
-    EDG_CUDA(cudaMemcpyAsync(cvec.data(), coef.p, size_t(j + 2) * sizeof(double), cudaMemcpyDeviceToHost, st));
-    k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
-    EDG_CUDA(cudaGetLastError());
-    EDG_CUDA(cudaStreamSynchronize(st));
-    const double wnorm0 = std::sqrt(std::max(cvec[j + 1], 0.0));  // |H q_j|
-    A.push_back(cvec[j]);
-    double b = 0.0;
-    EDG_CHECK(norm_of(w.p, &b));
-    if (b < 0.7071067811865476 * wnorm0) {
+    for (int pass = 0; pass < 2; ++pass) {
       k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, 0, part.p);
       k_multifinish<<<(j + 1 + 7) / 8, 256, 0, st>>>(part.p, nblk, j + 1, coef.p);
+      if (pass == 0) k_copy1<<<1, 1, 0, st>>>(dA + j, coef.p + j);  // a_j = <q_j, H q_j>
       k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
-      EDG_CUDA(cudaGetLastError());
-      EDG_CHECK(norm_of(w.p, &b));
-      ++npass2;
     }
+    EDG_CUDA(cudaGetLastError());
+    EDG_CHECK(norm_dev(st, w.p, n, part.p, dB + j + 1));
     m = j + 1;
-    const bool last = b < 1e-12 || m == n || m == mmax;  // invariant subspace reached, or full
-    // Ritz values and residual estimates of the lowest k: the host eigensolve costs O(m^2), so
-    // it runs every max(1, m/32) steps (at most m/32 extra H x v past convergence)
-    if ((m >= k && (m - k) % std::max(1, m / 32) == 0) || last) {
+    if ((m >= k && m >= next_check) || m == mmax || m == n) {
+      EDG_CUDA(cudaMemcpyAsync(hA.data(), dA, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
+      EDG_CUDA(cudaMemcpyAsync(hB.data(), dB, size_t(m + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+      EDG_CUDA(cudaStreamSynchronize(st));
+      bool last = m == mmax || m == n;
+      for (int t = 0; t < m; ++t)
+        if (!(hB[t + 1] >= 1e-12)) {  // invariant subspace reached at step t (or NaN)
+          m = t + 1;
+          last = true;
+          break;
+        }
+      A.assign(hA.begin(), hA.begin() + m);
+      B.assign(1, 0.0);
+      for (int t = 1; t < m; ++t) B.push_back(hB[t]);
+      const double b = hB[m];
       std::vector<double> th(m), zl(m);
       EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
       zlast = zl;
       blast = b;
-      if (m >= k) {
-        bool conv = true;
-        for (int i = 0; i < k; ++i)
-          if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) conv = false;
-        if (conv) done = true;
-      }
+      bool conv = m >= k;
+      for (int i = 0; i < k && conv; ++i)
+        if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) conv = false;
+      if (conv || last) break;
+      next_check = m + std::max(1, m / 32);
     }
-    if (last) done = true;
-    if (done) break;
-    B.push_back(b);
-    EDG_CHECK((convert_dev<double, double>(st, Q.p + size_t(m) * n, w.p, n, 1.0 / b)));
+    EDG_CHECK(scale_into<double>(st, Q.p + size_t(m) * n, w.p, dB + m, n));
   }
   if (niter) *niter = m;
   std::vector<double> th(m), Z(size_t(m) * m);
@@ -285,7 +283,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   }
   if (evecs_host) {
     EDG_CHECK(Zd.alloc(size_t(m) * m, "Ritz coefficients"));
-    EDG_CHECK(X.alloc(size_t(kk) * n, "Ritz vectors"));
+    EDG_CHECK(X.alloc(size_t(kk) * n, st, "Ritz vectors"));
     EDG_CUDA(cudaMemcpyAsync(Zd.p, Z.data(), size_t(m) * m * sizeof(double), cudaMemcpyHostToDevice, st));
     k_ritz_k<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p, m, kk, n, X.p);
     EDG_CUDA(cudaGetLastError());

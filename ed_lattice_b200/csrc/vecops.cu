@@ -382,6 +382,16 @@ int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const do
   return EDG_OK;
 }
 
+int norm_dev(cudaStream_t st, const double* x, int64_t n, double* partial, double* out) {
+  if (vec16_ok<double>(n, x, x))
+    k_dot_v<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n / V16<double>::K, partial);
+  else
+    k_dot<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n, partial);
+  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, out, 1);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
 int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, int do_sqrt) {
   k_finish<<<1, kRedThreads, 0, st>>>(partial, nblk, out, do_sqrt);
   EDG_CUDA(cudaGetLastError());

@@ -213,7 +213,7 @@ class Sector:
         return hv
 
     def set_stream(self, stream: int | None) -> None:
-        """Run the sector's device work on `stream` (a cudaStream_t as an int; None = own stream)."""
+        """Run the sector's device work on `stream` (a cudaStream_t as an int; None = the legacy default stream)."""
         L.check(L.lib().edg_sector_set_stream(self.handle, C.c_void_p(stream)), "edg_sector_set_stream")
 
     def lowest_k(self, k: int, v0: np.ndarray | None = None, seed: int = 1234, maxit: int = 512,

@@ -411,3 +411,27 @@ def test_half_filling_mapping_identical_hamiltonians():
     assert np.array_equal(ha, O.Stored(om, 6, 6).matvec_d(v))
     a.delete()
     b.delete()
+
+
+def test_hxv_long_hop_lists():
+    """All-to-all random hopping on 12 sites, sector (6,6): 36 hops per configuration, above the
+    32-entry hop lists of the grouped down pass, so the down spin takes the segment-warp
+    kernel; FP64 against the oracle (1e-13) and FP32 (2e-6)."""
+    import torch
+    rng = np.random.default_rng(21)
+    A = np.round(rng.normal(size=(12, 12)) * 1024) / 1024
+    h = (A + A.T) / 2
+    gm, om = models(h, uloc=2.5, xmu=1.0, hfmode=True)
+    s = E.Sector(gm, 6, 6)
+    rp, _, _ = s.hops(2)
+    assert np.diff(rp).max() == 36
+    v = O.random_vector(41, s.dim)
+    ref = O.Stored(om, 6, 6).matvec_d(v)
+    assert np.abs(s.hxv_real(v) - ref).max() <= 1e-13 * np.abs(ref).max()
+    dv = torch.tensor(v, dtype=torch.float32, device="cuda")
+    dh = torch.empty_like(dv)
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    L.check(L.lib().edg_hxv_dev_f32(s.handle, C.c_void_p(dv.data_ptr()), C.c_void_p(dh.data_ptr())), "f32")
+    torch.cuda.synchronize()
+    assert np.abs(dh.double().cpu().numpy() - ref).max() <= 2e-6 * np.abs(ref).max()
+    s.delete()
