@@ -1,6 +1,6 @@
 """Benchmark of the sector-Lanczos hot path on B200.
 
-Workload (BASELINE config 2): 4x4 periodic square lattice, nearest-neighbour t=1, U=8,
+Workload: 4x4 periodic square lattice, nearest-neighbour t=1, U=8,
 half filling Nup=Ndw=8, D = 12870^2 = 165,636,900. A step is one H x v of that sector in
 FP32 (the bulk precision of the engine), stored form, vectors resident in HBM; inputs are
 larger than L2 (662 MB per vector), so no flush is needed between steps.
@@ -116,7 +116,7 @@ def dist_env():
 
 
 def cpu_baseline_sample(target_seconds: float = 12.0):
-    """The oracle's stored-form spMatVec (FP64, OpenMP on all host threads) on config 2,
+    """The oracle's stored-form spMatVec (FP64, OpenMP on all host threads) on the 4x4 half-filled sector,
     timed on a bounded sample of output rows. Returns (GB/s in the metric's unit, info)."""
     from ed_lattice_b200.edlat import square_lattice
     from oracle import oracle as O

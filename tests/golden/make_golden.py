@@ -43,7 +43,7 @@ def square(lx, ly, t=1.0):
     return H
 
 
-def config1():
+def ring8():
     """L=8 periodic ring, t=1, U=4, mu=U/2 (HFMODE=F, XMU=2), sector (4,4), FP64,
     seeded uniform[-1,1) start vector (seed 2024), 100 tridiagonal steps."""
     m = O.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
@@ -54,7 +54,7 @@ def config1():
     obs = O.observables(8, 4, 4, vec)
     hv = st.matvec_d(v0)
     hvd = O.direct_matvec_d(m, 4, 4, v0)
-    np.savez_compressed(os.path.join(HERE, "config1_ring8.npz"), v0=v0, hv_stored=hv, hv_direct=hvd, alanc=a,
+    np.savez_compressed(os.path.join(HERE, "ring8_U4_sector44.npz"), v0=v0, hv_stored=hv, hv_direct=hvd, alanc=a,
                         blanc=b, norm2=n2, e0=e0, dens=obs["dens"], docc=obs["docc"],
                         map_up=O.build_map(8, 4))
 
@@ -135,7 +135,7 @@ def thermal3x4():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["config1", "disorder3x4", "thermal3x4"]
+    which = sys.argv[1:] or ["ring8", "disorder3x4", "thermal3x4"]
     for name in which:
         globals()[name]()
     for f in sorted(os.listdir(HERE)):

@@ -1,4 +1,4 @@
-"""Full-size checks on the 4x4 half-filled sector (D = 165,636,900),
+"""Full-size checks on the 4x4 half-filled sector (D = 165,636,900, U=8),
 where the CPU oracle is too slow to run: size-independent properties of the operator and
 agreement between the FP32 and FP64 device paths (the FP64 path is bit-exact against the
 oracle on the smaller sectors of test_gpu_parity.py)."""
@@ -73,7 +73,7 @@ def test_large_stored_vs_direct(sector):
     sd.delete()
 
 
-def test_gf_chains_config3_size():
+def test_gf_chains_4x4_U4_full_size():
     """4x4 lattice at U=4: ground state of (8,8), then c^+_{1,up} into (9,8) and c_{1,up} into
     (7,8) (D = 147,232,800 each). The particle and hole norms add up to 1 (the anticommutator
     {c, c^+} = 1 on a normalised state), their difference is 1 - 2 n_{1,up} from the state's

@@ -108,8 +108,8 @@ def test_hop_tables_golden():
 
 
 # ----------------------------------------------------------------------------- H x v
-def test_hxv_golden_config1_bit_exact():
-    g = np.load(os.path.join(GOLDEN, "config1_ring8.npz"))
+def test_hxv_golden_ring8_bit_exact():
+    g = np.load(os.path.join(GOLDEN, "ring8_U4_sector44.npz"))
     gm = E.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
     s = E.Sector(gm, 4, 4, E.EDG_FORM_STORED)
     assert np.array_equal(s.maps()[0], g["map_up"])
@@ -215,9 +215,9 @@ def test_hxv_errors():
 
 
 # ----------------------------------------------------------------------------- Lanczos
-def test_config1_lanczos_and_ground_state():
-    """Config 1: L=8 ring, U=4, mu=U/2, (4,4): a(1:100), b(2:100), E0, density, docc."""
-    g = np.load(os.path.join(GOLDEN, "config1_ring8.npz"))
+def test_ring8_lanczos_and_ground_state():
+    """L=8 ring, U=4, mu=U/2, (4,4): a(1:100), b(2:100), E0, density, docc."""
+    g = np.load(os.path.join(GOLDEN, "ring8_U4_sector44.npz"))
     gm = E.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
     s = E.Sector(gm, 4, 4)
     a, b, n2, n = E.tridiag_Hv_sector(s, g["v0"], 100)

@@ -209,7 +209,7 @@ def test_observables_vs_numpy():
 
 
 def test_golden_fixtures_reproduce():
-    g = np.load(os.path.join(GOLDEN, "config1_ring8.npz"))
+    g = np.load(os.path.join(GOLDEN, "ring8_U4_sector44.npz"))
     m = O.Model(ring(8), uloc=4.0, xmu=2.0, hfmode=False)
     st = O.Stored(m, 4, 4)
     v0 = O.random_vector(2024, st.dim)
