@@ -116,6 +116,31 @@ def test_f32_f64_and_symmetry(big):
     torch.cuda.empty_cache()
 
 
+def test_ground_state_and_momentum_chi_full_size(big):
+    """The full 2.36e9-state sector: FP32+refine ground state to 1e-8 (its energy terms add up
+    to E0: one FP64 H x v of the state), then spin and charge susceptibility chains at
+    q = (pi, 0) (site weights (-1)^x) with FP32 and FP64 vectors agreeing on chi(i nu_n)."""
+    e0, it = C.c_double(), C.c_int()
+    L.check(L.lib().edg_ground_state_keep(big.handle, None, C.c_uint64(2024), 400, 1e-8, E.EDG_GS_F32_REFINE,
+                                          C.byref(e0), C.byref(it)), "gs")
+    en = big.energy()
+    assert abs(en["ekin"] + en["epot"] + en["eknot"] - XMU * 2 * N - e0.value) <= 1e-8 * abs(e0.value)
+    qcos = np.array([(-1.0) ** (i % 6) for i in range(NS)])
+    beta = 10.0
+    vm = 2 * np.pi / beta * np.arange(0, 12)
+    for kind in (0, 1):
+        chi = {}
+        for prec in (E.EDG_PREC_F64, E.EDG_PREC_F32):
+            sp = E.chi_chain(big, 1, 60, e0.value, kind=kind, qcos=qcos, precision=prec)
+            assert sp.norm2 > 0 and np.all(sp.weight >= 0)
+            w, p_ = sp.weight, sp.poles
+            chi[prec] = np.array([(w * 2 * p_ / (v * v + p_ * p_)).sum() if v > 0 else (2 * w / np.maximum(p_, 1e-12)).sum()
+                                  for v in vm])
+            chi[(prec, "n2")] = sp.norm2
+        assert abs(chi[(E.EDG_PREC_F32, "n2")] - chi[(E.EDG_PREC_F64, "n2")]) <= 1e-12 * chi[(E.EDG_PREC_F64, "n2")]
+        assert np.abs(chi[E.EDG_PREC_F32][1:] - chi[E.EDG_PREC_F64][1:]).max() <= 1e-5 * np.abs(chi[E.EDG_PREC_F64]).max()
+
+
 @pytest.mark.parametrize("nup,ndw,hop", [(7, 1, "uniform"), (7, 2, "random"), (2, 7, "uniform")])
 def test_split_up_pass_vs_oracle(nup, ndw, hop):
     """DimUp = C(18,7) = 31,824: an FP64 row (255 KB) exceeds shared memory, so the FP64 up
