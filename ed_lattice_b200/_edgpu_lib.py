@@ -80,6 +80,7 @@ SIGNATURES = {
     "edg_gf_chain": (_i, [_p, _p, _i, _i, _i, _i, _i, _i, _d, _pd, _pd, _pd, _pi]),
     "edg_chi_chain": (_i, [_p, _i, _i, _i, _pd, _i, _i, _d, _pd, _pd, _pd, _pi]),
     "edg_oc_chain": (_i, [_p, _i, _i, _d, _pd, _pd, _pd, _pi]),
+    "edg_eval_poles": (_i, [_i64, _pd, _pd, _i64, _pd, _pd, _pd, _pd]),
     "edg_tridiag_block_dev": (_i, [_p, _i, _p, _i, _d, _i, _pd, _pd, _pd, _pi]),
     "edg_tridiag_eigh": (_i, [_i, _pd, _pd, _pd, _pd]),
     "edg_poles_weights": (_i, [_i, _pd, _pd, _d, _d, _i, _pd, _pd]),

@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libedgpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["basis.cu", "hxv.cu", "vecops.cu", "lanczos.cu", "excite.cu", "capi.cu", "noalloc.cu", "lowest.cu", "tridiag_host.cpp"]
+SOURCES = ["basis.cu", "hxv.cu", "vecops.cu", "lanczos.cu", "excite.cu", "capi.cu", "noalloc.cu", "lowest.cu", "evalgrid.cu", "tridiag_host.cpp"]
 HEADERS = ["common.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -19,6 +19,8 @@ int apply_diagop(const edg_sector_s* s, int kind, const double* wsite, const dou
 int apply_current(const edg_sector_s* s, const double* din, double* dout, cudaStream_t st);
 int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, double* epot, double* eknot,
            double* ehartree);
+int eval_poles(int64_t npoles, const double* poles, const double* weights, int64_t nz, const double* z_re,
+               const double* z_im, double* out_re, double* out_im);
 int observables(const edg_sector_s* s, const double* psi, double weight, double* dens, double* dens_up,
                 double* dens_dw, double* docc, double* magz, cudaStream_t st);
 }  // namespace edg
@@ -555,6 +557,19 @@ int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* pol
   EDG_CHECK(s->w64[3].alloc(s->dim, "excitation vector"));
   EDG_CHECK(edg_apply_current_dev_f64(s, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);
+}
+
+int edg_eval_poles(int64_t npoles, const double* poles, const double* weights, int64_t nz, const double* z_re,
+                   const double* z_im, double* out_re, double* out_im) {
+  EDG_ARG(npoles >= 0 && nz >= 0, "edg_eval_poles: negative size");
+  EDG_ARG((npoles == 0 || (poles && weights)) && (nz == 0 || (z_re && z_im && out_re && out_im)),
+          "edg_eval_poles: NULL array");
+  int ndev = 0;
+  if (edg_device_count(&ndev) != EDG_OK || ndev == 0) {
+    set_error("edg_eval_poles: no CUDA device");
+    return EDG_ERR_NODEVICE;
+  }
+  return eval_poles(npoles, poles, weights, nz, z_re, z_im, out_re, out_im);
 }
 
 int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc, double threshold, int precision,

@@ -105,6 +105,24 @@ struct Recurrence {
   }
   // scale that turns the current buffer U into v_j
   double vscale(int j) const { return fused ? 1.0 / bn_host[j] : 1.0; }
+  // step j queued on the stream: a_j and b_{j+1} land in the device scalars only
+  int step_dev(int j) {
+    const int64_t n = s->dim;
+    cudaStream_t st = s->stream;
+    if (fused) {
+      int nb = 0;
+      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, &nb));
+      EDG_CHECK(finish_dev(st, sc.partial, nb, sc.a + j, 0));
+      EDG_CHECK(lanczos_step_b2<T>(st, W, U, sc.a + j, sc.bn + j, n, sc.partial, sc.bn + j + 1));
+    } else {
+      EDG_CHECK(hxv_apply<T>(s, U, W));
+      EDG_CHECK(lanczos_step_a<T>(st, W, P, U, sc.b + j, n, sc.partial, sc.a + j));
+      EDG_CHECK(lanczos_step_b<T>(st, W, U, sc.a + j, n, sc.partial, sc.b + j + 1));
+    }
+    return EDG_OK;
+  }
+  // device array of b_{j+1} (index j+1)
+  const double* b_dev() const { return fused ? sc.bn : sc.b; }
   // step j: W <- the unnormalised u_{j+1}; returns a_j and b_{j+1} on the host
   int step(int j, double* a, double* b) {
     const int64_t n = s->dim;
@@ -169,18 +187,31 @@ int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, d
   if (n2 == 0.0 || nlanc <= 0) return EDG_OK;
   Recurrence<T> R;
   EDG_CHECK(R.init(s, dv0, 1.0 / std::sqrt(n2), nlanc + 1));
-  for (int j = 0; j < nlanc; ++j) {
-    double a, b;
-    EDG_CHECK(R.step(j, &a, &b));
-    alanc[j] = a;
-    *nsteps = j + 1;
-    if (j + 1 < nlanc) blanc[j + 1] = b;
-    if (!(b >= threshold)) {  // also stops on NaN
-      if (j + 1 < nlanc) blanc[j + 1] = 0.0;
-      break;
+  // Steps are queued kChunk at a time with the scalars left on the device; the host reads a
+  // chunk's a/b at its end and stops at the first b below threshold (the steps queued after
+  // it in the same chunk are discarded). The arithmetic is that of one step at a time.
+  constexpr int kChunk = 16;
+  std::vector<double> ha(kChunk), hb(kChunk);
+  for (int j0 = 0; j0 < nlanc; j0 += kChunk) {
+    const int j1 = std::min(nlanc, j0 + kChunk);
+    for (int j = j0; j < j1; ++j) {
+      EDG_CHECK(R.step_dev(j));
+      if (j + 1 < nlanc) EDG_CHECK(R.advance(j, 0.0));  // the fused form's host norms are unused here
     }
-    if (j + 1 == nlanc) break;
-    EDG_CHECK(R.advance(j, b));
+    EDG_CUDA(cudaMemcpyAsync(ha.data(), R.sc.a + j0, size_t(j1 - j0) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaMemcpyAsync(hb.data(), R.b_dev() + j0 + 1, size_t(j1 - j0) * sizeof(double), cudaMemcpyDeviceToHost,
+                             st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+    for (int j = j0; j < j1; ++j) {
+      const double b = hb[j - j0];
+      alanc[j] = ha[j - j0];
+      *nsteps = j + 1;
+      if (j + 1 < nlanc) blanc[j + 1] = b;
+      if (!(b >= threshold)) {  // also stops on NaN
+        if (j + 1 < nlanc) blanc[j + 1] = 0.0;
+        return EDG_OK;
+      }
+    }
   }
   return EDG_OK;
 }

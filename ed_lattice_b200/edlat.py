@@ -386,6 +386,17 @@ def grids(temp: float, lmats: int = 4096, lreal: int = 5000, ltau: int = 1024, w
     return wm, vm, wr, vr, tau
 
 
+def eval_poles(poles: np.ndarray, weights: np.ndarray, z: np.ndarray) -> np.ndarray:
+    """sum_k weights[k] / (z - poles[k]) for every z, on the device (edg_eval_poles)."""
+    p, w = _f64(poles), _f64(weights)
+    z = np.ascontiguousarray(z, dtype=np.complex128)
+    zr, zi = _f64(z.real), _f64(z.imag)
+    ore, oim = np.zeros(z.size), np.zeros(z.size)
+    L.check(L.lib().edg_eval_poles(p.size, _pd(p), _pd(w), z.size, _pd(zr), _pd(zi), _pd(ore), _pd(oim)),
+            "edg_eval_poles")
+    return ore + 1j * oim
+
+
 def eval_gf(channels: list[Spectrum], wm: np.ndarray, wr: np.ndarray, eps: float, pesoBZ: float = 1.0):
     """lanc_eval_gf_electrons' sum (src/GF/GF_ELECTRONS.f90:503-508)."""
     gm = np.zeros(wm.size, dtype=np.complex128)

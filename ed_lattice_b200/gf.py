@@ -25,7 +25,8 @@ import numpy as np
 
 from . import _edgpu_lib as L
 from .diag import StateList, _allgather, _rank_world
-from .edlat import Model, Sector, Spectrum, chi_chain, drude_weight, eval_chi, eval_oc, gf_chain, oc_chain
+from .edlat import (Model, Sector, Spectrum, chi_chain, drude_weight, eval_chi, eval_oc, eval_poles, gf_chain,
+                    oc_chain)
 
 LANC_NGFITER = 200  # LANC_NGFITER default (src/INPUT_VARS.f90:161)
 
@@ -118,16 +119,21 @@ def build_gf_electrons(model: Model, state_list: StateList, nlanc: int = LANC_NG
 
 
 def eval_gf_electrons(gmatrix: dict, state_list: StateList, zeta: float, temp: float, finite_temp: bool,
-                      cutoff: float, wm: np.ndarray, wr: np.ndarray, eps: float, nspin: int, ns: int):
+                      cutoff: float, wm: np.ndarray, wr: np.ndarray, eps: float, nspin: int, ns: int,
+                      backend: str = "device"):
     """impGmats[nspin, ns, ns, Lmats] and impGreal[nspin, ns, ns, Lreal] (0-based site axes):
     lanc_eval_gf_electrons' sum over the trimmed list with pesoBZ = exp(-(Ei-Egs)/T)/Z (1/Z
-    at T=0), then G_ij = (G~_ij - G_ii - G_jj)/2 for the off-diagonal pairs (:168-176)."""
+    at T=0), then G_ij = (G~_ij - G_ii - G_jj)/2 for the off-diagonal pairs (:168-176).
+    backend "device": every pole of an entry in one edg_eval_poles call per axis; "host": numpy."""
+    if backend not in ("device", "host"):
+        raise L.EdgError(L.EDG_ERR_ARG, "eval_gf_electrons", f"backend={backend!r}")
     gmats = np.zeros((nspin, ns, ns, wm.size), dtype=np.complex128)
     greal = np.zeros((nspin, ns, ns, wr.size), dtype=np.complex128)
     egs = state_list.emin
     n = state_list.trim_size(temp, cutoff, finite_temp)
     zm, zr = 1j * wm, wr + 1j * eps
     for (ispin, io, jo), states in gmatrix.items():
+        ps, ws = [], []
         for istate in range(1, n + 1):
             chans = states[istate - 1]
             if chans is None:
@@ -135,11 +141,20 @@ def eval_gf_electrons(gmatrix: dict, state_list: StateList, zeta: float, temp: f
             ei = state_list.energy(istate)
             peso_bz = (np.exp(-(ei - egs) / temp) if finite_temp else 1.0) / zeta
             for ch in chans:
-                if ch.poles.size == 0:
-                    continue
-                w = peso_bz * ch.weight
-                gmats[ispin - 1, io - 1, jo - 1] += (w[None, :] / (zm[:, None] - ch.poles[None, :])).sum(1)
-                greal[ispin - 1, io - 1, jo - 1] += (w[None, :] / (zr[:, None] - ch.poles[None, :])).sum(1)
+                if ch.poles.size:
+                    ps.append(ch.poles)
+                    ws.append(peso_bz * ch.weight)
+        if not ps:
+            continue
+        p, w = np.concatenate(ps), np.concatenate(ws)
+        if backend == "device":
+            gmats[ispin - 1, io - 1, jo - 1] = eval_poles(p, w, zm)
+            greal[ispin - 1, io - 1, jo - 1] = eval_poles(p, w, zr)
+        else:
+            for lo in range(0, p.size, 512):
+                pp, ww = p[lo:lo + 512], w[lo:lo + 512]
+                gmats[ispin - 1, io - 1, jo - 1] += (ww[None, :] / (zm[:, None] - pp[None, :])).sum(1)
+                greal[ispin - 1, io - 1, jo - 1] += (ww[None, :] / (zr[:, None] - pp[None, :])).sum(1)
     for (ispin, io, jo) in gmatrix:
         if io == jo:
             continue

@@ -227,6 +227,15 @@ int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qc
 int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* poles,
                  double* weights, double* norm2, int* nout);
 
+/* Pole sums on a frequency grid, the loop of lanc_eval_gf_electrons
+ * (src/GF/GF_ELECTRONS.f90:503-508): out(z_m) += sum_k weights[k] / (z_m - poles[k]) with
+ * z_m = z_re[m] + i z_im[m] (i w_n on the Matsubara axis, w + i eps on the real axis). Host
+ * arrays, evaluated on the current device in FP64 with a fixed summation order. The caller
+ * folds the Boltzmann factors into the weights and concatenates every state and channel of
+ * one Green's function entry into one call. */
+int edg_eval_poles(int64_t npoles, const double* poles, const double* weights, int64_t nz,
+                   const double* z_re, const double* z_im, double* out_re, double* out_im);
+
 /* Batched chains: k start vectors of one sector in one call, each tridiagonalised as by
  * edg_tridiag_dev_f64 (one alpha/beta sequence per column). The chains run one after
  * another, each H x v using the whole GPU; a block H x V over several vectors would gather

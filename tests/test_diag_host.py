@@ -187,7 +187,7 @@ def test_gf_driver_against_lehmann(temp, finite_temp):
     assert len(gm) == 16 and all(len(v) == sl.size for v in gm.values())
     wm = np.pi * temp * (2 * np.arange(1, 33) - 1)
     wr = np.linspace(-4, 4, 41)
-    gmats, greal = eval_gf_electrons(gm, sl, zeta, p.temp, p.finite_temp, p.cutoff, wm, wr, 0.1, 1, 4)
+    gmats, greal = eval_gf_electrons(gm, sl, zeta, p.temp, p.finite_temp, p.cutoff, wm, wr, 0.1, 1, 4, backend="host")
     pairs = [(1, 1), (2, 2), (1, 2), (1, 3), (4, 2)]
     ref_m = lehmann_g(om, 4, temp, p.cutoff, finite_temp, pairs, 1j * wm)
     ref_r = lehmann_g(om, 4, temp, p.cutoff, finite_temp, pairs, wr + 0.1j)

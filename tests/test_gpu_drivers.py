@@ -43,6 +43,8 @@ def test_gf_driver_device(setup):
     wm = np.pi * p.temp * (2 * np.arange(1, 33) - 1)
     wr = np.linspace(-4, 4, 41)
     gmats, greal = eval_gf_electrons(gm, sl, zeta, p.temp, True, p.cutoff, wm, wr, 0.1, 1, 4)
+    hm, hr = eval_gf_electrons(gm, sl, zeta, p.temp, True, p.cutoff, wm, wr, 0.1, 1, 4, backend="host")
+    assert np.abs(gmats - hm).max() < 1e-12 and np.abs(greal - hr).max() < 1e-10  # device pole sums
     pairs = [(1, 1), (3, 3), (1, 2), (2, 4)]
     ref = lehmann_g(om, 4, p.temp, p.cutoff, True, pairs, 1j * wm, spec=spec)
     for (i, j) in pairs:
