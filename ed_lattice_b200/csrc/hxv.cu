@@ -582,6 +582,98 @@ __global__ void __launch_bounds__(256) k_direct(HxvArgs<T> a, DirectArgsHdr d) {
   }
 }
 
+// Direct form by row blocks: a CTA takes kDirRows consecutive rows idw. One warp per row
+// derives that row's down-spin hop list once (in bond order, kept in shared memory); each
+// thread then derives the up-spin hops of its column iup once and applies them to all the
+// block's rows. Per element: diagonal, up hops, down hops, each in bond order, the order
+// k_direct sums them in.
+constexpr int kDirRows = 8;
+constexpr int kDirHops = 64;  // hop-list capacity per row (host checks the bound)
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_direct_rows(HxvArgs<T> a, DirectArgsHdr d, int64_t nrb) {
+  extern __shared__ unsigned char smem_raw[];
+  int32_t* sb = reinterpret_cast<int32_t*>(smem_raw);
+  const int nb = d.nb_up + d.nb_dw;
+  T* sh = reinterpret_cast<T*>(smem_raw + ((2 * nb * sizeof(int32_t) + 15) / 16) * 16);
+  __shared__ uint32_t sC[kBinomN * kBinomN];
+  __shared__ uint32_t s_src[kDirRows][kDirHops];
+  __shared__ T s_val[kDirRows][kDirHops];
+  __shared__ int s_cnt[kDirRows];
+  __shared__ uint32_t s_mdw[kDirRows];
+  __shared__ T s_edw[kDirRows];
+  for (int k = threadIdx.x; k < 2 * nb; k += blockDim.x) sb[k] = d.bonds[k];
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) sh[k] = T(d.bh[k]);
+  for (int k = threadIdx.x; k < kBinomN * kBinomN; k += blockDim.x) sC[k] = d.C[k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t dimup = a.dimup;
+  for (int64_t rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+    const int64_t r0 = rb * kDirRows;
+    __syncthreads();
+    if (warp < kDirRows) {
+      const int64_t row = r0 + warp;
+      int cnt = 0;
+      if (row < a.dimdw) {
+        const uint32_t mdw = a.map_dw[row];
+        for (int k0 = d.nb_up; k0 < nb; k0 += 32) {
+          const int k = k0 + lane;
+          bool ok = false;
+          int ba = 0, bb = 0;
+          if (k < nb) {
+            ba = sb[2 * k];
+            bb = sb[2 * k + 1];
+            ok = ((mdw >> ba) & 1u) && !((mdw >> bb) & 1u);
+          }
+          const unsigned ball = __ballot_sync(0xffffffffu, ok);
+          if (ok) {
+            const int pos = cnt + __popc(ball & ((1u << lane) - 1u));
+            if (pos < kDirHops) {
+              const uint32_t t = (mdw & ~(1u << ba)) | (1u << bb);
+              s_src[warp][pos] = rank_of_d(t, sC);
+              s_val[warp][pos] = between_parity_d(mdw, ba, bb) ? -sh[k] : sh[k];
+            }
+          }
+          cnt += __popc(ball);
+        }
+        if (lane == 0) {
+          s_mdw[warp] = mdw;
+          s_edw[warp] = a.e_dw[row];
+        }
+      }
+      if (lane == 0) s_cnt[warp] = cnt < kDirHops ? cnt : kDirHops;
+    }
+    __syncthreads();
+    for (int64_t iup = threadIdx.x; iup < dimup; iup += blockDim.x) {
+      const uint32_t mup = a.map_up[iup];
+      const T eu = a.e_up[iup];
+      T acc[kDirRows];
+#pragma unroll
+      for (int r = 0; r < kDirRows; ++r)
+        acc[r] = r0 + r < a.dimdw
+                     ? (eu + s_edw[r] + a.U * T(__popc(mup & s_mdw[r]))) * a.v[(r0 + r) * dimup + iup]
+                     : T(0);
+      for (int k = 0; k < d.nb_up; ++k) {
+        const int ba = sb[2 * k], bb = sb[2 * k + 1];
+        if (((mup >> ba) & 1u) && !((mup >> bb) & 1u)) {
+          const uint32_t t = (mup & ~(1u << ba)) | (1u << bb);
+          const T h = between_parity_d(mup, ba, bb) ? -sh[k] : sh[k];
+          const int64_t src = rank_of_d(t, sC);
+#pragma unroll
+          for (int r = 0; r < kDirRows; ++r)
+            if (r0 + r < a.dimdw) acc[r] = fmaT<T>(h, a.v[(r0 + r) * dimup + src], acc[r]);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kDirRows; ++r) {
+        if (r0 + r >= a.dimdw) continue;
+        for (int q = 0; q < s_cnt[r]; ++q)
+          acc[r] = fmaT<T>(s_val[r][q], a.v[int64_t(s_src[r][q]) * dimup + iup], acc[r]);
+        a.hv[(r0 + r) * dimup + iup] = acc[r];
+      }
+    }
+  }
+}
+
 template <typename T>
 const T* pick(const DevBuf<double>& d, const DevBuf<float>& f);
 template <>
@@ -747,11 +839,21 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
     d.C = s->binom.p;
     const int nb = d.nb_up + d.nb_dw;
     size_t smem = ((2 * nb * sizeof(int32_t) + 15) / 16) * 16 + nb * sizeof(T) + 16;
-    const int64_t n = a.dimup * a.dimdw;
-    const int64_t want = (n + 255) / 256;
-    const int g = int(want < int64_t(sms) * 8 ? want : int64_t(sms) * 8);
-    if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(k_direct<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_direct<T><<<g, 256, smem, st>>>(a, d);
+    // down hops of one configuration: at most min(directed bonds, Ndw * (Ns - Ndw))
+    const int64_t hop_bound = std::min<int64_t>(d.nb_dw, int64_t(s->ndw) * (s->model.ns - s->ndw));
+    if (hop_bound <= kDirHops) {
+      const int64_t nrb = (a.dimdw + kDirRows - 1) / kDirRows;
+      const int g = int(nrb < int64_t(sms) * 8 ? nrb : int64_t(sms) * 8);
+      if (smem > 32 * 1024)
+        EDG_CUDA(cudaFuncSetAttribute(k_direct_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      k_direct_rows<T><<<g, 256, smem, st>>>(a, d, nrb);
+    } else {
+      const int64_t n = a.dimup * a.dimdw;
+      const int64_t want = (n + 255) / 256;
+      const int g = int(want < int64_t(sms) * 8 ? want : int64_t(sms) * 8);
+      if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(k_direct<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      k_direct<T><<<g, 256, smem, st>>>(a, d);
+    }
     EDG_CUDA(cudaGetLastError());
   }
   return EDG_OK;
