@@ -83,6 +83,7 @@ SIGNATURES = {
     "edg_eval_poles": (_i, [_i64, _pd, _pd, _i64, _pd, _pd, _pd, _pd]),
     "edg_tridiag_block_dev": (_i, [_p, _i, _p, _i, _d, _i, _pd, _pd, _pd, _pi]),
     "edg_tridiag_eigh": (_i, [_i, _pd, _pd, _pd, _pd]),
+    "edg_tridiag_lowest": (_i, [_i, _pd, _pd, _i, _pd, _pd]),
     "edg_poles_weights": (_i, [_i, _pd, _pd, _d, _d, _i, _pd, _pd]),
 }
 

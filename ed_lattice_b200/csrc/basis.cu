@@ -43,50 +43,38 @@ const char* get_error() { return g_err; }
 // state and other users of the device.
 static const size_t kReserveBytes = size_t(1) << 30;
 
-int dev_alloc(void** p, size_t bytes, const char* what) {
-  *p = nullptr;
-  if (bytes == 0) return EDG_OK;
-  size_t freeb = 0, totalb = 0;
-  cudaError_t e = cudaMemGetInfo(&freeb, &totalb);
-  if (e != cudaSuccess) {
-    set_error("cudaMemGetInfo: %s", cudaGetErrorString(e));
-    return EDG_ERR_CUDA;
-  }
-  if (bytes + kReserveBytes > freeb) {
-    set_error("HBM admission refused for %s: %zu bytes requested, %zu free", what, bytes, freeb);
-    return EDG_ERR_NOMEM;
-  }
-  e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) {
-    (void)cudaGetLastError();
-    set_error("cudaMalloc(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
-    *p = nullptr;
-    return EDG_ERR_NOMEM;
-  }
-  return EDG_OK;
-}
-
-void dev_free(void* p) {
-  if (p) cudaFree(p);
-}
-
 // Stream-ordered allocations from a library-owned pool per device that keeps up to
-// kPoolKeepBytes of freed memory for reuse. Freeing a multi-GB buffer with cudaFree after
-// every solve cost up to a second at random in sector loops; returning it to this pool does
-// not. Admission is as in dev_alloc (memory held by the pool counts as used).
+// kPoolKeepBytes of freed memory for reuse. A request is refused when it would leave less than
+// kReserveBytes of HBM free (memory held by the pool counts as used); the driver's free-memory query is skipped when the pool already
+// holds enough idle memory for the request.
 namespace {
 constexpr int kPoolDevices = 64;
 constexpr uint64_t kPoolKeepBytes = uint64_t(8) << 30;
 cudaMemPool_t g_pool[kPoolDevices] = {};
 std::mutex g_pool_mu;
+thread_local cudaStream_t t_free_stream = nullptr;
+thread_local bool t_free_override = false;
 }  // namespace
+
+FreeStreamOverride::FreeStreamOverride(cudaStream_t st) : prev(t_free_stream), prev_set(t_free_override) {
+  t_free_stream = st;
+  t_free_override = true;
+}
+FreeStreamOverride::~FreeStreamOverride() {
+  t_free_stream = prev;
+  t_free_override = prev_set;
+}
+cudaStream_t free_stream(cudaStream_t recorded) { return t_free_override ? t_free_stream : recorded; }
 
 int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
   *p = nullptr;
   if (bytes == 0) return EDG_OK;
   int dev = 0;
   EDG_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kPoolDevices) return dev_alloc(p, bytes, what);
+  if (dev < 0 || dev >= kPoolDevices) {
+    set_error("%s: device %d outside the pool table (0..%d)", what, dev, kPoolDevices - 1);
+    return EDG_ERR_CUDA;
+  }
   cudaMemPool_t pool = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_pool_mu);
@@ -101,14 +89,17 @@ int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
     }
     pool = g_pool[dev];
   }
-  size_t freeb = 0, totalb = 0, held = 0, used = 0;
-  EDG_CUDA(cudaMemGetInfo(&freeb, &totalb));
+  size_t held = 0, used = 0;
   EDG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held));
   EDG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
   const size_t idle = held > used ? held - used : 0;  // reusable without new device memory
-  if (bytes + kReserveBytes > freeb + idle) {
-    set_error("HBM admission refused for %s: %zu bytes requested, %zu free", what, bytes, freeb + idle);
-    return EDG_ERR_NOMEM;
+  if (bytes > idle) {
+    size_t freeb = 0, totalb = 0;
+    EDG_CUDA(cudaMemGetInfo(&freeb, &totalb));
+    if (bytes + kReserveBytes > freeb + idle) {
+      set_error("HBM admission refused for %s: %zu bytes requested, %zu free", what, bytes, freeb + idle);
+      return EDG_ERR_NOMEM;
+    }
   }
   cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, st);
   if (e != cudaSuccess) {
@@ -248,7 +239,7 @@ int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
   B.nel = nel;
   B.dim = int64_t(binom_host(ns, nel));
   cudaStream_t st = s->stream;
-  EDG_CHECK(B.map.alloc(B.dim, "basis map"));
+  EDG_CHECK(B.map.alloc(B.dim, st, "basis map"));
   {
     int64_t nthr = (B.dim + kEnumChunk - 1) / kEnumChunk;
     int blocks = int((nthr + 255) / 256);
@@ -268,8 +259,8 @@ int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
   }
   EnergyParams ep{};
   for (int io = 0; io < ns; ++io) ep.eps[io] = m.hre[sp][io * ns + io] - shift;
-  EDG_CHECK(B.e64.alloc(B.dim, "local energies"));
-  EDG_CHECK(B.e32.alloc(B.dim, "local energies"));
+  EDG_CHECK(B.e64.alloc(B.dim, st, "local energies"));
+  EDG_CHECK(B.e32.alloc(B.dim, st, "local energies"));
   {
     int blocks = int((B.dim + 255) / 256);
     k_local_energy<<<blocks, 256, 0, st>>>(B.map.p, B.dim, ep, B.e64.p, B.e32.p);
@@ -315,13 +306,13 @@ int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   DevBuf<double> bh;
   std::vector<int32_t> hb(2 * nb + 2);
   for (int k = 0; k < nb; ++k) { hb[2 * k] = bl.a[k]; hb[2 * k + 1] = bl.b[k]; }
-  EDG_CHECK(bonds.alloc(hb.size(), "bond list"));
-  EDG_CHECK(bh.alloc(nb + 1, "bond values"));
+  EDG_CHECK(bonds.alloc(hb.size(), st, "bond list"));
+  EDG_CHECK(bh.alloc(nb + 1, st, "bond values"));
   EDG_CUDA(cudaMemcpyAsync(bonds.p, hb.data(), hb.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   if (nb) EDG_CUDA(cudaMemcpyAsync(bh.p, bl.h.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
-  EDG_CHECK(B.off.alloc(B.dim + 1, "hop offsets"));
+  EDG_CHECK(B.off.alloc(B.dim + 1, st, "hop offsets"));
   DevBuf<uint32_t> cnt;
-  EDG_CHECK(cnt.alloc(B.dim, "hop counts"));
+  EDG_CHECK(cnt.alloc(B.dim, st, "hop counts"));
   int blocks = int((B.dim + 255) / 256);
   k_hop_count<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, nb, cnt.p);
   EDG_CUDA(cudaGetLastError());
@@ -329,15 +320,15 @@ int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   size_t tmp_bytes = 0;
   EDG_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp_bytes, cnt.p, B.off.p + 1, B.dim, st));
   DevBuf<unsigned char> tmp;
-  EDG_CHECK(tmp.alloc(tmp_bytes + 1, "scan scratch"));
+  EDG_CHECK(tmp.alloc(tmp_bytes + 1, st, "scan scratch"));
   EDG_CUDA(cub::DeviceScan::InclusiveSum(tmp.p, tmp_bytes, cnt.p, B.off.p + 1, B.dim, st));
   uint32_t nnz = 0;
   EDG_CUDA(cudaMemcpyAsync(&nnz, B.off.p + B.dim, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));
   B.nnz = nnz;
-  EDG_CHECK(B.src.alloc(nnz + 1, "hop sources"));
-  EDG_CHECK(B.val64.alloc(nnz + 1, "hop values"));
-  EDG_CHECK(B.val32.alloc(nnz + 1, "hop values"));
+  EDG_CHECK(B.src.alloc(nnz + 1, st, "hop sources"));
+  EDG_CHECK(B.val64.alloc(nnz + 1, st, "hop values"));
+  EDG_CHECK(B.val32.alloc(nnz + 1, st, "hop values"));
   k_hop_fill<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, bh.p, nb, s->binom.p, B.off.p, B.src.p, B.val64.p,
                                      B.val32.p);
   EDG_CUDA(cudaGetLastError());
@@ -504,8 +495,8 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
       B.group_max = std::max<int>(B.group_max, int(members[g].size()));
     }
     B.groups = int(G);
-    EDG_CHECK(B.group_off.alloc(G + 1, "row groups"));
-    EDG_CHECK(B.group_rows.alloc(grows.size() + 1, "row groups"));
+    EDG_CHECK(B.group_off.alloc(G + 1, st, "row groups"));
+    EDG_CHECK(B.group_rows.alloc(grows.size() + 1, st, "row groups"));
     EDG_CUDA(cudaMemcpyAsync(B.group_off.p, goff.data(), goff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     EDG_CUDA(cudaMemcpyAsync(B.group_rows.p, grows.data(), grows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     EDG_CUDA(cudaStreamSynchronize(st));
@@ -552,8 +543,8 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
     build_schedule(dim, rt32, off, src, sg, qoff, qent, &ok);
     if (ok) {
       qent.push_back(uint32_t(dim));
-      EDG_CHECK(B.sched_off.alloc(qoff.size(), "SELL schedule"));
-      EDG_CHECK(B.sched_ent.alloc(qent.size(), "SELL schedule"));
+      EDG_CHECK(B.sched_off.alloc(qoff.size(), st, "SELL schedule"));
+      EDG_CHECK(B.sched_ent.alloc(qent.size(), st, "SELL schedule"));
       EDG_CUDA(cudaMemcpyAsync(B.sched_off.p, qoff.data(), qoff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
       EDG_CUDA(cudaMemcpyAsync(B.sched_ent.p, qent.data(), qent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
       B.sched_rt = rt32;
@@ -601,15 +592,15 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
         poff[size_t(p) * (nsl + 1) + nsl] = uint32_t(base);
       }
       pent.push_back(0u);
-      EDG_CHECK(B.split_off.alloc(poff.size(), "split SELL offsets"));
-      EDG_CHECK(B.split_ent.alloc(pent.size(), "split SELL entries"));
+      EDG_CHECK(B.split_off.alloc(poff.size(), st, "split SELL offsets"));
+      EDG_CHECK(B.split_ent.alloc(pent.size(), st, "split SELL entries"));
       EDG_CUDA(cudaMemcpyAsync(B.split_off.p, poff.data(), poff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
       EDG_CUDA(cudaMemcpyAsync(B.split_ent.p, pent.data(), pent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
       if (!uniform) {
         pval.push_back(0.0);
         std::vector<float> pv32(pval.begin(), pval.end());
-        EDG_CHECK(B.split_v64.alloc(pval.size(), "split SELL values"));
-        EDG_CHECK(B.split_v32.alloc(pv32.size(), "split SELL values"));
+        EDG_CHECK(B.split_v64.alloc(pval.size(), st, "split SELL values"));
+        EDG_CHECK(B.split_v32.alloc(pv32.size(), st, "split SELL values"));
         EDG_CUDA(cudaMemcpyAsync(B.split_v64.p, pval.data(), pval.size() * sizeof(double), cudaMemcpyHostToDevice, st));
         EDG_CUDA(cudaMemcpyAsync(B.split_v32.p, pv32.data(), pv32.size() * sizeof(float), cudaMemcpyHostToDevice, st));
       }
@@ -617,14 +608,14 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
       B.split_parts = P;
     }
   }
-  EDG_CHECK(B.sell_off.alloc(nsl + 1, "SELL offsets"));
-  EDG_CHECK(B.sell_ent.alloc(ent.size(), "SELL entries"));
+  EDG_CHECK(B.sell_off.alloc(nsl + 1, st, "SELL offsets"));
+  EDG_CHECK(B.sell_ent.alloc(ent.size(), st, "SELL entries"));
   EDG_CUDA(cudaMemcpyAsync(B.sell_off.p, soff.data(), soff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   EDG_CUDA(cudaMemcpyAsync(B.sell_ent.p, ent.data(), ent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   if (!uniform) {
     std::vector<float> sv32(sv.begin(), sv.end());
-    EDG_CHECK(B.sell_v64.alloc(sv.size(), "SELL values"));
-    EDG_CHECK(B.sell_v32.alloc(sv.size(), "SELL values"));
+    EDG_CHECK(B.sell_v64.alloc(sv.size(), st, "SELL values"));
+    EDG_CHECK(B.sell_v32.alloc(sv.size(), st, "SELL values"));
     EDG_CUDA(cudaMemcpyAsync(B.sell_v64.p, sv.data(), sv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     EDG_CUDA(cudaMemcpyAsync(B.sell_v32.p, sv32.data(), sv32.size() * sizeof(float), cudaMemcpyHostToDevice, st));
   }
@@ -639,7 +630,7 @@ int sector_build(edg_sector_s* s) {
   std::vector<uint32_t> C(kBinomN * kBinomN, 0);
   for (int n = 0; n < kBinomN; ++n)
     for (int k = 0; k < kBinomN; ++k) C[n * kBinomN + k] = uint32_t(binom_host(n, k));
-  EDG_CHECK(s->binom.alloc(C.size(), "binomial table"));
+  EDG_CHECK(s->binom.alloc(C.size(), s->stream, "binomial table"));
   EDG_CUDA(cudaMemcpyAsync(s->binom.p, C.data(), C.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream));
   EDG_CHECK(build_spin(s, 1, s->up, s->nup));
   EDG_CHECK(build_spin(s, 2, s->dw, s->ndw));
@@ -656,8 +647,8 @@ int sector_build(edg_sector_s* s) {
       const BondList& bl = s->bonds[sp];
       for (int k = 0; k < bl.nb; ++k) { hb.push_back(bl.a[k]); hb.push_back(bl.b[k]); hv.push_back(bl.h[k]); }
     }
-    EDG_CHECK(s->bond_dev.alloc(hb.size() + 2, "bond list"));
-    EDG_CHECK(s->bondh_dev.alloc(hv.size() + 1, "bond values"));
+    EDG_CHECK(s->bond_dev.alloc(hb.size() + 2, s->stream, "bond list"));
+    EDG_CHECK(s->bondh_dev.alloc(hv.size() + 1, s->stream, "bond values"));
     if (!hb.empty()) {
       EDG_CUDA(cudaMemcpyAsync(s->bond_dev.p, hb.data(), hb.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
       EDG_CUDA(cudaMemcpyAsync(s->bondh_dev.p, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));

@@ -23,6 +23,31 @@ int eval_poles(int64_t npoles, const double* poles, const double* weights, int64
                const double* z_im, double* out_re, double* out_im);
 int observables(const edg_sector_s* s, const double* psi, double weight, double* dens, double* dens_up,
                 double* dens_dw, double* docc, double* magz, cudaStream_t st);
+
+// Sectors draw their stream from a per-device pool created on first use and kept until
+// exit. Creating and destroying a stream per sector (hundreds in a finite-temperature run)
+// stalled the process for up to a second at random; with the pool, up to kStreamPool sectors
+// still run concurrently on separate streams.
+constexpr int kStreamPool = 16;
+constexpr int kMaxDevices = 64;
+cudaError_t pooled_stream(int dev, cudaStream_t* out) {
+  static std::mutex mu;
+  static cudaStream_t pool[kMaxDevices][kStreamPool] = {};
+  static unsigned next[kMaxDevices] = {};
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  const unsigned slot = next[dev]++ % kStreamPool;
+  if (!pool[dev][slot]) {
+    const cudaError_t e = cudaStreamCreateWithFlags(&pool[dev][slot], cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      pool[dev][slot] = nullptr;
+      return e;
+    }
+  }
+  *out = pool[dev][slot];
+  return cudaSuccess;
+}
+
 }  // namespace edg
 
 using namespace edg;
@@ -55,30 +80,6 @@ __global__ void k_interleave(double* __restrict__ z, const double* __restrict__ 
 int grid1(int64_t n) {
   int64_t g = (n + 255) / 256;
   return int(g < 148 * 16 ? (g < 1 ? 1 : g) : 148 * 16);
-}
-
-// Sectors draw their stream from a per-device pool created on first use and kept until
-// exit. Creating and destroying a stream per sector (hundreds in a finite-temperature run)
-// stalled the process for up to a second at random; with the pool, up to kStreamPool sectors
-// still run concurrently on separate streams.
-constexpr int kStreamPool = 16;
-constexpr int kMaxDevices = 64;
-cudaError_t pooled_stream(int dev, cudaStream_t* out) {
-  static std::mutex mu;
-  static cudaStream_t pool[kMaxDevices][kStreamPool] = {};
-  static unsigned next[kMaxDevices] = {};
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(mu);
-  const unsigned slot = next[dev]++ % kStreamPool;
-  if (!pool[dev][slot]) {
-    const cudaError_t e = cudaStreamCreateWithFlags(&pool[dev][slot], cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-      pool[dev][slot] = nullptr;
-      return e;
-    }
-  }
-  *out = pool[dev][slot];
-  return cudaSuccess;
 }
 
 int check_sector(const edg_sector_s* s) {
@@ -202,6 +203,7 @@ int edg_sector_create(const edg_model* m, int nup, int ndw, int form, edg_sector
   s->form = form;
   cudaError_t e = cudaGetDevice(&s->device);
   if (e == cudaSuccess) e = pooled_stream(s->device, &s->stream);
+  s->home_stream = s->stream;
   if (e != cudaSuccess) {
     set_error("edg_sector_create: %s", cudaGetErrorString(e));
     delete s;
@@ -223,7 +225,12 @@ int edg_sector_destroy(edg_sector* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   cudaStream_t st = s->stream;
   bool own = s->own_stream;
-  delete s;  // DevBuf destructors free device memory
+  {
+    // nothing of the sector's is in flight now; its buffers go back to the pool on the
+    // library's own stream (a caller's stream set by edg_sector_set_stream may be gone)
+    FreeStreamOverride on(s->home_stream);
+    delete s;
+  }
   if (own && st) cudaStreamDestroy(st);
   return EDG_OK;
 }
@@ -239,8 +246,12 @@ int edg_sector_dims(const edg_sector* s, int64_t* dim, int64_t* dimup, int64_t* 
 int edg_sector_get_maps(const edg_sector* s, int32_t* map_up, int32_t* map_dw) {
   EDG_CHECK(check_sector(s));
   EDG_CHECK(ensure_device(s));
-  if (map_up) EDG_CUDA(cudaMemcpy(map_up, s->up.map.p, s->up.dim * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-  if (map_dw) EDG_CUDA(cudaMemcpy(map_dw, s->dw.map.p, s->dw.dim * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  cudaStream_t st = s->stream;
+  if (map_up)
+    EDG_CUDA(cudaMemcpyAsync(map_up, s->up.map.p, s->up.dim * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (map_dw)
+    EDG_CUDA(cudaMemcpyAsync(map_dw, s->dw.map.p, s->dw.dim * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
   return EDG_OK;
 }
 
@@ -254,13 +265,16 @@ int edg_sector_get_hops(const edg_sector* s, int spin, int64_t* rowptr, int32_t*
   EDG_CHECK(ensure_device(s));
   const SpinBasis& B = spin == 1 ? s->up : s->dw;
   if (nnz) *nnz = B.nnz;
-  if (rowptr) {
-    std::vector<uint32_t> off(B.dim + 1);
-    EDG_CUDA(cudaMemcpy(off.data(), B.off.p, off.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    for (size_t i = 0; i < off.size(); ++i) rowptr[i] = off[i];
-  }
-  if (cols && B.nnz) EDG_CUDA(cudaMemcpy(cols, B.src.p, B.nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-  if (vals && B.nnz) EDG_CUDA(cudaMemcpy(vals, B.val64.p, B.nnz * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaStream_t st = s->stream;
+  std::vector<uint32_t> off(rowptr ? B.dim + 1 : 0);
+  if (rowptr)
+    EDG_CUDA(cudaMemcpyAsync(off.data(), B.off.p, off.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (cols && B.nnz)
+    EDG_CUDA(cudaMemcpyAsync(cols, B.src.p, B.nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (vals && B.nnz)
+    EDG_CUDA(cudaMemcpyAsync(vals, B.val64.p, B.nnz * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < off.size(); ++i) rowptr[i] = off[i];
   return EDG_OK;
 }
 
@@ -295,8 +309,8 @@ int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv) {
           (long long)s->dim);
   EDG_CHECK(ensure_device(s));
   const int64_t n = s->dim;
-  EDG_CHECK(s->w64[0].alloc(n, "H x v input"));
-  EDG_CHECK(s->w64[1].alloc(n, "H x v output"));
+  EDG_CHECK(s->w64[0].alloc(n, s->stream, "H x v input"));
+  EDG_CHECK(s->w64[1].alloc(n, s->stream, "H x v output"));
   EDG_CUDA(cudaMemcpyAsync(s->w64[0].p, v, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   EDG_CHECK(hxv_apply<double>(s, s->w64[0].p, s->w64[1].p));
   EDG_CUDA(cudaMemcpyAsync(hv, s->w64[1].p, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -311,8 +325,8 @@ int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv) {
           (long long)s->dim);
   EDG_CHECK(ensure_device(s));
   const int64_t n = s->dim;
-  for (int k = 0; k < 4; ++k) EDG_CHECK(s->w64[k].alloc(n, "H x v work"));
-  EDG_CHECK(s->zstage.alloc(size_t(2 * n), "complex staging"));
+  for (int k = 0; k < 4; ++k) EDG_CHECK(s->w64[k].alloc(n, s->stream, "H x v work"));
+  EDG_CHECK(s->zstage.alloc(size_t(2 * n), s->stream, "complex staging"));
   double* stage = s->zstage.p;
   EDG_CUDA(cudaMemcpyAsync(stage, v, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   k_deinterleave<<<grid1(n), 256, 0, s->stream>>>(stage, s->w64[0].p, s->w64[1].p, n);
@@ -341,7 +355,7 @@ int edg_tridiag_d(edg_sector* s, const double* vvinit, int nlanc, double thresho
   EDG_CHECK(check_sector(s));
   EDG_ARG(vvinit, "edg_tridiag_d: NULL start vector");
   EDG_CHECK(ensure_device(s));
-  EDG_CHECK(s->w64[3].alloc(s->dim, "start vector"));
+  EDG_CHECK(s->w64[3].alloc(s->dim, s->stream, "start vector"));
   EDG_CUDA(cudaMemcpyAsync(s->w64[3].p, vvinit, s->dim * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   return edg_tridiag_dev_f64(s, s->w64[3].p, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
 }
@@ -403,7 +417,8 @@ int edg_state_get(const edg_sector* s, double* evec) {
     return EDG_ERR_STATE;
   }
   EDG_CHECK(ensure_device(s));
-  EDG_CUDA(cudaMemcpy(evec, s->state.p, s->dim * sizeof(double), cudaMemcpyDeviceToHost));
+  EDG_CUDA(cudaMemcpyAsync(evec, s->state.p, s->dim * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EDG_CUDA(cudaStreamSynchronize(s->stream));
   return EDG_OK;
 }
 
@@ -411,8 +426,9 @@ int edg_state_set(edg_sector* s, const double* evec) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(evec, "edg_state_set: NULL");
   EDG_CHECK(ensure_device(s));
-  EDG_CHECK(s->state.alloc(s->dim, "state"));
-  EDG_CUDA(cudaMemcpy(s->state.p, evec, s->dim * sizeof(double), cudaMemcpyHostToDevice));
+  EDG_CHECK(s->state.alloc(s->dim, s->stream, "state"));
+  EDG_CUDA(cudaMemcpyAsync(s->state.p, evec, s->dim * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EDG_CUDA(cudaStreamSynchronize(s->stream));
   s->has_state = true;
   return EDG_OK;
 }
@@ -495,6 +511,11 @@ int edg_tridiag_eigh(int n, const double* d, const double* e, double* w, double*
   return tridiag_eigh_host(n, d, e, w, z1, nullptr);
 }
 
+int edg_tridiag_lowest(int n, const double* d, const double* e, int k, double* w, double* zn) {
+  EDG_ARG(n >= 0 && k >= 0 && (n == 0 || k == 0 || (d && e && w)), "edg_tridiag_lowest: bad arguments");
+  return tridiag_lowest_host(n, d, e, k, w, zn);
+}
+
 int edg_poles_weights(int n, const double* alanc, const double* blanc, double norm2, double ei, int isign,
                       double* poles, double* weights) {
   EDG_ARG(n >= 0 && (n == 0 || (alanc && blanc && poles && weights)), "edg_poles_weights: bad arguments");
@@ -526,7 +547,7 @@ int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int s
     set_error("edg_gf_chain: origin sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(to->w64[3].alloc(to->dim, "excitation vector"));
+  EDG_CHECK(to->w64[3].alloc(to->dim, to->stream, "excitation vector"));
   EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, site, spin, 1.0, 0, from->state.p, to->w64[3].p));
   if (site2 > 0)
     EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, site2, spin, 1.0, 1, from->state.p, to->w64[3].p));
@@ -541,7 +562,7 @@ int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qc
     set_error("edg_chi_chain: sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(s->w64[3].alloc(s->dim, "excitation vector"));
+  EDG_CHECK(s->w64[3].alloc(s->dim, s->stream, "excitation vector"));
   EDG_CHECK(edg_apply_diagop_dev_f64(s, kind, site, site2, qcos, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);
 }
@@ -554,7 +575,7 @@ int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* pol
     set_error("edg_oc_chain: sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(s->w64[3].alloc(s->dim, "excitation vector"));
+  EDG_CHECK(s->w64[3].alloc(s->dim, s->stream, "excitation vector"));
   EDG_CHECK(edg_apply_current_dev_f64(s, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);
 }

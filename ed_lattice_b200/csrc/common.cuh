@@ -34,50 +34,55 @@ const char* get_error();
     if (s_ != EDG_OK) return s_; \
   } while (0)
 
-// Device allocation with HBM admission: refuse when the request would leave less than
-// `reserve` bytes free, instead of letting cudaMalloc fail half-way through a pipeline.
-int dev_alloc(void** p, size_t bytes, const char* what);
-void dev_free(void* p);
-
-// Stream-ordered buffers from a per-device pool that keeps freed memory for reuse (large,
-// short-lived solver work space); freed on the same stream when the owner goes out of scope.
+// Stream-ordered buffers from a per-device pool that keeps freed memory for reuse; freed on
+// the same stream when the owner goes out of scope. Every device buffer of the library comes
+// from this pool: on a machine whose driver is busy with other processes, a plain
+// cudaMalloc/cudaFree pair took up to 0.8 s, and a finite-temperature loop makes hundreds.
 int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what);
 void pool_free(void* p, cudaStream_t st);
 
-template <typename T>
-struct PoolBuf {
-  T* p = nullptr;
-  cudaStream_t st = nullptr;
-  PoolBuf() = default;
-  PoolBuf(const PoolBuf&) = delete;
-  PoolBuf& operator=(const PoolBuf&) = delete;
-  ~PoolBuf() { pool_free(p, st); }
-  int alloc(size_t count, cudaStream_t stream, const char* what) {
-    pool_free(p, st);
-    p = nullptr;
-    st = stream;
-    return pool_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), stream, what);
-  }
+// While one of these is alive on a thread, buffers released on that thread go back to the
+// pool on `st` instead of the stream they were last allocated on. The sector destructor
+// uses it after synchronising the sector's stream: a stream that a caller handed to the
+// sector may no longer exist by then.
+struct FreeStreamOverride {
+  explicit FreeStreamOverride(cudaStream_t st);
+  ~FreeStreamOverride();
+  FreeStreamOverride(const FreeStreamOverride&) = delete;
+  FreeStreamOverride& operator=(const FreeStreamOverride&) = delete;
+  cudaStream_t prev;
+  bool prev_set;
 };
+cudaStream_t free_stream(cudaStream_t recorded);
 
+// One of a per-device set of library-owned streams, handed out round robin and never
+// destroyed (creating a stream per sector stalled sector loops like cudaMalloc does).
+cudaError_t pooled_stream(int dev, cudaStream_t* out);
+
+
+// A device buffer that grows on demand. Allocation and release are ordered on the stream
+// of the latest alloc() call: work queued on other streams must be finished (or ordered
+// before that stream) when the buffer grows or is destroyed.
 template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { reset(); }
-  int alloc(size_t count, const char* what) {
+  int alloc(size_t count, cudaStream_t stream, const char* what) {
+    st = stream;
     if (n >= count && p) return EDG_OK;
     reset();
     if (count == 0) return EDG_OK;
-    int s = dev_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), what);
+    int s = pool_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), stream, what);
     if (s == EDG_OK) n = count;
     return s;
   }
   void reset() {
-    if (p) dev_free(p);
+    if (p) pool_free(p, free_stream(st));
     p = nullptr;
     n = 0;
   }
@@ -167,6 +172,7 @@ struct edg_sector_s {
   edg::DevBuf<double> bondh_dev;
   double U = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t home_stream = nullptr;  // the library stream the sector was created on
   bool own_stream = false;
   // work space of the Lanczos drivers (grown on demand, freed with the sector)
   edg::DevBuf<double> w64[4];
@@ -259,5 +265,10 @@ int sector_dense_dev(edg_sector_s* s, double* dH);
 // zn (optional): last components of the eigenvectors (Ritz residual estimates b*|zn|).
 int tridiag_eigh_host(int n, const double* d, const double* e, double* w, double* z1, double* zfull,
                       double* zn = nullptr);
+// k lowest eigenvalues and |last eigenvector components| (bisection + twisted factorisation)
+int tridiag_lowest_host(int n, const double* d, const double* e, int k, double* w, double* zn);
+// k lowest eigenpairs (vectors z[k][n]) by bisection + twisted factorisation; EDG_ERR_NOCONV
+// when two of the k+1 lowest eigenvalues are closer than relgap * spectral radius
+int tridiag_lowest_vectors(int n, const double* d, const double* e, int k, double relgap, double* w, double* z);
 
 }  // namespace edg

@@ -64,24 +64,29 @@ __global__ void k_eval_sum(const double* __restrict__ part, int nchunks, int64_t
 int eval_poles(int64_t npoles, const double* poles, const double* weights, int64_t nz, const double* z_re,
                const double* z_im, double* out_re, double* out_im) {
   if (npoles == 0 || nz == 0) return EDG_OK;
+  int dev = 0;
+  EDG_CUDA(cudaGetDevice(&dev));
+  cudaStream_t st = nullptr;
+  EDG_CUDA(pooled_stream(dev, &st));
   DevBuf<double> dp, dw, dzr, dzi, part, out;
-  EDG_CHECK(dp.alloc(npoles, "poles"));
-  EDG_CHECK(dw.alloc(npoles, "weights"));
-  EDG_CHECK(dzr.alloc(nz, "frequencies"));
-  EDG_CHECK(dzi.alloc(nz, "frequencies"));
+  EDG_CHECK(dp.alloc(npoles, st, "poles"));
+  EDG_CHECK(dw.alloc(npoles, st, "weights"));
+  EDG_CHECK(dzr.alloc(nz, st, "frequencies"));
+  EDG_CHECK(dzi.alloc(nz, st, "frequencies"));
   const int chunks = int(npoles < kEvalChunks ? npoles : kEvalChunks);
-  EDG_CHECK(part.alloc(size_t(chunks) * nz * 2, "pole-sum partials"));
-  EDG_CHECK(out.alloc(size_t(nz) * 2, "pole sums"));
-  EDG_CUDA(cudaMemcpy(dp.p, poles, npoles * sizeof(double), cudaMemcpyHostToDevice));
-  EDG_CUDA(cudaMemcpy(dw.p, weights, npoles * sizeof(double), cudaMemcpyHostToDevice));
-  EDG_CUDA(cudaMemcpy(dzr.p, z_re, nz * sizeof(double), cudaMemcpyHostToDevice));
-  EDG_CUDA(cudaMemcpy(dzi.p, z_im, nz * sizeof(double), cudaMemcpyHostToDevice));
+  EDG_CHECK(part.alloc(size_t(chunks) * nz * 2, st, "pole-sum partials"));
+  EDG_CHECK(out.alloc(size_t(nz) * 2, st, "pole sums"));
+  EDG_CUDA(cudaMemcpyAsync(dp.p, poles, npoles * sizeof(double), cudaMemcpyHostToDevice, st));
+  EDG_CUDA(cudaMemcpyAsync(dw.p, weights, npoles * sizeof(double), cudaMemcpyHostToDevice, st));
+  EDG_CUDA(cudaMemcpyAsync(dzr.p, z_re, nz * sizeof(double), cudaMemcpyHostToDevice, st));
+  EDG_CUDA(cudaMemcpyAsync(dzi.p, z_im, nz * sizeof(double), cudaMemcpyHostToDevice, st));
   dim3 grid(unsigned((nz + kEvalThreads - 1) / kEvalThreads), unsigned(chunks));
-  k_eval_poles<<<grid, kEvalThreads>>>(dp.p, dw.p, npoles, dzr.p, dzi.p, nz, part.p);
-  k_eval_sum<<<unsigned((nz + 255) / 256), 256>>>(part.p, chunks, nz, out.p);
+  k_eval_poles<<<grid, kEvalThreads, 0, st>>>(dp.p, dw.p, npoles, dzr.p, dzi.p, nz, part.p);
+  k_eval_sum<<<unsigned((nz + 255) / 256), 256, 0, st>>>(part.p, chunks, nz, out.p);
   EDG_CUDA(cudaGetLastError());
   std::vector<double> h(size_t(nz) * 2);
-  EDG_CUDA(cudaMemcpy(h.data(), out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  EDG_CUDA(cudaMemcpyAsync(h.data(), out.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
   for (int64_t m = 0; m < nz; ++m) {
     out_re[m] += h[2 * m];
     out_im[m] += h[2 * m + 1];

@@ -230,8 +230,8 @@ int apply_cop(const edg_sector_s* from, const edg_sector_s* to, int op, int site
   const SpinBasis& BJ = spin == 1 ? to->up : to->dw;
   DevBuf<int64_t> src;
   DevBuf<double> sg;
-  EDG_CHECK(src.alloc(BJ.dim, "c-op table"));
-  EDG_CHECK(sg.alloc(BJ.dim, "c-op table"));
+  EDG_CHECK(src.alloc(BJ.dim, st, "c-op table"));
+  EDG_CHECK(sg.alloc(BJ.dim, st, "c-op table"));
   k_cop_table<<<int((BJ.dim + 255) / 256), 256, 0, st>>>(BJ.map.p, BJ.dim, pos, op, to->binom.p, src.p, sg.p);
   EDG_CUDA(cudaGetLastError());
   if (spin == 1) {
@@ -250,9 +250,9 @@ int apply_diagop(const edg_sector_s* s, int kind, const double* wsite, const dou
                  cudaStream_t st) {
   const int ns = s->model.ns;
   DevBuf<double> w, fu, fd;
-  EDG_CHECK(w.alloc(ns, "site weights"));
-  EDG_CHECK(fu.alloc(s->up.dim, "site sums"));
-  EDG_CHECK(fd.alloc(s->dw.dim, "site sums"));
+  EDG_CHECK(w.alloc(ns, st, "site weights"));
+  EDG_CHECK(fu.alloc(s->up.dim, st, "site sums"));
+  EDG_CHECK(fd.alloc(s->dw.dim, st, "site sums"));
   EDG_CUDA(cudaMemcpyAsync(w.p, wsite, ns * sizeof(double), cudaMemcpyHostToDevice, st));
   k_site_sum<<<int((s->up.dim + 255) / 256), 256, 0, st>>>(s->up.map.p, s->up.dim, w.p, ns, fu.p);
   k_site_sum<<<int((s->dw.dim + 255) / 256), 256, 0, st>>>(s->dw.map.p, s->dw.dim, w.p, ns, fd.p);
@@ -294,7 +294,7 @@ int observables(const edg_sector_s* s, const double* psi, double weight, double*
   const int ns = s->model.ns;
   const int g = grid_rows(s->dw.dim);
   DevBuf<double> part;
-  EDG_CHECK(part.alloc(size_t(g) * 3 * kMaxSites, "observable partials"));
+  EDG_CHECK(part.alloc(size_t(g) * 3 * kMaxSites, st, "observable partials"));
   k_obs_rows<<<g, 256, 0, st>>>(psi, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, ns, part.p);
   EDG_CUDA(cudaGetLastError());
   std::vector<double> h(size_t(g) * 3 * kMaxSites);
@@ -327,11 +327,11 @@ int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, doub
   cudaStream_t st = s->stream;
   std::vector<double> dens(ns, 0.0), nup(ns, 0.0), ndw(ns, 0.0), docc(ns, 0.0);
   EDG_CHECK(observables(s, psi, 1.0, dens.data(), nup.data(), ndw.data(), docc.data(), nullptr, st));
-  EDG_CHECK(s->w64[0].alloc(n, "energy work vector"));
+  EDG_CHECK(s->w64[0].alloc(n, st, "energy work vector"));
   double* hv = s->w64[0].p;
   EDG_CHECK(hxv_apply<double>(s, psi, hv));
   DevBuf<double> part;
-  EDG_CHECK(part.alloc(size_t(kRedBlocks) + kDiagBlocks + 4, "energy partials"));
+  EDG_CHECK(part.alloc(size_t(kRedBlocks) + kDiagBlocks + 4, st, "energy partials"));
   double* out = part.p + kRedBlocks + kDiagBlocks;
   EDG_CHECK(dot_dev<double>(st, psi, hv, n, part.p, out));
   k_diag_dot<<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, n, s->up.e64.p, s->dw.e64.p, s->up.map.p, s->dw.map.p,

@@ -39,7 +39,7 @@ struct Scalars {
 
 int scalars(edg_sector_s* s, int cap, Scalars* sc) {
   const size_t need = size_t(kRedBlocks) + 3 * size_t(cap + 2) + 8;
-  EDG_CHECK(s->red.alloc(need, "reduction scratch"));
+  EDG_CHECK(s->red.alloc(need, s->stream, "reduction scratch"));
   sc->partial = s->red.p;
   sc->a = sc->partial + kRedBlocks;
   sc->b = sc->a + cap + 2;
@@ -85,7 +85,7 @@ struct Recurrence {
     EDG_CHECK(scalars(s, cap, &sc));
     DevBuf<T>* wb = work<T>(s);
     for (int k = 0; k < 3; ++k) {
-      EDG_CHECK(wb[k].alloc(n, "Lanczos vectors"));
+      EDG_CHECK(wb[k].alloc(n, s->stream, "Lanczos vectors"));
       wbuf[k] = wb[k].p;
     }
     U = wb[0].p;
@@ -361,8 +361,8 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
   cudaStream_t st = s->stream;
   if (maxit <= 0) maxit = 1;
   if (maxit > n) maxit = int(n);
-  EDG_CHECK(s->state.alloc(n, "eigenvector"));
-  EDG_CHECK(s->w64[3].alloc(n, "start vector"));
+  EDG_CHECK(s->state.alloc(n, st, "eigenvector"));
+  EDG_CHECK(s->w64[3].alloc(n, st, "start vector"));
   double* x0 = s->w64[3].p;
   if (v0_host) {
     EDG_CUDA(cudaMemcpyAsync(x0, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -399,7 +399,7 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
       if (size_t(cols) > s->basis32_cols) {
         s->basis32.reset();
         s->basis32_cols = 0;
-        if (cols > 0 && s->basis32.alloc(size_t(cols) * n, "FP32 Lanczos basis") == EDG_OK) s->basis32_cols = cols;
+        if (cols > 0 && s->basis32.alloc(size_t(cols) * n, st, "FP32 Lanczos basis") == EDG_OK) s->basis32_cols = cols;
       }
     }
     const int cols = int(s->basis32_cols);

@@ -165,13 +165,18 @@ int sector_dense(edg_sector_s* s, double* H_host) {
     return EDG_ERR_ARG;
   }
   DevBuf<double> Hd;
-  EDG_CHECK(Hd.alloc(size_t(D) * D, "dense sector matrix"));
+  EDG_CHECK(Hd.alloc(size_t(D) * D, s->stream, "dense sector matrix"));
   EDG_CHECK(sector_dense_dev(s, Hd.p));
   cudaStream_t st = s->stream;
   EDG_CUDA(cudaMemcpyAsync(H_host, Hd.p, size_t(D) * D * sizeof(double), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));
   return EDG_OK;
 }
+
+// Eigenvalues of T closer than this fraction of its spectral radius get their Ritz
+// coefficients from the QL eigenvector matrix (the twisted-factorisation vectors of such a
+// pair are accurate to about eps / kRitzRelGap only).
+constexpr double kRitzRelGap = 1e-5;
 
 int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, double* evals,
              double* evecs_host, double* resid, int* niter) {
@@ -196,13 +201,13 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     }
   }
   // device: basis Q[mmax][n], w, scratch
-  PoolBuf<double> Q, X;
+  DevBuf<double> Q, X;
   DevBuf<double> w, part, coef, Zd;
   EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
-  EDG_CHECK(w.alloc(n, "Lanczos vector"));
+  EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
   const int nblk = std::min<int64_t>(592, (n + kLkThreads - 1) / kLkThreads);
-  EDG_CHECK(part.alloc(size_t(mmax + 1) * nblk + kRedBlocks, "multi-dot partials"));
-  EDG_CHECK(coef.alloc(size_t(mmax) + 8, "multi-dot coefficients"));
+  EDG_CHECK(part.alloc(size_t(mmax + 1) * nblk + kRedBlocks, st, "multi-dot partials"));
+  EDG_CHECK(coef.alloc(size_t(mmax) + 8, st, "multi-dot coefficients"));
   // start vector
   if (v0_host) {
     EDG_CUDA(cudaMemcpyAsync(Q.p, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -210,7 +215,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     EDG_CHECK(random_dev(st, Q.p, n, seed));
   }
   DevBuf<double> dab;  // a_j at [j], b_{j+1} at [mmax + 1 + j + 1]
-  EDG_CHECK(dab.alloc(2 * size_t(mmax) + 4, "Lanczos scalars"));
+  EDG_CHECK(dab.alloc(2 * size_t(mmax) + 4, st, "Lanczos scalars"));
   double* dA = dab.p;
   double* dB = dab.p + mmax + 1;
   EDG_CHECK(norm_dev(st, Q.p, n, part.p, dB));
@@ -224,7 +229,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   EDG_CHECK((scale_inplace_dev<double>(st, Q.p, n, 1.0 / nrm)));
   // Steps are queued without waiting on the host: the scalars stay on the device (v_{j+1} =
   // w / b_{j+1} reads b from there) and the host reads them only when it tests convergence,
-  // every max(1, m/32) steps past the first k. Each step reorthogonalises against the whole
+  // every max(1, m/32) steps past the first k (more while far from convergence). Each step reorthogonalises against the whole
   // basis by classical Gram-Schmidt applied twice: one pass lost orthogonality entirely on
   // small sectors, and the test of Daniel, Gragg, Kaufman & Stewart (Math. Comp. 30 (1976)
   // 772) asked for the second pass at nearly every step (|a_j| is well above b_j for the
@@ -259,22 +264,44 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
       B.assign(1, 0.0);
       for (int t = 1; t < m; ++t) B.push_back(hB[t]);
       const double b = hB[m];
-      std::vector<double> th(m), zl(m);
-      EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
-      zlast = zl;
-      blast = b;
-      bool conv = m >= k;
-      for (int i = 0; i < k && conv; ++i)
-        if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) conv = false;
+      auto converged = [&](const std::vector<double>& th, const std::vector<double>& zl) {
+        if (m < k) return false;
+        for (int i = 0; i < k; ++i)
+          if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) return false;
+        return true;
+      };
+      // the O(k m) test between steps; the QL eigenvectors confirm it before the loop stops
+      std::vector<double> th(std::max(m, k)), zl(std::max(m, k));
+      bool conv = false;
+      double worst = 0.0;  // largest b|z_i| / (tol max(1,|theta_i|)) over the k pairs
+      if (!last && tridiag_lowest_host(m, A.data(), B.data(), std::min(k, m), th.data(), zl.data()) == EDG_OK) {
+        conv = converged(th, zl);
+        for (int i = 0; i < std::min(k, m); ++i)
+          worst = std::max(worst, b * std::fabs(zl[i]) / (tol * std::max(1.0, std::fabs(th[i]))));
+      }
+      if (conv || last) {
+        EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
+        conv = converged(th, zl);
+        zlast = zl;
+        blast = b;
+      }
       if (conv || last) break;
-      next_check = m + std::max(1, m / 32);
+      // Ritz residuals fall by a modest factor per step, so far from the tolerance the
+      // next few steps run without a test (steps past convergence cost less than tests)
+      int gap = std::max(1, m / 32);
+      if (worst > 1e6) gap = std::max(gap, 8);
+      else if (worst > 1e3) gap = std::max(gap, 3);
+      next_check = m + gap;
     }
     EDG_CHECK(scale_into<double>(st, Q.p + size_t(m) * n, w.p, dB + m, n));
   }
   if (niter) *niter = m;
-  std::vector<double> th(m), Z(size_t(m) * m);
-  EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, Z.data()));
   const int kk = std::min(k, m);
+  // the kk lowest eigenvectors of T by twisted factorisation, O(kk m), when their eigenvalues
+  // stand apart; the full QL eigenvector matrix, O(m^3), when two of them are close
+  std::vector<double> th(m), Z(size_t(m) * m);
+  if (tridiag_lowest_vectors(m, A.data(), B.data(), kk, kRitzRelGap, th.data(), Z.data()) != EDG_OK)
+    EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, Z.data()));
   for (int i = 0; i < kk; ++i) evals[i] = th[i];
   for (int i = kk; i < k; ++i) evals[i] = NAN;
   if (resid) {
@@ -282,9 +309,9 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     for (int i = kk; i < k; ++i) resid[i] = NAN;
   }
   if (evecs_host) {
-    EDG_CHECK(Zd.alloc(size_t(m) * m, "Ritz coefficients"));
+    EDG_CHECK(Zd.alloc(size_t(m) * kk, st, "Ritz coefficients"));
     EDG_CHECK(X.alloc(size_t(kk) * n, st, "Ritz vectors"));
-    EDG_CUDA(cudaMemcpyAsync(Zd.p, Z.data(), size_t(m) * m * sizeof(double), cudaMemcpyHostToDevice, st));
+    EDG_CUDA(cudaMemcpyAsync(Zd.p, Z.data(), size_t(m) * kk * sizeof(double), cudaMemcpyHostToDevice, st));
     k_ritz_k<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p, m, kk, n, X.p);
     EDG_CUDA(cudaGetLastError());
     EDG_CUDA(cudaMemcpyAsync(evecs_host, X.p, size_t(kk) * n * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -12,11 +12,19 @@ The eigenpairs of each sector come from the device: edg_lowest_k for the sp_eigh
 branch, edg_ground_state for lanc_method="lanczos", and for dim <= lanc_dim_threshold the dense
 sector matrix of edg_sector_dense_dev handed to the device dense eigensolver (the LAPACK
 branch). ed_twin (twin-sector symmetry) is not supported: every sector is visited.
+
+Sectors are independent, so the device solves several at once: a pool of host threads takes
+them largest first, each on its own library stream, and a sector starts only when the HBM
+it needs is free (SectorScheduler). Small sectors are bound by launch and synchronisation
+latency, which overlaps across threads. The state list is assembled in sector order
+afterwards, so the result does not depend on the order in which sectors finish.
 """
 from __future__ import annotations
 
 import bisect
 import math
+import threading
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -150,6 +158,7 @@ class DiagParams:
     lanc_tolerance: float = 1e-10    # LANC_TOLERANCE
     lanc_dim_threshold: int = 1024   # LANC_DIM_THRESHOLD
     lanc_nstates_total: int = 1      # set by setup()
+    sector_threads: int = 4          # sectors solved at once on one device (no reference key)
 
     def setup(self, nsectors: int) -> "DiagParams":
         """State counts of the Lanczos method (src/SETUP.f90:89-104): at finite T an even
@@ -203,6 +212,92 @@ def device_solver(model: Model, nup: int, ndw: int, neigen: int, lanc_solve: boo
         sec.delete()
 
 
+def sector_device_bytes(dim: int, neigen: int, lanc_solve: bool, params: DiagParams) -> int:
+    """Device memory one sector solve holds at its peak, in bytes: the Lanczos basis of
+    edg_lowest_k (min(lanc_niter, dim) vectors) plus its Ritz vectors and work vectors, the
+    ground-state vectors of edg_ground_state, or the dense matrix with the eigensolver's
+    copy and workspace. The hop tables of a sector are small beside these."""
+    if not lanc_solve:
+        return 3 * dim * dim * 8 + (1 << 20)
+    if params.lanc_method == "lanczos":
+        return 8 * dim * 8 + (1 << 20)
+    return (min(params.lanc_niter, dim) + neigen + 4) * dim * 8 + (1 << 20)
+
+
+class SectorScheduler:
+    """Admits sector solves by device memory: a solve starts when its byte estimate fits in
+    what is left of `capacity`, and a solve larger than the whole capacity runs alone."""
+
+    def __init__(self, capacity: int):
+        self.capacity = max(int(capacity), 1)
+        self.free = self.capacity
+        self.cv = threading.Condition()
+
+    def acquire(self, nbytes: int) -> int:
+        need = min(int(nbytes), self.capacity)
+        with self.cv:
+            while self.free < need:
+                self.cv.wait()
+            self.free -= need
+        return need
+
+    def release(self, held: int) -> None:
+        with self.cv:
+            self.free += held
+            self.cv.notify_all()
+
+
+def _device_capacity() -> int:
+    """Free HBM of the current device less a 2 GB reserve (the library's own admission
+    checks keep a further margin)."""
+    import torch
+
+    free, _ = torch.cuda.mem_get_info()
+    return max(free - (2 << 30), 1)
+
+
+def solve_sectors(model: Model, jobs, params: DiagParams, seed: int, solver=None, threads: int | None = None,
+                  capacity: int | None = None) -> dict:
+    """Runs solver(model, nup, ndw, neigen, lanc_solve, params, seed) over `jobs`, a list of
+    (key, nup, ndw, neigen, lanc_solve); returns {key: (evals, evecs)}.
+
+    `threads` solves run at once (default: params.sector_threads for the device solver, 1
+    for a caller-supplied one), largest sector first, each admitted by SectorScheduler
+    against `capacity` bytes (default: the device's free HBM). With one thread the jobs run
+    in the given order. The first failure in job order is raised once every started solve
+    has ended."""
+    fn = solver or device_solver
+    if threads is None:
+        threads = params.sector_threads if solver is None else 1
+    if threads <= 1 or len(jobs) <= 1:
+        return {key: fn(model, nup, ndw, ne, lz, params, seed) for key, nup, ndw, ne, lz in jobs}
+    import torch
+
+    on_gpu = torch.cuda.is_available()
+    dev = torch.cuda.current_device() if on_gpu else None
+    if on_gpu and solver is None and any(not job[4] for job in jobs):
+        # torch loads its dense eigensolver on first use, and that first use must not
+        # happen on several threads at once
+        torch.linalg.eigh(torch.ones((1, 1), dtype=torch.float64, device=torch.device("cuda", dev)))
+    sched = SectorScheduler(capacity if capacity is not None else _device_capacity())
+    ns = model.ns
+
+    def run(job):
+        key, nup, ndw, ne, lz = job
+        if on_gpu:
+            torch.cuda.set_device(dev)
+        held = sched.acquire(sector_device_bytes(math.comb(ns, nup) * math.comb(ns, ndw), ne, lz, params))
+        try:
+            return fn(model, nup, ndw, ne, lz, params, seed)
+        finally:
+            sched.release(held)
+
+    order = sorted(range(len(jobs)), key=lambda i: -math.comb(ns, jobs[i][1]) * math.comb(ns, jobs[i][2]))
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        futs = {i: ex.submit(run, jobs[i]) for i in order}
+    return {job[0]: futs[i].result() for i, job in enumerate(jobs)}
+
+
 # ----------------------------------------------------------------------------- ranks
 def _rank_world(comm):
     """(rank, world size) of a torch.distributed process group, (0, 1) without one."""
@@ -249,14 +344,13 @@ def diagonalize_lattice(model: Model, params: DiagParams, seed: int = 1234, solv
     skipping those of the wrong filling when ED_FILLING != 0). Returns (state_list, eig_list)
     where eig_list holds (isector, evals, lanc_solve) per visited sector, the content of
     eigenvalues_list.ed. `solver(model, nup, ndw, neigen, lanc_solve, params, seed)` returns
-    (evals, evecs); the default runs on the device.
+    (evals, evecs); the default runs on the device, params.sector_threads sectors at once.
 
     With a torch.distributed group `comm`, the visited sectors are dealt round-robin to the
     ranks (independent units, one GPU each). Each rank solves its own sectors and keeps their
     vectors; the eigenvalues are all-gathered so that every rank builds the same state list,
     in the same sector order as one process would. A state's vector lives on its owner rank
     only (EState.vec is None elsewhere); lanc_observables sums over ranks."""
-    solver = solver or device_solver
     rank, world = _rank_world(comm)
     ns = model.ns
     nsectors = (ns + 1) ** 2
@@ -272,10 +366,10 @@ def diagonalize_lattice(model: Model, params: DiagParams, seed: int = 1234, solv
         lanc_solve = not (neigen == dim or dim <= params.lanc_dim_threshold)
         visit.append((isector, nup, ndw, neigen, lanc_solve))
     mine, vectors = [], {}
-    for pos, (isector, nup, ndw, neigen, lanc_solve) in enumerate(visit):
-        if pos % world != rank:
-            continue
-        evals, evecs = solver(model, nup, ndw, neigen, lanc_solve, params, seed)
+    jobs = [v for pos, v in enumerate(visit) if pos % world == rank]
+    results = solve_sectors(model, jobs, params, seed, solver)
+    for isector, nup, ndw, neigen, lanc_solve in jobs:
+        evals, evecs = results[isector]
         evals = np.asarray(evals, dtype=np.float64)[:neigen]
         mine.append((isector, evals))
         if keep_vectors and evecs is not None:

@@ -322,6 +322,17 @@ def tridiag_eigh(d: np.ndarray, e: np.ndarray):
     return w, z
 
 
+def tridiag_lowest(d: np.ndarray, e: np.ndarray, k: int):
+    """k lowest eigenvalues of the tridiagonal (e[0] ignored) and |last component| of each
+    unit eigenvector."""
+    d, e = _f64(d), _f64(e)
+    n = d.size
+    kk = min(k, n)
+    w, zn = np.zeros(kk), np.zeros(kk)
+    L.check(L.lib().edg_tridiag_lowest(n, _pd(d), _pd(e), kk, _pd(w), _pd(zn)), "tridiag_lowest")
+    return w, zn
+
+
 def poles_weights(alanc, blanc, norm2: float, ei: float, isign: int):
     """add_to_lanczos_gf_normal's loop (src/GF/GF_ELECTRONS.f90:445-456)."""
     a, b = _f64(alanc), _f64(blanc)

@@ -248,6 +248,12 @@ int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc,
  * src/GF/GF_ELECTRONS.f90:447): FP64 implicit QL, eigenvalues ascending; z1 receives the
  * first component of each eigenvector (may be NULL). d[n], e[n] with e[0] ignored. */
 int edg_tridiag_eigh(int n, const double* d, const double* e, double* w, double* z1);
+/* The k lowest eigenvalues of the same tridiagonal, ascending, and the magnitude of the last
+ * component of each unit eigenvector (zn, may be NULL): Sturm bisection and a twisted
+ * factorisation, O(k n). Stands in for the Ritz-residual test |b z_n| of ARPACK's dsaupd
+ * reverse-communication loop (sp_eigh at src/DIAG/DIAG.f90:191-202); edg_lowest_k uses it
+ * between steps and confirms with the QL eigenvectors before it stops. */
+int edg_tridiag_lowest(int n, const double* d, const double* e, int k, double* w, double* zn);
 /* poles/weights from (a,b,norm2): the loop of add_to_lanczos_gf_normal (:451-456). */
 int edg_poles_weights(int n, const double* alanc, const double* blanc, double norm2, double ei,
                       int isign, double* poles, double* weights);

@@ -117,3 +117,77 @@ def test_null_handles_are_errors_not_crashes():
     assert lib.edg_hxv_d(None, 1, None, None) == L.EDG_ERR_ARG
     assert lib.edg_sector_destroy(None) == L.EDG_OK
     assert lib.edg_model_destroy(None) == L.EDG_OK
+
+
+def _lanczos_tridiag(h, m, seed):
+    """a, b (b[0] = 0) of m steps of fully reorthogonalised Lanczos on the dense h."""
+    rng = np.random.default_rng(seed)
+    q = rng.standard_normal(h.shape[0])
+    Q = [q / np.linalg.norm(q)]
+    a, b = [], [0.0]
+    for j in range(m):
+        w = h @ Q[j]
+        a.append(Q[j] @ w)
+        for _ in range(2):
+            w -= np.array(Q).T @ (np.array(Q) @ w)
+        bj = np.linalg.norm(w)
+        if j + 1 < m:
+            b.append(bj)
+            Q.append(w / bj)
+    return np.array(a), np.array(b)
+
+
+@pytest.mark.parametrize("n,k,seed", [(1, 4, 0), (2, 1, 1), (7, 3, 2), (60, 4, 3), (230, 8, 4)])
+def test_tridiag_lowest_vs_numpy(n, k, seed):
+    """edg_tridiag_lowest: the k lowest eigenvalues and |last eigenvector components| of a
+    random tridiagonal against numpy's dense eigh."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=n) * 3 - 20
+    e = np.abs(rng.normal(size=n)) + 0.3
+    e[0] = 0.0
+    T = np.diag(d) + np.diag(e[1:], 1) + np.diag(e[1:], -1)
+    wr, V = np.linalg.eigh(T)
+    w, zn = E.tridiag_lowest(d, e, k)
+    kk = min(k, n)
+    span = np.abs(wr).max()
+    assert w.shape == (kk,)
+    assert np.abs(w - wr[:kk]).max() <= 4e-15 * span
+    assert np.abs(zn - np.abs(V[-1, :kk])).max() <= 1e-12
+
+
+def test_tridiag_lowest_on_converged_lanczos():
+    """A Lanczos tridiagonal whose lowest Ritz values have converged: their last components
+    are tiny, and the twisted factorisation keeps them to high relative accuracy; QL's last
+    row holds them to absolute accuracy, so both agree to ~1e-15 absolute."""
+    rng = np.random.default_rng(9)
+    n = 400
+    A = rng.standard_normal((n, n))
+    h = (A + A.T) / 2 + np.diag(np.linspace(-40, 0, n))
+    a, b = _lanczos_tridiag(h, 150, 1)
+    w, zn = E.tridiag_lowest(a, b, 4)
+    wq, Zq = O.tridiag_eigh(a, b)
+    wr = np.linalg.eigvalsh(h)
+    assert np.abs(w - wq[:4]).max() <= 1e-12 * np.abs(wq).max()
+    assert np.abs(w - wr[:4]).max() < 1e-8  # converged
+    Tm = np.diag(a) + np.diag(b[1:], 1) + np.diag(b[1:], -1)
+    V = np.linalg.eigh(Tm)[1]
+    assert np.abs(zn - np.abs(V[-1, :4])).max() <= 1e-14
+    assert zn.max() < 1e-6
+
+
+def test_tridiag_lowest_close_pair():
+    """Two nearly decoupled blocks with equal spectra give eigenvalue pairs 1e-14 apart:
+    the eigenvalues stay exact to rounding and the last components stay finite in [0, 1]."""
+    rng = np.random.default_rng(5)
+    m = 20
+    d1 = rng.normal(size=m)
+    e1 = np.abs(rng.normal(size=m)) + 0.5
+    d = np.concatenate([d1, d1])
+    e = np.concatenate([e1, e1])
+    e[0] = 0.0
+    e[m] = 1e-14
+    T = np.diag(d) + np.diag(e[1:], 1) + np.diag(e[1:], -1)
+    wr = np.linalg.eigvalsh(T)
+    w, zn = E.tridiag_lowest(d, e, 4)
+    assert np.abs(w - wr[:4]).max() <= 1e-14 * np.abs(wr).max()
+    assert np.all(np.isfinite(zn)) and np.all((zn >= 0) & (zn <= 1 + 1e-12))

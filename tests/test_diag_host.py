@@ -277,3 +277,80 @@ def test_oc_driver_and_drude_weight():
     # sums like D = sum w/dE agree with the exact spectra to ~1e-7 relative
     assert abs(dw - dw_ex) < 1e-6 * abs(dw_ex) and np.abs(oc - oc_ex).max() < 1e-6 * np.abs(oc_ex).max()
     assert ekin < 0.0
+
+
+def test_sector_scheduler_admission():
+    """SectorScheduler: a solve waits until its bytes fit, and one larger than the whole
+    capacity is clamped so it runs alone instead of waiting for ever."""
+    import threading
+
+    from ed_lattice_b200.diag import SectorScheduler
+
+    sch = SectorScheduler(100)
+    a = sch.acquire(60)
+    assert a == 60 and sch.free == 40
+    got = []
+    t = threading.Thread(target=lambda: got.append(sch.acquire(50)))
+    t.start()
+    t.join(0.2)
+    assert t.is_alive() and not got  # 50 > 40 free: waits
+    sch.release(a)
+    t.join(5)
+    assert got == [50] and sch.free == 50
+    sch.release(50)
+    assert sch.acquire(10**6) == 100 and sch.free == 0
+
+
+def test_threaded_sector_solves_match_sequential_and_respect_capacity():
+    """solve_sectors with 4 threads and the oracle's dense solver: the same eigenpairs as the
+    sequential run, keyed by sector; solves start largest first; the byte estimates held at
+    once never exceed the capacity; a failing sector raises after the others end."""
+    import threading
+    import time
+
+    from ed_lattice_b200.diag import sector_device_bytes, solve_sectors
+
+    H = _chain4()
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    p = DiagParams(finite_temp=True, temp=0.1, lanc_nstates_sector=4, lanc_dim_threshold=0)
+    jobs = []
+    for isector in range(1, 26):
+        nup, ndw = m.get_nup(isector), m.get_ndw(isector)
+        dim = math.comb(4, nup) * math.comb(4, ndw)
+        jobs.append((isector, nup, ndw, min(4, dim), dim > 4))
+    base = _oracle_solver(om)
+    lock = threading.Lock()
+    state = {"held": 0, "peak": 0, "starts": []}
+    cap = 2 * max(sector_device_bytes(math.comb(4, j[1]) * math.comb(4, j[2]), j[3], j[4], p) for j in jobs)
+
+    def solver(model, nup, ndw, neigen, lanc_solve, params, seed):
+        b = sector_device_bytes(math.comb(4, nup) * math.comb(4, ndw), neigen, lanc_solve, params)
+        with lock:
+            state["held"] += b
+            state["peak"] = max(state["peak"], state["held"])
+            state["starts"].append(math.comb(4, nup) * math.comb(4, ndw))
+        time.sleep(0.01)
+        try:
+            return base(model, nup, ndw, neigen, lanc_solve, params, seed)
+        finally:
+            with lock:
+                state["held"] -= b
+
+    seq = solve_sectors(m, jobs, p, 1, solver=base)
+    par = solve_sectors(m, jobs, p, 1, solver=solver, threads=4, capacity=cap)
+    assert sorted(par) == sorted(seq) == [j[0] for j in jobs]
+    for k in seq:
+        assert np.array_equal(par[k][0], seq[k][0]) and np.array_equal(par[k][1], seq[k][1])
+    assert state["peak"] <= cap
+    state["starts"].clear()
+    solve_sectors(m, jobs, p, 1, solver=solver, threads=4, capacity=1 << 40)
+    assert sorted(state["starts"][:4]) == sorted(state["starts"])[-4:]  # largest dispatched first
+
+    def failing(model, nup, ndw, neigen, lanc_solve, params, seed):
+        if (nup, ndw) == (2, 2):
+            raise RuntimeError("sector (2,2) failed")
+        return base(model, nup, ndw, neigen, lanc_solve, params, seed)
+
+    with pytest.raises(RuntimeError, match=r"\(2,2\)"):
+        solve_sectors(m, jobs, p, 1, solver=failing, threads=4, capacity=cap)
