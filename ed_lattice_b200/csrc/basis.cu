@@ -43,8 +43,10 @@ const char* get_error() { return g_err; }
 // state and other users of the device.
 static const size_t kReserveBytes = size_t(1) << 30;
 
-// Stream-ordered allocations from a library-owned pool per device that keeps up to
-// kPoolKeepBytes of freed memory for reuse. A request is refused when it would leave less than
+// Stream-ordered allocations from a library-owned pool per device that keeps up to a
+// quarter of the device memory (at least kPoolKeepBytes) of freed memory for reuse: above
+// that, every synchronisation hands memory back to the driver, which stalls like cudaFree
+// when several sectors' Lanczos bases are alive at once. A request is refused when it would leave less than
 // kReserveBytes of HBM free (memory held by the pool counts as used); the driver's free-memory query is skipped when the pool already
 // holds enough idle memory for the request.
 namespace {
@@ -84,7 +86,9 @@ int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
       props.location.type = cudaMemLocationTypeDevice;
       props.location.id = dev;
       EDG_CUDA(cudaMemPoolCreate(&g_pool[dev], &props));
-      uint64_t keep = kPoolKeepBytes;
+      size_t fr = 0, total = 0;
+      EDG_CUDA(cudaMemGetInfo(&fr, &total));
+      uint64_t keep = std::max<uint64_t>(kPoolKeepBytes, total / 4);
       EDG_CUDA(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
     }
     pool = g_pool[dev];

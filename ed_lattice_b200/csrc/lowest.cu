@@ -26,43 +26,70 @@ constexpr int kMaxK = 16;         // eigenpairs per call
 constexpr int kLkThreads = 256;
 constexpr int kDenseMaxDim = 16384;  // 2 GB dense matrix
 
-// partial[j * nblk + blk] = sum over this block's chunk of Q[j][i] * w[i] for j < m, and with
-// `self` also column m = <w, w>. Each warp takes groups of kColGrp columns, its lanes stride
-// over the chunk with one load of w and kColGrp loads of Q in flight per step; no block
-// barrier. Fixed summation order (deterministic).
-constexpr int kColGrp = 8;
+// partial[j * nsplit + s] = sum over element stream s of Q[j][i] * w[i], j < m. blockIdx.y
+// takes a group of G columns and stream s = blockIdx.x * 8 + warp a contiguous run of
+// elements, so every warp streams G + 1 long coalesced rows; the grid spans all column
+// groups at once (about 7 blocks per SM). On the 853,776-state sector this reads the basis
+// at 5.8-6.2 TB/s for 112-224 columns, where one element chunk per block with the column
+// groups shared out among its warps reached 3.3 TB/s. Fixed summation order.
+template <int G>
 __global__ void __launch_bounds__(kLkThreads) k_multidot(const double* __restrict__ Q, int m, int64_t n,
-                                                         const double* __restrict__ w, int self,
-                                                         double* __restrict__ partial) {
-  int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+                                                         const double* __restrict__ w, double* __restrict__ partial) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nsplit = gridDim.x * (kLkThreads / 32);
+  const int split = blockIdx.x * (kLkThreads / 32) + warp;
+  int64_t chunk = (n + nsplit - 1) / nsplit;
   chunk = (chunk + 31) & ~int64_t(31);
-  const int64_t i0 = blockIdx.x * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int mt = m + (self ? 1 : 0);
-  const int ngrp = (mt + kColGrp - 1) / kColGrp;
-  for (int g = threadIdx.x >> 5; g < ngrp; g += nw) {
-    const int j0 = g * kColGrp;
-    const double* __restrict__ q[kColGrp];
+  const int64_t i0 = split * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
+  const int j0 = blockIdx.y * G;
+  const double* __restrict__ q[G];
 #pragma unroll
-    for (int c = 0; c < kColGrp; ++c) {
-      const int j = j0 + c < mt ? j0 + c : mt - 1;  // tail columns repeat the last one
-      q[c] = j < m ? Q + int64_t(j) * n : w;
-    }
-    double acc[kColGrp];
+  for (int c = 0; c < G; ++c) q[c] = Q + int64_t(j0 + c < m ? j0 + c : m - 1) * n;  // tail repeats column m-1
+  double acc[G];
 #pragma unroll
-    for (int c = 0; c < kColGrp; ++c) acc[c] = 0.0;
-    for (int64_t i = i0 + lane; i < i1; i += 32) {
-      const double wi = w[i];
+  for (int c = 0; c < G; ++c) acc[c] = 0.0;
+#pragma unroll 2
+  for (int64_t i = i0 + lane; i < i1; i += 32) {
+    const double wi = w[i];
 #pragma unroll
-      for (int c = 0; c < kColGrp; ++c) acc[c] = __fma_rn(q[c][i], wi, acc[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < kColGrp; ++c) {
-      double t = acc[c];
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-      if (lane == 0 && j0 + c < mt) partial[int64_t(j0 + c) * gridDim.x + blockIdx.x] = t;
-    }
+    for (int c = 0; c < G; ++c) acc[c] = __fma_rn(q[c][i], wi, acc[c]);
   }
+#pragma unroll
+  for (int c = 0; c < G; ++c) {
+    double t = acc[c];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0 && j0 + c < m) partial[int64_t(j0 + c) * nsplit + split] = t;
+  }
+}
+
+constexpr int kDotBlocks = 148 * 7;  // blocks per multi-dot launch, over all column groups
+
+// Launch shape of k_multidot for m columns of n elements: column group width, blocks per
+// group (each 8 element streams of at least 32 elements).
+struct DotShape {
+  int G, gx;
+  int nsplit() const { return gx * (kLkThreads / 32); }
+};
+DotShape dot_shape(int m, int64_t n) {
+  DotShape d;
+  d.G = m >= 64 ? 8 : 4;
+  const int ngrp = (m + d.G - 1) / d.G;
+  int64_t gx = (kDotBlocks + ngrp - 1) / ngrp;
+  const int64_t most = std::max<int64_t>(1, n / (32 * (kLkThreads / 32)));
+  d.gx = int(std::min(gx, most));
+  return d;
+}
+
+int launch_multidot(const double* Q, int m, int64_t n, const double* w, double* partial, cudaStream_t st,
+                    int* nsplit) {
+  const DotShape d = dot_shape(m, n);
+  const dim3 grid(d.gx, (m + d.G - 1) / d.G);
+  if (d.G == 8)
+    k_multidot<8><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, partial);
+  else
+    k_multidot<4><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, partial);
+  *nsplit = d.nsplit();
+  return EDG_OK;
 }
 
 __global__ void k_copy1(double* __restrict__ dst, const double* __restrict__ src) { *dst = *src; }
@@ -205,8 +232,9 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   DevBuf<double> w, part, coef, Zd;
   EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
   EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
-  const int nblk = std::min<int64_t>(592, (n + kLkThreads - 1) / kLkThreads);
-  EDG_CHECK(part.alloc(size_t(mmax + 1) * nblk + kRedBlocks, st, "multi-dot partials"));
+  size_t npart = kRedBlocks;  // also the norm's scratch
+  for (int mm = 1; mm <= mmax; ++mm) npart = std::max(npart, size_t(mm) * dot_shape(mm, n).nsplit());
+  EDG_CHECK(part.alloc(npart, st, "multi-dot partials"));
   EDG_CHECK(coef.alloc(size_t(mmax) + 8, st, "multi-dot coefficients"));
   // start vector
   if (v0_host) {
@@ -241,8 +269,9 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     double* qj = Q.p + size_t(j) * n;
     EDG_CHECK(hxv_apply<double>(s, qj, w.p));
     for (int pass = 0; pass < 2; ++pass) {
-      k_multidot<<<nblk, kLkThreads, 0, st>>>(Q.p, j + 1, n, w.p, 0, part.p);
-      k_multifinish<<<(j + 1 + 7) / 8, 256, 0, st>>>(part.p, nblk, j + 1, coef.p);
+      int nsplit = 0;
+      EDG_CHECK(launch_multidot(Q.p, j + 1, n, w.p, part.p, st, &nsplit));
+      k_multifinish<<<(j + 1 + 7) / 8, 256, 0, st>>>(part.p, nsplit, j + 1, coef.p);
       if (pass == 0) k_copy1<<<1, 1, 0, st>>>(dA + j, coef.p + j);  // a_j = <q_j, H q_j>
       k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
     }
