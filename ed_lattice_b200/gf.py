@@ -18,8 +18,17 @@ less) run on the device through edg_gf_chain; a sector without such a neighbour 
 empty channel (Nexc=0). CHI and OC: one same-sector chain per state (and site) on
 O|state>. Weights and poles are those of the add_to_lanczos_* routines. Chains of a state
 run on the rank that holds its vector; the spectra are all-gathered.
+
+On the device, the states of a rank are shared out among host threads (`threads`, default
+4): each thread keeps its own sectors (a bounded cache) and runs all the chains of one state
+at a time on them, so chains of different states overlap on the GPU. Results are keyed by
+state, so they do not depend on which thread ran what.
 """
 from __future__ import annotations
+
+import threading
+from collections import OrderedDict
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -29,6 +38,7 @@ from .edlat import (Model, Sector, Spectrum, chi_chain, drude_weight, eval_chi, 
                     oc_chain)
 
 LANC_NGFITER = 200  # LANC_NGFITER default (src/INPUT_VARS.f90:161)
+STATE_THREADS = 4   # host threads that run the chains of different states at once
 
 
 def get_cdg_sector(model: Model, ispin: int, isector: int) -> int:
@@ -46,24 +56,32 @@ def get_c_sector(model: Model, ispin: int, isector: int) -> int:
 
 
 class _DeviceChains:
-    """Default chain runner: sectors built once and kept for the whole build."""
+    """Default chain runner of one thread: the sectors it has used, built once and kept (the
+    `keep` most recently used), and the state loaded into its source sector."""
 
-    def __init__(self, model: Model, precision: int):
-        self.model, self.precision = model, precision
-        self.sectors: dict[int, Sector] = {}
-        self.loaded = None
+    def __init__(self, model: Model, precision: int, keep: int = 8):
+        self.model, self.precision, self.keep = model, precision, max(keep, 2)
+        self.sectors: OrderedDict[int, Sector] = OrderedDict()
+        self.loaded = None  # (isector, vec) whose vector the source sector holds
 
     def sector(self, isector: int) -> Sector:
         s = self.sectors.get(isector)
         if s is None:
             s = self.sectors[isector] = Sector.from_index(self.model, isector)
+            while len(self.sectors) > self.keep:
+                old, sec = self.sectors.popitem(last=False)
+                sec.delete()
+                if self.loaded is not None and self.loaded[0] == old:
+                    self.loaded = None
+        else:
+            self.sectors.move_to_end(isector)
         return s
 
     def load(self, isector: int, vec) -> Sector:
         src = self.sector(isector)
-        if self.loaded is not vec:
+        if self.loaded is None or self.loaded[0] != isector or self.loaded[1] is not vec:
             src.set_state(np.real(vec))
-            self.loaded = vec
+            self.loaded = (isector, vec)
         return src
 
     def __call__(self, isector, vec, jsector, op, io, jo, ispin, nlanc, ei) -> Spectrum:
@@ -77,40 +95,84 @@ class _DeviceChains:
         self.sectors.clear()
 
 
+def _map_states(state_list: StateList, comm, what: str, fn, threads: int, make_ctx=None) -> dict:
+    """{istate: fn(istate, state, ctx)} over the states this rank owns. With threads > 1 the
+    states are shared out among that many host threads, each with its own ctx = make_ctx()
+    (closed at the end); the first failure in state order is raised once all have ended."""
+    rank, _ = _rank_world(comm)
+    todo = []
+    for istate in range(1, state_list.size + 1):
+        st = state_list.states[istate - 1]
+        if st.owner != rank:
+            continue
+        if st.vec is None:
+            raise L.EdgError(L.EDG_ERR_STATE, what, "state list holds no vectors")
+        todo.append((istate, st))
+    ctxs = []
+    lock = threading.Lock()
+    local = threading.local()
+
+    def context():
+        c = getattr(local, "ctx", None)
+        if c is None and make_ctx is not None:
+            c = local.ctx = make_ctx()
+            with lock:
+                ctxs.append(c)
+        return c
+
+    try:
+        if threads <= 1 or len(todo) <= 1:
+            return {istate: fn(istate, st, context()) for istate, st in todo}
+        import torch
+
+        dev = torch.cuda.current_device() if torch.cuda.is_available() else None
+
+        def work(item):
+            if dev is not None:
+                torch.cuda.set_device(dev)
+            return fn(item[0], item[1], context())
+
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            futs = [ex.submit(work, item) for item in todo]
+        return {item[0]: f.result() for item, f in zip(todo, futs)}
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def build_gf_electrons(model: Model, state_list: StateList, nlanc: int = LANC_NGFITER, offdiag: bool = False,
-                       precision: int = L.EDG_PREC_F64, chain_fn=None, comm=None) -> dict:
+                       precision: int = L.EDG_PREC_F64, chain_fn=None, comm=None, threads: int | None = None) -> dict:
     """impGmatrix: {(ispin, io, jo): [[particle, hole] per state]} with 1-based sites, for
     io == jo (the diagonal) and, with `offdiag`, every ordered pair io != jo built from
     (c_io + c_jo) chains. `chain_fn(isector, vec, jsector, op, io, jo, ispin, nlanc, ei)`
-    returns one channel (jo = 0 for a single site); the default runs on the device."""
-    rank, _ = _rank_world(comm)
-    runner = chain_fn or _DeviceChains(model, precision)
+    returns one channel (jo = 0 for a single site); the default runs on the device, on
+    `threads` host threads (default STATE_THREADS; 1 for a caller-supplied chain_fn)."""
+    if threads is None:
+        threads = 1 if chain_fn else STATE_THREADS
     ns = model.ns
     pairs = [(io, io) for io in range(1, ns + 1)]
     if offdiag:
         pairs += [(io, jo) for io in range(1, ns + 1) for jo in range(1, ns + 1) if io != jo]
-    mine = {}
-    try:
-        for istate in range(1, state_list.size + 1):
-            st = state_list.states[istate - 1]
-            if st.owner != rank:
-                continue
-            if st.vec is None:
-                raise L.EdgError(L.EDG_ERR_STATE, "build_gf_electrons", "state list holds no vectors")
-            for ispin in range(1, model.nspin + 1):
-                jp, jh = get_cdg_sector(model, ispin, st.sector), get_c_sector(model, ispin, st.sector)
-                for io, jo in pairs:
-                    chans = []
-                    for jsec, op in ((jp, +1), (jh, -1)):
-                        if jsec == 0:
-                            chans.append(Spectrum(np.zeros(0), np.zeros(0), 0.0))
-                        else:
-                            chans.append(runner(st.sector, st.vec, jsec, op, io, 0 if io == jo else jo, ispin,
-                                                nlanc, st.e))
-                    mine[(ispin, io, jo, istate)] = chans
-    finally:
-        if chain_fn is None:
-            runner.close()
+
+    def run(istate, st, dev):
+        runner = chain_fn or dev
+        out = {}
+        for ispin in range(1, model.nspin + 1):
+            jp, jh = get_cdg_sector(model, ispin, st.sector), get_c_sector(model, ispin, st.sector)
+            for io, jo in pairs:
+                chans = []
+                for jsec, op in ((jp, +1), (jh, -1)):
+                    if jsec == 0:
+                        chans.append(Spectrum(np.zeros(0), np.zeros(0), 0.0))
+                    else:
+                        chans.append(runner(st.sector, st.vec, jsec, op, io, 0 if io == jo else jo, ispin,
+                                            nlanc, st.e))
+                out[(ispin, io, jo)] = chans
+        return out
+
+    per = _map_states(state_list, comm, "build_gf_electrons", run, threads,
+                      None if chain_fn else (lambda: _DeviceChains(model, precision)))
+    mine = {(ispin, io, jo, istate): chans for istate, res in per.items() for (ispin, io, jo), chans in res.items()}
     gm: dict = {}
     for part in _allgather(mine, comm):
         for (ispin, io, jo, istate), chans in part.items():
@@ -164,17 +226,10 @@ def eval_gf_electrons(gmatrix: dict, state_list: StateList, zeta: float, temp: f
     return gmats, greal
 
 
-def _per_state(state_list: StateList, comm, what: str, fn) -> list:
-    """fn(istate, state) on the rank that owns each state; results gathered in list order."""
-    rank, _ = _rank_world(comm)
-    mine = {}
-    for istate in range(1, state_list.size + 1):
-        st = state_list.states[istate - 1]
-        if st.owner != rank:
-            continue
-        if st.vec is None:
-            raise L.EdgError(L.EDG_ERR_STATE, what, "state list holds no vectors")
-        mine[istate] = fn(istate, st)
+def _per_state(state_list: StateList, comm, what: str, fn, threads: int = 1, make_ctx=None) -> list:
+    """fn(istate, state, ctx) on the rank that owns each state (see _map_states); results
+    gathered in list order."""
+    mine = _map_states(state_list, comm, what, fn, threads, make_ctx)
     out = [None] * state_list.size
     for part in _allgather(mine, comm):
         for istate, res in part.items():
@@ -183,14 +238,16 @@ def _per_state(state_list: StateList, comm, what: str, fn) -> list:
 
 
 def build_chi(model: Model, state_list: StateList, kind: int = 0, nlanc: int = LANC_NGFITER,
-              precision: int = L.EDG_PREC_F64, chain_fn=None, comm=None) -> dict:
+              precision: int = L.EDG_PREC_F64, chain_fn=None, comm=None, threads: int | None = None) -> dict:
     """SpinChiMatrix (kind 0: S^z_i) or the charge analogue (kind 1: n_i): {io: [[chain] per
     state]} for every site (1-based), a same-sector chain on O_io|state> per state. Norb=1
     has no mixed spin-chi (the reference builds those only for Norb > 1).
-    `chain_fn(isector, vec, io, nlanc, ei)` returns one channel; the default runs on the device."""
-    dev = None if chain_fn else _DeviceChains(model, precision)
+    `chain_fn(isector, vec, io, nlanc, ei)` returns one channel; the default runs on the device
+    on `threads` host threads (default STATE_THREADS)."""
+    if threads is None:
+        threads = 1 if chain_fn else STATE_THREADS
 
-    def run(istate, st):
+    def run(istate, st, dev):
         res = {}
         for io in range(1, model.ns + 1):
             if chain_fn:
@@ -200,11 +257,8 @@ def build_chi(model: Model, state_list: StateList, kind: int = 0, nlanc: int = L
                 res[io] = [chi_chain(sec, io, min(nlanc, sec.dim), st.e, kind=kind, precision=precision)]
         return res
 
-    try:
-        per = _per_state(state_list, comm, "build_chi", run)
-    finally:
-        if dev:
-            dev.close()
+    per = _per_state(state_list, comm, "build_chi", run, threads,
+                     None if chain_fn else (lambda: _DeviceChains(model, precision)))
     return {io: [per[k][io] for k in range(state_list.size)] for io in range(1, model.ns + 1)}
 
 
@@ -238,23 +292,22 @@ def eval_chi_electrons(chimatrix: dict, state_list: StateList, zeta: float, temp
 
 
 def build_oc(model: Model, state_list: StateList, nlanc: int = LANC_NGFITER, precision: int = L.EDG_PREC_F64,
-             chain_fn=None, comm=None) -> list:
+             chain_fn=None, comm=None, threads: int | None = None) -> list:
     """OcMatrix: [[chain] per state], the chain of the current J (hop i+1 -> i minus h.c.
     along the ring of sites) on each state, in its own sector. `chain_fn(isector, vec, nlanc,
-    ei)` returns one channel; the default runs on the device."""
-    dev = None if chain_fn else _DeviceChains(model, precision)
+    ei)` returns one channel; the default runs on the device on `threads` host threads
+    (default STATE_THREADS)."""
+    if threads is None:
+        threads = 1 if chain_fn else STATE_THREADS
 
-    def run(istate, st):
+    def run(istate, st, dev):
         if chain_fn:
             return [chain_fn(st.sector, st.vec, nlanc, st.e)]
         sec = dev.load(st.sector, st.vec)
         return [oc_chain(sec, min(nlanc, sec.dim), st.e, precision=precision)]
 
-    try:
-        return _per_state(state_list, comm, "build_oc", run)
-    finally:
-        if dev:
-            dev.close()
+    return _per_state(state_list, comm, "build_oc", run, threads,
+                      None if chain_fn else (lambda: _DeviceChains(model, precision)))
 
 
 def eval_oc_electrons(ocmatrix: list, state_list: StateList, zeta: float, temp: float, finite_temp: bool,

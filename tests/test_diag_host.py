@@ -354,3 +354,47 @@ def test_threaded_sector_solves_match_sequential_and_respect_capacity():
 
     with pytest.raises(RuntimeError, match=r"\(2,2\)"):
         solve_sectors(m, jobs, p, 1, solver=failing, threads=4, capacity=cap)
+
+
+def test_threaded_state_map_contexts_and_errors():
+    """gf._map_states with 4 threads: every owned state once, one context per worker thread
+    (never shared between threads at once), all contexts closed, and a failing state raised
+    after the others end."""
+    import threading
+    import time
+
+    from ed_lattice_b200.gf import _map_states
+
+    sl = StateList()
+    for i in range(20):
+        sl.add_state(-1.0 - 0.01 * i, np.zeros(3), 1 + i % 5, size=100)
+    made = []
+
+    class Ctx:
+        def __init__(self):
+            self.thread = threading.get_ident()
+            self.closed = False
+            made.append(self)
+
+        def close(self):
+            self.closed = True
+
+    def fn(istate, st, ctx):
+        assert ctx.thread == threading.get_ident()
+        time.sleep(0.002)
+        return (istate, st.sector)
+
+    out = _map_states(sl, None, "test", fn, 4, Ctx)
+    assert out == {i: (i, sl.states[i - 1].sector) for i in range(1, 21)}
+    assert 1 <= len(made) <= 4 and all(c.closed for c in made)
+
+    def bad(istate, st, ctx):
+        if istate == 7:
+            raise ValueError("state 7")
+        return istate
+
+    made.clear()
+    with pytest.raises(ValueError, match="state 7"):
+        _map_states(sl, None, "test", bad, 4, Ctx)
+    assert all(c.closed for c in made)
+    assert _map_states(sl, None, "test", lambda i, st, c: i, 1) == {i: i for i in range(1, 21)}
