@@ -210,8 +210,12 @@ __device__ __forceinline__ int between_parity(uint32_t t, int a, int b) {
   return __popc(t & mask) & 1;
 }
 
-__global__ void k_hop_fill(const uint32_t* map, int64_t dim, const int32_t* bonds, const double* bh, int nb,
-                           const uint32_t* C, const uint32_t* off, uint32_t* src, double* v64, float* v32) {
+// Row r of the stored hop table: sources ascending, value sign * Hij(a,b); with bhi (complex
+// Hij) also the imaginary parts, stored as -sign * Im Hij(a,b): the stored form keeps
+// conjg(Hij) (src/DIAG/stored/H_up.f90:19-21).
+__global__ void k_hop_fill(const uint32_t* map, int64_t dim, const int32_t* bonds, const double* bh,
+                           const double* bhi, int nb, const uint32_t* C, const uint32_t* off, uint32_t* src,
+                           double* v64, float* v32, double* v64i, float* v32i) {
   int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (r >= dim) return;
   uint32_t t = map[r];
@@ -221,21 +225,27 @@ __global__ void k_hop_fill(const uint32_t* map, int64_t dim, const int32_t* bond
     int a = bonds[2 * k], b = bonds[2 * k + 1];
     if (((t >> a) & 1u) && !((t >> b) & 1u)) {
       uint32_t s = (t & ~(1u << a)) | (1u << b);
-      double v = between_parity(t, a, b) ? -bh[k] : bh[k];
+      const bool neg = between_parity(t, a, b);
+      double v = neg ? -bh[k] : bh[k];
+      double vi = bhi ? (neg ? bhi[k] : -bhi[k]) : 0.0;
       uint32_t j = rank_of(s, C);
       // insertion into the row, ascending source rank (the reference's summation order)
       uint32_t pos = n;
       while (pos > 0 && src[o + pos - 1] > j) {
         src[o + pos] = src[o + pos - 1];
         v64[o + pos] = v64[o + pos - 1];
+        if (bhi) v64i[o + pos] = v64i[o + pos - 1];
         --pos;
       }
       src[o + pos] = j;
       v64[o + pos] = v;
+      if (bhi) v64i[o + pos] = vi;
       ++n;
     }
   }
   for (uint32_t q = 0; q < n; ++q) v32[o + q] = float(v64[o + q]);
+  if (bhi)
+    for (uint32_t q = 0; q < n; ++q) v32i[o + q] = float(v64i[o + q]);
 }
 
 int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
@@ -281,7 +291,8 @@ int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
       if (h == 0.0 && hi == 0.0) continue;
       bl.a.push_back(a);
       bl.b.push_back(b);
-      bl.h.push_back(h);  // real part; the imaginary part is rejected at model level
+      bl.h.push_back(h);
+      bl.hi.push_back(hi);
     }
   bl.nb = int(bl.a.size());
   // Order bonds by d = 2^b - 2^a: the source of a hop is target + d, so this order yields
@@ -294,7 +305,12 @@ int build_spin(edg_sector_s* s, int spin, SpinBasis& B, int nel) {
     return dx < dy;
   });
   BondList sorted;
-  for (int k : ord) { sorted.a.push_back(bl.a[k]); sorted.b.push_back(bl.b[k]); sorted.h.push_back(bl.h[k]); }
+  for (int k : ord) {
+    sorted.a.push_back(bl.a[k]);
+    sorted.b.push_back(bl.b[k]);
+    sorted.h.push_back(bl.h[k]);
+    sorted.hi.push_back(bl.hi[k]);
+  }
   sorted.nb = bl.nb;
   bl = sorted;
   return EDG_OK;
@@ -307,13 +323,17 @@ int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   const BondList& bl = s->bonds[spin - 1];
   const int nb = bl.nb;
   DevBuf<int32_t> bonds;
-  DevBuf<double> bh;
+  DevBuf<double> bh, bhi;
   std::vector<int32_t> hb(2 * nb + 2);
   for (int k = 0; k < nb; ++k) { hb[2 * k] = bl.a[k]; hb[2 * k + 1] = bl.b[k]; }
   EDG_CHECK(bonds.alloc(hb.size(), st, "bond list"));
   EDG_CHECK(bh.alloc(nb + 1, st, "bond values"));
   EDG_CUDA(cudaMemcpyAsync(bonds.p, hb.data(), hb.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
   if (nb) EDG_CUDA(cudaMemcpyAsync(bh.p, bl.h.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (s->cplx) {
+    EDG_CHECK(bhi.alloc(nb + 1, st, "bond values"));
+    if (nb) EDG_CUDA(cudaMemcpyAsync(bhi.p, bl.hi.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+  }
   EDG_CHECK(B.off.alloc(B.dim + 1, st, "hop offsets"));
   DevBuf<uint32_t> cnt;
   EDG_CHECK(cnt.alloc(B.dim, st, "hop counts"));
@@ -333,11 +353,16 @@ int build_tables(edg_sector_s* s, int spin, SpinBasis& B) {
   EDG_CHECK(B.src.alloc(nnz + 1, st, "hop sources"));
   EDG_CHECK(B.val64.alloc(nnz + 1, st, "hop values"));
   EDG_CHECK(B.val32.alloc(nnz + 1, st, "hop values"));
-  k_hop_fill<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, bh.p, nb, s->binom.p, B.off.p, B.src.p, B.val64.p,
-                                     B.val32.p);
+  if (s->cplx) {
+    EDG_CHECK(B.val64i.alloc(nnz + 1, st, "hop values"));
+    EDG_CHECK(B.val32i.alloc(nnz + 1, st, "hop values"));
+  }
+  k_hop_fill<<<blocks, 256, 0, st>>>(B.map.p, B.dim, bonds.p, bh.p, s->cplx ? bhi.p : nullptr, nb, s->binom.p,
+                                     B.off.p, B.src.p, B.val64.p, B.val32.p, B.val64i.p, B.val32i.p);
   EDG_CUDA(cudaGetLastError());
   EDG_CUDA(cudaStreamSynchronize(st));
-  return build_sell(s, B);
+  // the complex H x v gathers straight from this table; the SELL layouts serve the real kernels
+  return s->cplx ? EDG_OK : build_sell(s, B);
 }
 
 // Proper edge colouring of a bipartite multigraph (left: lanes [0,G), right: banks [0,M))
@@ -639,6 +664,7 @@ int sector_build(edg_sector_s* s) {
   EDG_CHECK(build_spin(s, 1, s->up, s->nup));
   EDG_CHECK(build_spin(s, 2, s->dw, s->ndw));
   s->dim = s->up.dim * s->dw.dim;
+  s->vlen = s->cplx ? 2 * s->dim : s->dim;
   s->U = s->model.uloc;
   if (s->form == EDG_FORM_STORED) {
     EDG_CHECK(build_tables(s, 1, s->up));
@@ -646,16 +672,25 @@ int sector_build(edg_sector_s* s) {
   } else {
     // direct form: bond lists only (both spins packed: [spin][k] -> a,b ; values)
     std::vector<int32_t> hb;
-    std::vector<double> hv;
+    std::vector<double> hv, hvi;
     for (int sp = 0; sp < 2; ++sp) {
       const BondList& bl = s->bonds[sp];
-      for (int k = 0; k < bl.nb; ++k) { hb.push_back(bl.a[k]); hb.push_back(bl.b[k]); hv.push_back(bl.h[k]); }
+      for (int k = 0; k < bl.nb; ++k) {
+        hb.push_back(bl.a[k]);
+        hb.push_back(bl.b[k]);
+        hv.push_back(bl.h[k]);
+        hvi.push_back(bl.hi[k]);
+      }
     }
     EDG_CHECK(s->bond_dev.alloc(hb.size() + 2, s->stream, "bond list"));
     EDG_CHECK(s->bondh_dev.alloc(hv.size() + 1, s->stream, "bond values"));
+    if (s->cplx) EDG_CHECK(s->bondhi_dev.alloc(hvi.size() + 1, s->stream, "bond values"));
     if (!hb.empty()) {
       EDG_CUDA(cudaMemcpyAsync(s->bond_dev.p, hb.data(), hb.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
       EDG_CUDA(cudaMemcpyAsync(s->bondh_dev.p, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+      if (s->cplx)
+        EDG_CUDA(cudaMemcpyAsync(s->bondhi_dev.p, hvi.data(), hvi.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 s->stream));
     }
   }
   EDG_CUDA(cudaStreamSynchronize(s->stream));

@@ -90,6 +90,26 @@ int check_sector(const edg_sector_s* s) {
   return EDG_OK;
 }
 
+// Entry points whose complex-Hij form is not built: excitations, observables and energies of
+// complex states, the lowest-k solver and the dense sector matrix.
+int real_only(const edg_sector_s* s, const char* what) {
+  if (s && s->cplx) {
+    set_error("%s: not available for complex Hij sectors", what);
+    return EDG_ERR_UNSUPPORTED;
+  }
+  return EDG_OK;
+}
+
+// Device vectors of a complex sector hold (re, im) pairs: 2*sizeof(T)-aligned.
+template <typename T>
+int check_vec_align(const edg_sector_s* s, const void* p, const char* what) {
+  if (s->cplx && reinterpret_cast<uintptr_t>(p) % (2 * sizeof(T)) != 0) {
+    set_error("%s: complex vectors must be %zu-byte aligned", what, 2 * sizeof(T));
+    return EDG_ERR_ARG;
+  }
+  return EDG_OK;
+}
+
 int ensure_device(const edg_sector_s* s) {
   int cur = -1;
   EDG_CUDA(cudaGetDevice(&cur));
@@ -189,15 +209,12 @@ int edg_sector_create(const edg_model* m, int nup, int ndw, int form, edg_sector
   EDG_ARG(nup >= 0 && nup <= m->ns && ndw >= 0 && ndw <= m->ns, "edg_sector_create: (Nup,Ndw)=(%d,%d) outside 0..%d",
           nup, ndw, m->ns);
   EDG_ARG(form == EDG_FORM_STORED || form == EDG_FORM_DIRECT, "edg_sector_create: form=%d", form);
-  if (m->complex_hij) {
-    set_error("edg_sector_create: complex Hij is not supported on the device (real Hij only)");
-    return EDG_ERR_UNSUPPORTED;
-  }
   int ndev = 0;
   if (edg_device_count(&ndev) != EDG_OK) return EDG_ERR_NODEVICE;
   edg_sector_s* s = new (std::nothrow) edg_sector_s();
   if (!s) return EDG_ERR_NOMEM;
   s->model = *m;
+  s->cplx = m->complex_hij;
   s->nup = nup;
   s->ndw = ndw;
   s->form = form;
@@ -232,6 +249,13 @@ int edg_sector_destroy(edg_sector* s) {
     delete s;
   }
   if (own && st) cudaStreamDestroy(st);
+  return EDG_OK;
+}
+
+int edg_sector_vlen(const edg_sector* s, int64_t* vlen) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(vlen, "edg_sector_vlen: NULL");
+  *vlen = s->vlen;
   return EDG_OK;
 }
 
@@ -291,6 +315,8 @@ int edg_sector_set_stream(edg_sector* s, void* stream) {
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(dv && dhv && dv != dhv, "edg_hxv_dev_f64: bad vectors");
+  EDG_CHECK(check_vec_align<double>(s, dv, "edg_hxv_dev_f64"));
+  EDG_CHECK(check_vec_align<double>(s, dhv, "edg_hxv_dev_f64"));
   EDG_CHECK(ensure_device(s));
   return hxv_apply<double>(s, dv, dhv);
 }
@@ -298,6 +324,8 @@ int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv) {
 int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(dv && dhv && dv != dhv, "edg_hxv_dev_f32: bad vectors");
+  EDG_CHECK(check_vec_align<float>(s, dv, "edg_hxv_dev_f32"));
+  EDG_CHECK(check_vec_align<float>(s, dhv, "edg_hxv_dev_f32"));
   EDG_CHECK(ensure_device(s));
   return hxv_apply<float>(s, dv, dhv);
 }
@@ -305,6 +333,10 @@ int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv) {
 int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(v && hv, "edg_hxv_d: NULL vector");
+  if (s->cplx) {
+    set_error("edg_hxv_d: complex Hij maps real vectors to complex ones; use edg_hxv_z");
+    return EDG_ERR_ARG;
+  }
   EDG_ARG(nloc == s->dim, "directMatVec ERROR: Nloc != dim(isector) (%lld vs %lld)", (long long)nloc,
           (long long)s->dim);
   EDG_CHECK(ensure_device(s));
@@ -325,6 +357,15 @@ int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv) {
           (long long)s->dim);
   EDG_CHECK(ensure_device(s));
   const int64_t n = s->dim;
+  if (s->cplx) {  // complex H x v straight on the interleaved vector
+    EDG_CHECK(s->w64[0].alloc(2 * n, s->stream, "H x v input"));
+    EDG_CHECK(s->w64[1].alloc(2 * n, s->stream, "H x v output"));
+    EDG_CUDA(cudaMemcpyAsync(s->w64[0].p, v, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    EDG_CHECK(hxv_apply<double>(s, s->w64[0].p, s->w64[1].p));
+    EDG_CUDA(cudaMemcpyAsync(hv, s->w64[1].p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    EDG_CUDA(cudaStreamSynchronize(s->stream));
+    return EDG_OK;
+  }
   for (int k = 0; k < 4; ++k) EDG_CHECK(s->w64[k].alloc(n, s->stream, "H x v work"));
   EDG_CHECK(s->zstage.alloc(size_t(2 * n), s->stream, "complex staging"));
   double* stage = s->zstage.p;
@@ -346,6 +387,7 @@ int edg_tridiag_dev_f64(edg_sector* s, const double* dvinit, int nlanc, double t
   EDG_ARG(dvinit && alanc && blanc && norm2 && nsteps, "edg_tridiag: NULL argument");
   EDG_ARG(nlanc >= 0, "edg_tridiag: nlanc=%d", nlanc);
   EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_tridiag: precision=%d", precision);
+  EDG_CHECK(check_vec_align<double>(s, dvinit, "edg_tridiag_dev_f64"));
   EDG_CHECK(ensure_device(s));
   return tridiag_dev(s, dvinit, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
 }
@@ -355,8 +397,8 @@ int edg_tridiag_d(edg_sector* s, const double* vvinit, int nlanc, double thresho
   EDG_CHECK(check_sector(s));
   EDG_ARG(vvinit, "edg_tridiag_d: NULL start vector");
   EDG_CHECK(ensure_device(s));
-  EDG_CHECK(s->w64[3].alloc(s->dim, s->stream, "start vector"));
-  EDG_CUDA(cudaMemcpyAsync(s->w64[3].p, vvinit, s->dim * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EDG_CHECK(s->w64[3].alloc(s->vlen, s->stream, "start vector"));
+  EDG_CUDA(cudaMemcpyAsync(s->w64[3].p, vvinit, s->vlen * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   return edg_tridiag_dev_f64(s, s->w64[3].p, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
 }
 
@@ -380,6 +422,7 @@ int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, 
 int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol, double* evals,
                  double* evecs, double* resid, int* niter) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_lowest_k"));
   EDG_ARG(evals && niter, "edg_lowest_k: NULL output");
   EDG_ARG(k >= 1 && k <= 16, "edg_lowest_k: k=%d outside 1..16", k);
   EDG_ARG(maxit >= 1, "edg_lowest_k: maxit=%d", maxit);
@@ -390,6 +433,7 @@ int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxi
 
 int edg_sector_dense(edg_sector* s, double* h) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_sector_dense"));
   EDG_ARG(h, "edg_sector_dense: NULL");
   EDG_CHECK(ensure_device(s));
   return sector_dense(s, h);
@@ -397,6 +441,7 @@ int edg_sector_dense(edg_sector* s, double* h) {
 
 int edg_sector_dense_dev(edg_sector* s, double* dh) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_sector_dense_dev"));
   EDG_ARG(dh, "edg_sector_dense_dev: NULL");
   EDG_CHECK(ensure_device(s));
   return sector_dense_dev(s, dh);
@@ -417,7 +462,7 @@ int edg_state_get(const edg_sector* s, double* evec) {
     return EDG_ERR_STATE;
   }
   EDG_CHECK(ensure_device(s));
-  EDG_CUDA(cudaMemcpyAsync(evec, s->state.p, s->dim * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EDG_CUDA(cudaMemcpyAsync(evec, s->state.p, s->vlen * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   EDG_CUDA(cudaStreamSynchronize(s->stream));
   return EDG_OK;
 }
@@ -426,8 +471,8 @@ int edg_state_set(edg_sector* s, const double* evec) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(evec, "edg_state_set: NULL");
   EDG_CHECK(ensure_device(s));
-  EDG_CHECK(s->state.alloc(s->dim, s->stream, "state"));
-  EDG_CUDA(cudaMemcpyAsync(s->state.p, evec, s->dim * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EDG_CHECK(s->state.alloc(s->vlen, s->stream, "state"));
+  EDG_CUDA(cudaMemcpyAsync(s->state.p, evec, s->vlen * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   EDG_CUDA(cudaStreamSynchronize(s->stream));
   s->has_state = true;
   return EDG_OK;
@@ -446,6 +491,8 @@ int edg_apply_cop_dev_f64(const edg_sector* from, const edg_sector* to, int op, 
                           int accumulate, const double* din, double* dout) {
   EDG_CHECK(check_sector(from));
   EDG_CHECK(check_sector(to));
+  EDG_CHECK(real_only(from, "edg_apply_cop_dev_f64"));
+  EDG_CHECK(real_only(to, "edg_apply_cop_dev_f64"));
   EDG_ARG(din && dout && din != dout, "edg_apply_cop: bad vectors");
   EDG_ARG(op == 1 || op == -1, "edg_apply_cop: op=%d", op);
   EDG_ARG(spin == 1 || spin == 2, "edg_apply_cop: spin=%d", spin);
@@ -461,6 +508,7 @@ int edg_apply_cop_dev_f64(const edg_sector* from, const edg_sector* to, int op, 
 int edg_apply_diagop_dev_f64(const edg_sector* s, int kind, int site, int site2, const double* qcos, const double* din,
                              double* dout) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_apply_diagop_dev_f64"));
   EDG_ARG(din && dout, "edg_apply_diagop: NULL vector");
   EDG_ARG(kind == 0 || kind == 1, "edg_apply_diagop: kind=%d", kind);
   const int ns = s->model.ns;
@@ -479,6 +527,7 @@ int edg_apply_diagop_dev_f64(const edg_sector* s, int kind, int site, int site2,
 
 int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* dout) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_apply_current_dev_f64"));
   EDG_ARG(din && dout && din != dout, "edg_apply_current: bad vectors");
   EDG_CHECK(ensure_device(s));
   return apply_current(s, din, dout, s->stream);
@@ -486,6 +535,7 @@ int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* do
 
 int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double* eknot, double* ehartree) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_energy"));
   if (!s->has_state) {
     set_error("edg_energy: the sector holds no state");
     return EDG_ERR_STATE;
@@ -498,6 +548,7 @@ int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double*
 int edg_observables(const edg_sector* s, double weight, double* dens, double* dens_up, double* dens_dw, double* docc,
                     double* magz) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_observables"));
   if (!s->has_state) {
     set_error("edg_observables: the sector holds no state");
     return EDG_ERR_STATE;
@@ -542,6 +593,8 @@ int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int s
                  int precision, double ei, double* poles, double* weights, double* norm2, int* nout) {
   EDG_CHECK(check_sector(from));
   EDG_CHECK(check_sector(to));
+  EDG_CHECK(real_only(from, "edg_gf_chain"));
+  EDG_CHECK(real_only(to, "edg_gf_chain"));
   EDG_ARG(poles && weights && norm2 && nout, "edg_gf_chain: NULL output");
   if (!from->has_state) {
     set_error("edg_gf_chain: origin sector holds no state");
@@ -557,6 +610,7 @@ int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int s
 int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qcos, int nlanc, int precision,
                   double ei, double* poles, double* weights, double* norm2, int* nout) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_chi_chain"));
   EDG_ARG(poles && weights && norm2 && nout, "edg_chi_chain: NULL output");
   if (!s->has_state) {
     set_error("edg_chi_chain: sector holds no state");
@@ -570,6 +624,7 @@ int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qc
 int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* poles, double* weights, double* norm2,
                  int* nout) {
   EDG_CHECK(check_sector(s));
+  EDG_CHECK(real_only(s, "edg_oc_chain"));
   EDG_ARG(poles && weights && norm2 && nout, "edg_oc_chain: NULL output");
   if (!s->has_state) {
     set_error("edg_oc_chain: sector holds no state");
@@ -598,7 +653,7 @@ int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc,
   EDG_CHECK(check_sector(s));
   EDG_ARG(k >= 1 && dvinit && alanc && blanc && norm2 && nsteps, "edg_tridiag_block_dev: bad arguments");
   for (int c = 0; c < k; ++c)
-    EDG_CHECK(edg_tridiag_dev_f64(s, dvinit + size_t(c) * s->dim, nlanc, threshold, precision,
+    EDG_CHECK(edg_tridiag_dev_f64(s, dvinit + size_t(c) * s->vlen, nlanc, threshold, precision,
                                   alanc + size_t(c) * nlanc, blanc + size_t(c) * nlanc, norm2 + c, nsteps + c));
   return EDG_OK;
 }

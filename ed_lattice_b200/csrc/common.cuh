@@ -101,6 +101,8 @@ struct SpinBasis {
   DevBuf<uint32_t> src;         // [nnz]
   DevBuf<double> val64;         // [nnz]
   DevBuf<float> val32;
+  DevBuf<double> val64i;        // [nnz] imaginary parts (complex Hij only)
+  DevBuf<float> val32i;
   int64_t nnz = 0;
   // The same table in SELL-32 layout (slices of 32 consecutive target rows padded to the
   // slice's longest row, stored entry-major) so a warp reading the k-th entry of its 32
@@ -147,7 +149,7 @@ struct SpinBasis {
 struct BondList {
   int nb = 0;
   std::vector<int> a, b;
-  std::vector<double> h;
+  std::vector<double> h, hi;  // Hij(a,b): real and imaginary parts
 };
 
 }  // namespace edg
@@ -170,7 +172,12 @@ struct edg_sector_s {
   edg::DevBuf<uint32_t> binom;    // C(n,k) table [kBinomN*kBinomN], exact integers
   edg::DevBuf<int32_t> bond_dev;  // device bond list for the direct form: [spin][a,b] packed
   edg::DevBuf<double> bondh_dev;
+  edg::DevBuf<double> bondhi_dev;  // imaginary parts (complex Hij only)
   double U = 0;
+  // Complex Hij: vectors are complex, stored interleaved (re, im), so every vector of the
+  // sector holds vlen = 2*dim reals; the Lanczos scalars stay real (H is Hermitian).
+  bool cplx = false;
+  int64_t vlen = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t home_stream = nullptr;  // the library stream the sector was created on
   bool own_stream = false;

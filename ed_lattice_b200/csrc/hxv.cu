@@ -674,6 +674,104 @@ __global__ void __launch_bounds__(256) k_direct_rows(HxvArgs<T> a, DirectArgsHdr
   }
 }
 
+// ---- complex Hij: vectors of complex elements stored interleaved (re, im)
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<float> {
+  using type = float2;
+};
+template <>
+struct Cplx<double> {
+  using type = double2;
+};
+
+// acc += h * y for complex h = (hr, hi), y
+template <typename T, typename T2>
+__device__ __forceinline__ void cmad(T hr, T hi, T2 y, T& re, T& im) {
+  re = fmaT<T>(hr, y.x, re);
+  re = fmaT<T>(-hi, y.y, re);
+  im = fmaT<T>(hr, y.y, im);
+  im = fmaT<T>(hi, y.x, im);
+}
+
+// Stored form, one thread per element: the diagonal, then the down hops, then the up hops,
+// each row's sources ascending (the order of the real passes and of spMatVec). Table values
+// hold sign * conjg(Hij) (real parts in val_*, imaginary parts in vi_*).
+template <typename T>
+__global__ void __launch_bounds__(256) k_cplx_stored(HxvArgs<T> a, const T* __restrict__ vi_up,
+                                                     const T* __restrict__ vi_dw) {
+  using T2 = typename Cplx<T>::type;
+  const T2* __restrict__ v = reinterpret_cast<const T2*>(a.v);
+  T2* __restrict__ hv = reinterpret_cast<T2*>(a.hv);
+  const int64_t n = a.dimup * a.dimdw;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t idw = e / a.dimup, iup = e - idw * a.dimup;
+    const T d = a.e_up[iup] + a.e_dw[idw] + a.U * T(__popc(a.map_up[iup] & a.map_dw[idw]));
+    const T2 x = v[e];
+    T re = d * x.x, im = d * x.y;
+    for (uint32_t k = a.off_dw[idw]; k < a.off_dw[idw + 1]; ++k)
+      cmad(a.val_dw[k], vi_dw[k], v[int64_t(a.src_dw[k]) * a.dimup + iup], re, im);
+    for (uint32_t k = a.off_up[iup]; k < a.off_up[iup + 1]; ++k)
+      cmad(a.val_up[k], vi_up[k], v[idw * a.dimup + a.src_up[k]], re, im);
+    T2 out;
+    out.x = re;
+    out.y = im;
+    hv[e] = out;
+  }
+}
+
+// Direct form, one thread per element, bonds in shared memory: the diagonal, then the up
+// hops, then the down hops in bond order (directMatVec's order), value sign * Hij (not
+// conjugated: the reference's direct and stored forms differ by conjugation here).
+template <typename T>
+__global__ void __launch_bounds__(256) k_cplx_direct(HxvArgs<T> a, DirectArgsHdr d, const double* __restrict__ bhi) {
+  using T2 = typename Cplx<T>::type;
+  extern __shared__ unsigned char smem_raw[];
+  int32_t* sb = reinterpret_cast<int32_t*>(smem_raw);
+  const int nb = d.nb_up + d.nb_dw;
+  T* shr = reinterpret_cast<T*>(smem_raw + ((2 * nb * sizeof(int32_t) + 15) / 16) * 16);
+  T* shi = shr + nb;
+  __shared__ uint32_t sC[kBinomN * kBinomN];
+  for (int k = threadIdx.x; k < 2 * nb; k += blockDim.x) sb[k] = d.bonds[k];
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    shr[k] = T(d.bh[k]);
+    shi[k] = T(bhi[k]);
+  }
+  for (int k = threadIdx.x; k < kBinomN * kBinomN; k += blockDim.x) sC[k] = d.C[k];
+  __syncthreads();
+  const T2* __restrict__ v = reinterpret_cast<const T2*>(a.v);
+  T2* __restrict__ hv = reinterpret_cast<T2*>(a.hv);
+  const int64_t n = a.dimup * a.dimdw;
+  for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t idw = e / a.dimup, iup = e - idw * a.dimup;
+    const uint32_t mup = a.map_up[iup], mdw = a.map_dw[idw];
+    const T dg = a.e_up[iup] + a.e_dw[idw] + a.U * T(__popc(mup & mdw));
+    const T2 x = v[e];
+    T re = dg * x.x, im = dg * x.y;
+    for (int k = 0; k < d.nb_up; ++k) {
+      const int ba = sb[2 * k], bb = sb[2 * k + 1];
+      if (((mup >> ba) & 1u) && !((mup >> bb) & 1u)) {
+        const uint32_t t = (mup & ~(1u << ba)) | (1u << bb);
+        const T sg = between_parity_d(mup, ba, bb) ? T(-1) : T(1);
+        cmad(sg * shr[k], sg * shi[k], v[idw * a.dimup + rank_of_d(t, sC)], re, im);
+      }
+    }
+    for (int k = d.nb_up; k < nb; ++k) {
+      const int ba = sb[2 * k], bb = sb[2 * k + 1];
+      if (((mdw >> ba) & 1u) && !((mdw >> bb) & 1u)) {
+        const uint32_t t = (mdw & ~(1u << ba)) | (1u << bb);
+        const T sg = between_parity_d(mdw, ba, bb) ? T(-1) : T(1);
+        cmad(sg * shr[k], sg * shi[k], v[int64_t(rank_of_d(t, sC)) * a.dimup + iup], re, im);
+      }
+    }
+    T2 out;
+    out.x = re;
+    out.y = im;
+    hv[e] = out;
+  }
+}
+
 template <typename T>
 const T* pick(const DevBuf<double>& d, const DevBuf<float>& f);
 template <>
@@ -827,6 +925,28 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
   HxvArgs<T> a = make_args<T>(s, v, hv);
   const int sms = sm_count();
   cudaStream_t st = s->stream;
+  if (s->cplx) {
+    const int64_t n = a.dimup * a.dimdw;
+    const int64_t want = (n + 255) / 256;
+    const int g = int(want < int64_t(sms) * 8 ? (want < 1 ? 1 : want) : int64_t(sms) * 8);
+    if (s->form == EDG_FORM_STORED) {
+      k_cplx_stored<T><<<g, 256, 0, st>>>(a, pick<T>(s->up.val64i, s->up.val32i), pick<T>(s->dw.val64i, s->dw.val32i));
+    } else {
+      DirectArgsHdr d;
+      d.nb_up = s->bonds[0].nb;
+      d.nb_dw = s->bonds[1].nb;
+      d.bonds = s->bond_dev.p;
+      d.bh = s->bondh_dev.p;
+      d.C = s->binom.p;
+      const int nb = d.nb_up + d.nb_dw;
+      const size_t smem = ((2 * nb * sizeof(int32_t) + 15) / 16) * 16 + 2 * nb * sizeof(T) + 16;
+      if (smem > 48 * 1024)
+        EDG_CUDA(cudaFuncSetAttribute(k_cplx_direct<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      k_cplx_direct<T><<<g, 256, smem, st>>>(a, d, s->bondhi_dev.p);
+    }
+    EDG_CUDA(cudaGetLastError());
+    return EDG_OK;
+  }
   if (s->form == EDG_FORM_STORED) {
     EDG_CHECK((dw_pass<T, true, false>(a, s->dw, st, sms)));
     EDG_CHECK((up_pass<T, false, false>(a, s->up, st, sms, nullptr)));
@@ -868,8 +988,8 @@ template int hxv_apply<double>(edg_sector_s*, const double*, double*);
 template <typename T>
 int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double* bn, int j, double* partial,
                  int* nblocks) {
-  if (s->form != EDG_FORM_STORED || up_rows_per_cta(s->up.dim, sizeof(T)) == 0 || s->dw.max_row > kDwHops ||
-      s->dw.groups == 0) {
+  if (s->cplx || s->form != EDG_FORM_STORED || up_rows_per_cta(s->up.dim, sizeof(T)) == 0 ||
+      s->dw.max_row > kDwHops || s->dw.groups == 0) {
     set_error("fused Lanczos H x v not available for this sector");
     return EDG_ERR_UNSUPPORTED;
   }
@@ -884,8 +1004,8 @@ int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double
   return EDG_OK;
 }
 bool hxv_lz_available(const edg_sector_s* s, size_t elem) {
-  return s->form == EDG_FORM_STORED && up_rows_per_cta(s->up.dim, elem) > 0 && s->dw.max_row <= kDwHops &&
-         s->dw.groups > 0;
+  return !s->cplx && s->form == EDG_FORM_STORED && up_rows_per_cta(s->up.dim, elem) > 0 &&
+         s->dw.max_row <= kDwHops && s->dw.groups > 0;
 }
 template int hxv_apply_lz<float>(edg_sector_s*, const float*, const float*, float*, const double*, int, double*, int*);
 template int hxv_apply_lz<double>(edg_sector_s*, const double*, const double*, double*, const double*, int, double*,

@@ -81,7 +81,7 @@ struct Recurrence {
   // columns of dim elements that receive u_0, u_1, ... (fused form only)
   int init(edg_sector_s* sec, const double* dv0, double scale, int cap, T* basis = nullptr, int ncols = 0) {
     s = sec;
-    const int64_t n = s->dim;
+    const int64_t n = s->vlen;
     EDG_CHECK(scalars(s, cap, &sc));
     DevBuf<T>* wb = work<T>(s);
     for (int k = 0; k < 3; ++k) {
@@ -107,7 +107,7 @@ struct Recurrence {
   double vscale(int j) const { return fused ? 1.0 / bn_host[j] : 1.0; }
   // step j queued on the stream: a_j and b_{j+1} land in the device scalars only
   int step_dev(int j) {
-    const int64_t n = s->dim;
+    const int64_t n = s->vlen;
     cudaStream_t st = s->stream;
     if (fused) {
       int nb = 0;
@@ -125,7 +125,7 @@ struct Recurrence {
   const double* b_dev() const { return fused ? sc.bn : sc.b; }
   // step j: W <- the unnormalised u_{j+1}; returns a_j and b_{j+1} on the host
   int step(int j, double* a, double* b) {
-    const int64_t n = s->dim;
+    const int64_t n = s->vlen;
     cudaStream_t st = s->stream;
     if (fused) {
       int nb = 0;
@@ -152,7 +152,7 @@ struct Recurrence {
       P = U;
       U = W;
       if (ext && j + 2 < ext_cols) {
-        W = ext + size_t(j + 2) * s->dim;
+        W = ext + size_t(j + 2) * s->vlen;
       } else if (ext) {  // out of basis columns: a work vector that is neither P nor U
         W = wbuf[0] != P && wbuf[0] != U ? wbuf[0] : (wbuf[1] != P && wbuf[1] != U ? wbuf[1] : wbuf[2]);
       } else {
@@ -160,7 +160,7 @@ struct Recurrence {
       }
       bn_host.push_back(b);
     } else {
-      EDG_CHECK(scale_into<T>(s->stream, P, W, sc.b + j + 1, s->dim));
+      EDG_CHECK(scale_into<T>(s->stream, P, W, sc.b + j + 1, s->vlen));
       T* t = P;
       P = U;
       U = t;
@@ -173,7 +173,7 @@ struct Recurrence {
 template <typename T>
 int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, double* alanc, double* blanc,
               double* norm2, int* nsteps) {
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;
   cudaStream_t st = s->stream;
   for (int j = 0; j < nlanc; ++j) { alanc[j] = 0.0; blanc[j] = 0.0; }
   *nsteps = 0;
@@ -245,7 +245,7 @@ Ritz lowest_ritz(const std::vector<double>& a, const std::vector<double>& b, dou
 template <typename T>
 int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vector<double>* A,
            std::vector<double>* B, float* basis, int basis_cols, std::vector<double>* colscale, double* e0) {
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;
   cudaStream_t st = s->stream;
   Recurrence<T> R;
   T* own = std::is_same<T, float>::value ? reinterpret_cast<T*>(basis) : nullptr;
@@ -291,7 +291,7 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
 template <typename T>
 int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A, const std::vector<double>& B,
                 const float* basis, int basis_cols, const std::vector<double>& colscale, double* x) {
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;
   cudaStream_t st = s->stream;
   const int m = int(A.size());
   std::vector<double> w(m), Z(size_t(m) * m);
@@ -336,7 +336,7 @@ int ritz_vector(edg_sector_s* s, const double* dv0, const std::vector<double>& A
 int normalise(edg_sector_s* s, double* dv) {
   Scalars sc;
   EDG_CHECK(scalars(s, 2, &sc));
-  EDG_CHECK(dot_dev<double>(s->stream, dv, dv, s->dim, sc.partial, sc.tmp));
+  EDG_CHECK(dot_dev<double>(s->stream, dv, dv, s->vlen, sc.partial, sc.tmp));
   double nn = 0.0;
   EDG_CUDA(cudaMemcpyAsync(&nn, sc.tmp, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   EDG_CUDA(cudaStreamSynchronize(s->stream));
@@ -344,7 +344,7 @@ int normalise(edg_sector_s* s, double* dv) {
     set_error("start vector has zero norm");
     return EDG_ERR_ARG;
   }
-  return scale_inplace_dev<double>(s->stream, dv, s->dim, 1.0 / std::sqrt(nn));
+  return scale_inplace_dev<double>(s->stream, dv, s->vlen, 1.0 / std::sqrt(nn));
 }
 
 }  // namespace
@@ -357,10 +357,10 @@ int tridiag_dev(edg_sector_s* s, const double* dv0, int nlanc, double threshold,
 
 int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
                  double* e0, int* niter) {
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;
   cudaStream_t st = s->stream;
   if (maxit <= 0) maxit = 1;
-  if (maxit > n) maxit = int(n);
+  if (maxit > s->dim) maxit = int(s->dim);  // the Krylov space has at most dim (complex) dimensions
   EDG_CHECK(s->state.alloc(n, st, "eigenvector"));
   EDG_CHECK(s->w64[3].alloc(n, st, "start vector"));
   double* x0 = s->w64[3].p;

@@ -70,8 +70,8 @@ extern "C" int edg_tridiag_dev_f64_noalloc(edg_sector* s, const double* dvinit, 
     set_error("edg_tridiag_dev_f64_noalloc: NULL argument");
     return EDG_ERR_ARG;
   }
-  if (s->dim > kNoAllocMaxDim || nlanc < 0 || nlanc > kNoAllocMaxLanc) {
-    set_error("edg_tridiag_dev_f64_noalloc: dim %lld > %lld or nlanc %d outside 0..%d", (long long)s->dim,
+  if (s->vlen > kNoAllocMaxDim || nlanc < 0 || nlanc > kNoAllocMaxLanc) {
+    set_error("edg_tridiag_dev_f64_noalloc: vector length %lld > %lld or nlanc %d outside 0..%d", (long long)s->vlen,
               (long long)kNoAllocMaxDim, nlanc, kNoAllocMaxLanc);
     return EDG_ERR_ARG;
   }
@@ -80,7 +80,7 @@ extern "C" int edg_tridiag_dev_f64_noalloc(edg_sector* s, const double* dvinit, 
   if (cur != s->device) EDG_CUDA(cudaSetDevice(s->device));
   double* base = nullptr;
   EDG_CHECK(scratch_ptr(s->device, &base));
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;
   cudaStream_t st = s->stream;
   double* V = base;
   double* P = base + kNoAllocMaxDim;

@@ -105,7 +105,8 @@ def ring(L_: int, t: float = 1.0) -> np.ndarray:
 
 # ----------------------------------------------------------------------------- model / sector
 class Model:
-    """Real Hij (Ns x Ns, or [2,Ns,Ns] for Nspin=2) with Uloc, xmu, HFMODE, ED_FILLING."""
+    """Hij (Ns x Ns, or [2,Ns,Ns] for Nspin=2; real or complex) with Uloc, xmu, HFMODE,
+    ED_FILLING. With complex Hij the sectors' vectors are complex."""
 
     def __init__(self, hij, uloc: float = 0.0, xmu: float = 0.0, hfmode: bool = True, ed_filling: int = 0):
         H = np.asarray(hij)
@@ -159,6 +160,10 @@ class Sector:
         d, du, dd = C.c_int64(), C.c_int64(), C.c_int64()
         L.check(L.lib().edg_sector_dims(h, C.byref(d), C.byref(du), C.byref(dd)), "edg_sector_dims")
         self.dim, self.dimup, self.dimdw = d.value, du.value, dd.value
+        vl = C.c_int64()
+        L.check(L.lib().edg_sector_vlen(h, C.byref(vl)), "edg_sector_vlen")
+        self.vlen = vl.value            # reals per vector
+        self.cplx = self.vlen != self.dim  # complex Hij: complex vectors, stored interleaved
 
     @classmethod
     def from_index(cls, model: Model, isector: int, form: int = L.EDG_FORM_STORED) -> "Sector":
@@ -207,6 +212,7 @@ class Sector:
         return hv
 
     def hxv_real(self, v: np.ndarray) -> np.ndarray:
+        """H x v on a real host vector (real Hij only)."""
         v = _f64(v)
         hv = np.empty_like(v)
         L.check(L.lib().edg_hxv_d(self.handle, v.size, _pd(v), _pd(hv)), "spHtimesV")
@@ -244,15 +250,28 @@ class Sector:
 
     # ---- state buffer (the eigenvector kept on the device)
     def get_state(self) -> np.ndarray:
-        x = np.empty(self.dim)
+        """The state kept on the device: real, or complex for a complex-Hij sector."""
+        x = np.empty(self.vlen)
         L.check(L.lib().edg_state_get(self.handle, _pd(x)), "edg_state_get")
-        return x
+        return x.view(np.complex128) if self.cplx else x
 
     def set_state(self, x: np.ndarray) -> None:
-        x = _f64(x)
-        if x.size != self.dim:
-            raise ValueError("state size != sector dimension")
+        x = self._vec(x, "state")
         L.check(L.lib().edg_state_set(self.handle, _pd(x)), "edg_state_set")
+
+    def _vec(self, x, what: str) -> np.ndarray:
+        """x as the library's FP64 layout for this sector: real [dim], or complex [dim]
+        interleaved as [2*dim] reals (a real x is taken as a complex vector with zero
+        imaginary part)."""
+        if self.cplx:
+            x = np.ascontiguousarray(x, dtype=np.complex128)
+            if x.size != self.dim:
+                raise ValueError(f"{what} size != sector dimension")
+            return x.view(np.float64)
+        x = _f64(np.real(x))
+        if x.size != self.dim:
+            raise ValueError(f"{what} size != sector dimension")
+        return x
 
     def observables(self, weight: float = 1.0) -> dict:
         """lanc_observables for the stored state (src/OBSERVABLES.f90:127-152)."""
@@ -285,9 +304,10 @@ def tridiag_Hv_sector(sector: Sector, vvinit: np.ndarray, nlanc: int | None = No
     Returns (alanc, blanc, norm2, nsteps) with blanc[0] = 0."""
     if nlanc is None:
         nlanc = min(sector.dim, 200)
-    v = _f64(np.real(vvinit))
-    if v.size != sector.dim:
-        raise L.EdgError(L.EDG_ERR_ARG, "tridiag_Hv_sector", "vvinit size != sector dimension")
+    try:
+        v = sector._vec(vvinit, "vvinit")
+    except ValueError as e:
+        raise L.EdgError(L.EDG_ERR_ARG, "tridiag_Hv_sector", str(e)) from None
     a = np.zeros(max(nlanc, 1))
     b = np.zeros(max(nlanc, 1))
     n2 = C.c_double()
@@ -304,7 +324,7 @@ def sp_lanc_eigh(sector: Sector, v0: np.ndarray | None = None, seed: int = 1234,
     Returns (E0, evec or None, number of H x v applications)."""
     e0 = C.c_double()
     it = C.c_int()
-    v0a = _f64(v0) if v0 is not None else None
+    v0a = sector._vec(v0, "v0") if v0 is not None else None
     if not want_vector:
         mode |= L.EDG_GS_E0_ONLY
     L.check(L.lib().edg_ground_state_keep(sector.handle, _pd(v0a), C.c_uint64(seed), maxit, tol, mode, C.byref(e0),

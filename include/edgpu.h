@@ -84,6 +84,14 @@ int64_t edg_binomial(int n, int k);
 int edg_sector_create(const edg_model* m, int nup, int ndw, int form, edg_sector** out);
 int edg_sector_destroy(edg_sector* s);
 int edg_sector_dims(const edg_sector* s, int64_t* dim, int64_t* dimup, int64_t* dimdw);
+/* Reals per vector of this sector: dim, or 2*dim when the model's Hij is complex. The
+ * reference's vectors are complex(8) throughout; with complex Hij every vector argument of
+ * this API (host or device: start vectors, H x v operands, states) holds dim complex
+ * elements interleaved (re, im), device ones 2*sizeof(T)-aligned, and the Lanczos scalars
+ * stay real. Not built for complex Hij (EDG_ERR_UNSUPPORTED): edg_lowest_k,
+ * edg_sector_dense(_dev), the excitation operators, edg_observables, edg_energy and the
+ * GF/CHI/OC chains. */
+int edg_sector_vlen(const edg_sector* s, int64_t* vlen);
 /* Copy the device-built maps Hsector%H(1)%map / H(2)%map (bitstrings, ascending). */
 int edg_sector_get_maps(const edg_sector* s, int32_t* map_up, int32_t* map_dw);
 /* Copy one spin's hop table (spin 1 = spH0ups(1), 2 = spH0dws(1)) as CSR over target rows:
@@ -97,11 +105,14 @@ int edg_sector_set_stream(edg_sector* s, void* stream);
 /* ------------------------------------------------------------------ H x v
  * dd_sparse_HxV(Nloc,v,Hv) (src/VARS_GLOBAL.f90:102-108), the callback that
  * spHtimesV_p points to (spMatVec / directMatVec). Host complex(8) vectors, interleaved
- * (re,im); Hv is overwritten. Real Hij only on the device: H acts on the real and the
- * imaginary parts separately. nloc must equal the sector dimension (the reference stops
- * with "Nloc != dim(isector)", src/DIAG/HAMILTONIAN_DIRECT_HxV.f90:33). */
+ * (re,im); Hv is overwritten. With real Hij, H acts on the real and the imaginary parts
+ * separately; with complex Hij the complex H is applied, the stored form with the
+ * conjugated hop values the reference stores (src/DIAG/stored/H_up.f90:19-21) and the
+ * direct form with Hij itself (src/DIAG/direct/HxV_up.f90:24). nloc must equal the sector
+ * dimension (the reference stops with "Nloc != dim(isector)",
+ * src/DIAG/HAMILTONIAN_DIRECT_HxV.f90:33). */
 int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv);
-/* Same on real host vectors. */
+/* Same on real host vectors (real Hij only). */
 int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv);
 /* Device-resident forms (vectors in HBM, reference layout); stream-ordered, no sync. */
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv);

@@ -1,0 +1,186 @@
+"""Complex Hij on the device (Peierls phases, complex random hoppings): the complex H x v
+of both reference forms against the oracle's complex restatements (orc_stored_matvec_z,
+orc_direct_matvec_z), including the reference's conjugation quirk between the forms; the
+Lanczos chain and the ground state against a numpy restatement of the same recurrence and
+dense diagonalisation built from the oracle's H x v. FP64 within 1e-13 relative per H x v
+(the complex products are fused differently from std::complex), coefficients within 1e-9,
+E0 within 1e-10; FP32 within FP32 round-off."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import ed_lattice_b200 as E
+from ed_lattice_b200 import _edgpu_lib as L
+from ed_lattice_b200.edlat import ring
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def flux_ring(ns, phi, t=1.0, seed=None):
+    """Ring threaded by flux phi: Hij(i, i+1) = -t e^{i phi/ns}, Hermitian; optional site
+    energies quantised to 2^-16."""
+    H = np.zeros((ns, ns), complex)
+    for i in range(ns):
+        j = (i + 1) % ns
+        H[i, j] = -t * np.exp(1j * phi / ns)
+        H[j, i] = np.conj(H[i, j])
+    if seed is not None:
+        rng = np.random.default_rng(seed)
+        H[np.diag_indices(ns)] = np.round(rng.uniform(-1, 1, ns) * 65536) / 65536
+    return H
+
+
+def random_hermitian(ns, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(ns, ns)) + 1j * rng.normal(size=(ns, ns))
+    return (A + A.conj().T) / 2
+
+
+def models(h, **kw):
+    return E.Model(h, **kw), O.Model(h, **kw)
+
+
+def cvec(seed, n):
+    rng = np.random.default_rng(seed)
+    return rng.normal(size=n) + 1j * rng.normal(size=n)
+
+
+def np_lanczos(matvec, v0, nlanc):
+    """sp_lanc_tridiag's recurrence on complex vectors (real a, b): the reference's
+    convention b[0] = 0, b[j] = b_{j+1}."""
+    v = v0 / np.linalg.norm(v0)
+    vp = np.zeros_like(v)
+    a, b = np.zeros(nlanc), np.zeros(nlanc)
+    bj = 0.0
+    for j in range(nlanc):
+        w = matvec(v) - bj * vp
+        a[j] = np.vdot(v, w).real
+        w = w - a[j] * v
+        bj = np.linalg.norm(w)
+        if j + 1 < nlanc:
+            b[j + 1] = bj
+        vp, v = v, w / bj
+    return a, b
+
+
+def dense_from_matvec(matvec, dim):
+    H = np.zeros((dim, dim), complex)
+    for i in range(dim):
+        e = np.zeros(dim, complex)
+        e[i] = 1.0
+        H[:, i] = matvec(e)
+    return H
+
+
+@pytest.mark.parametrize("form", [E.EDG_FORM_STORED, E.EDG_FORM_DIRECT])
+@pytest.mark.parametrize("case", ["flux", "random", "nspin2"])
+def test_complex_hxv_vs_oracle(form, case):
+    if case == "flux":
+        H, nup, ndw = flux_ring(8, 0.7, seed=3), 4, 3
+    elif case == "random":
+        H, nup, ndw = random_hermitian(6, 5), 3, 2
+    else:
+        H, nup, ndw = np.stack([flux_ring(6, 0.4), flux_ring(6, -1.1, t=0.5, seed=2)]), 3, 2
+    gm, om = models(H, uloc=2.0, xmu=0.3, hfmode=True)
+    s = E.Sector(gm, nup, ndw, form)
+    assert s.cplx and s.vlen == 2 * s.dim
+    v = cvec(7, s.dim)
+    ref = O.Stored(om, nup, ndw).matvec_z(v) if form == E.EDG_FORM_STORED else O.direct_matvec_z(om, nup, ndw, v)
+    hv = s.HxV(v)
+    assert np.abs(hv - ref).max() <= 1e-13 * np.abs(ref).max()
+    s.delete()
+
+
+def test_complex_forms_differ_by_conjugation():
+    """The reference's stored form keeps conjg(Hij) where the direct form uses Hij: on the
+    device as in the oracle, stored(H) = direct(conj H) and stored(H) != direct(H)."""
+    H = flux_ring(8, 1.3, seed=1)
+    gm = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    gc = E.Model(H.conj(), uloc=4.0, xmu=2.0, hfmode=False)
+    st = E.Sector(gm, 4, 4, E.EDG_FORM_STORED)
+    dr = E.Sector(gm, 4, 4, E.EDG_FORM_DIRECT)
+    dc = E.Sector(gc, 4, 4, E.EDG_FORM_DIRECT)
+    v = cvec(2, st.dim)
+    a, b, c = st.HxV(v), dr.HxV(v), dc.HxV(v)
+    assert np.abs(a - c).max() <= 1e-13 * np.abs(a).max()
+    assert np.abs(a - b).max() > 1e-3 * np.abs(a).max()
+    for s in (st, dr, dc):
+        s.delete()
+
+
+def test_complex_hermitian_and_device_f32():
+    """<x|H y> = <H x|y> on the device, and the FP32 device H x v on interleaved vectors
+    against FP64 within FP32 round-off."""
+    import torch
+    gm, _ = models(flux_ring(10, 0.9, seed=4), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 5, 5)
+    x, y = cvec(1, s.dim), cvec(2, s.dim)
+    hx, hy = s.HxV(x), s.HxV(y)
+    assert abs(np.vdot(x, hy) - np.vdot(hx, y)) <= 1e-12 * np.abs(np.vdot(x, hy))
+    s.set_stream(torch.cuda.current_stream().cuda_stream)
+    dx = torch.tensor(x.view(np.float64), dtype=torch.float32, device="cuda")
+    dh = torch.empty_like(dx)
+    L.check(L.lib().edg_hxv_dev_f32(s.handle, C.c_void_p(dx.data_ptr()), C.c_void_p(dh.data_ptr())), "f32")
+    torch.cuda.synchronize()
+    h32 = dh.double().cpu().numpy().view(np.complex128)
+    assert np.abs(h32 - hx).max() <= 2e-6 * np.abs(hx).max()
+    s.delete()
+
+
+@pytest.mark.parametrize("precision,tol", [(E.EDG_PREC_F64, 1e-9), (E.EDG_PREC_F32, 2e-4)])
+def test_complex_tridiag_vs_numpy(precision, tol):
+    """tridiag_Hv_sector on a complex start vector: norm2, a(1:40), b(2:40) against the same
+    recurrence in numpy over the oracle's complex stored H x v."""
+    gm, om = models(flux_ring(8, 0.7, seed=3), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 4, 4)
+    st = O.Stored(om, 4, 4)
+    v0 = cvec(11, s.dim)
+    a, b, n2, k = E.tridiag_Hv_sector(s, v0, nlanc=40, precision=precision)
+    ar, br = np_lanczos(st.matvec_z, v0, 40)
+    assert k == 40
+    assert abs(n2 - np.vdot(v0, v0).real) <= 1e-12 * n2
+    assert np.abs(a - ar).max() <= tol * np.abs(ar).max()
+    assert np.abs(b[1:] - br[1:]).max() <= tol * np.abs(br).max()
+    assert b[0] == 0.0
+    s.delete()
+
+
+@pytest.mark.parametrize("mode", [E.EDG_GS_F64, E.EDG_GS_F32_REFINE])
+def test_complex_ground_state_vs_dense(mode):
+    """sp_lanc_eigh on a complex sector: E0 against dense diagonalisation of the oracle's
+    complex H (1e-10 relative), the eigenvector's residual under the oracle's H x v."""
+    gm, om = models(flux_ring(8, 1.1, seed=6), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 4, 4)
+    st = O.Stored(om, 4, 4)
+    Hd = dense_from_matvec(st.matvec_z, s.dim)
+    assert np.abs(Hd - Hd.conj().T).max() < 1e-12
+    e_ref = np.linalg.eigvalsh(Hd)[0]
+    e0, vec, _ = E.sp_lanc_eigh(s, tol=1e-12, mode=mode)
+    assert abs(e0 - e_ref) <= 1e-10 * abs(e_ref)
+    assert vec.dtype == np.complex128 and abs(np.linalg.norm(vec) - 1.0) < 1e-10
+    assert np.linalg.norm(st.matvec_z(vec) - e0 * vec) < 1e-6
+    s.delete()
+
+
+def test_complex_unsupported_entries_and_errors():
+    gm = E.Model(flux_ring(6, 0.5), uloc=1.0)
+    s = E.Sector(gm, 3, 3)
+    with pytest.raises(E.EdgError) as ei:
+        s.hxv_real(np.zeros(s.dim))
+    assert ei.value.status == L.EDG_ERR_ARG
+    with pytest.raises(E.EdgError) as ei:
+        s.lowest_k(2)
+    assert ei.value.status == L.EDG_ERR_UNSUPPORTED
+    E.sp_lanc_eigh(s, tol=1e-10)
+    with pytest.raises(E.EdgError) as ei:
+        s.observables()
+    assert ei.value.status == L.EDG_ERR_UNSUPPORTED
+    with pytest.raises(ValueError):
+        s.set_state(np.zeros(s.dim + 1))
+    s.delete()
+    # a real model keeps real vectors
+    r = E.Sector(E.Model(ring(6), uloc=1.0), 3, 3)
+    assert not r.cplx and r.vlen == r.dim
+    r.delete()

@@ -208,10 +208,10 @@ def test_hxv_errors():
     assert ei.value.status == L.EDG_ERR_ARG
     with pytest.raises(E.EdgError):
         E.Sector(gm, 7, 1)
-    hc = np.array([[0.0, -1.0 + 0.5j], [-1.0 - 0.5j, 0.0]])
+    hn = np.array([[0.0, -1.0 + 0.5j], [-1.0 + 0.5j, 0.0]])  # not Hermitian
     with pytest.raises(E.EdgError) as ei:
-        E.Sector(E.Model(hc), 1, 1)
-    assert ei.value.status == L.EDG_ERR_UNSUPPORTED
+        E.Model(hn)
+    assert ei.value.status == L.EDG_ERR_ARG
 
 
 # ----------------------------------------------------------------------------- Lanczos
