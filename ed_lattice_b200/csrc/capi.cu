@@ -90,8 +90,8 @@ int check_sector(const edg_sector_s* s) {
   return EDG_OK;
 }
 
-// Entry points whose complex-Hij form is not built: excitations, observables and energies of
-// complex states, the lowest-k solver and the dense sector matrix.
+// Entry points whose complex-Hij form is not built: the lowest-k solver and the dense sector
+// matrix.
 int real_only(const edg_sector_s* s, const char* what) {
   if (s && s->cplx) {
     set_error("%s: not available for complex Hij sectors", what);
@@ -491,8 +491,7 @@ int edg_apply_cop_dev_f64(const edg_sector* from, const edg_sector* to, int op, 
                           int accumulate, const double* din, double* dout) {
   EDG_CHECK(check_sector(from));
   EDG_CHECK(check_sector(to));
-  EDG_CHECK(real_only(from, "edg_apply_cop_dev_f64"));
-  EDG_CHECK(real_only(to, "edg_apply_cop_dev_f64"));
+  EDG_ARG(from->cplx == to->cplx, "edg_apply_cop_dev_f64: the two sectors come from models of different Hij types");
   EDG_ARG(din && dout && din != dout, "edg_apply_cop: bad vectors");
   EDG_ARG(op == 1 || op == -1, "edg_apply_cop: op=%d", op);
   EDG_ARG(spin == 1 || spin == 2, "edg_apply_cop: spin=%d", spin);
@@ -508,7 +507,6 @@ int edg_apply_cop_dev_f64(const edg_sector* from, const edg_sector* to, int op, 
 int edg_apply_diagop_dev_f64(const edg_sector* s, int kind, int site, int site2, const double* qcos, const double* din,
                              double* dout) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_apply_diagop_dev_f64"));
   EDG_ARG(din && dout, "edg_apply_diagop: NULL vector");
   EDG_ARG(kind == 0 || kind == 1, "edg_apply_diagop: kind=%d", kind);
   const int ns = s->model.ns;
@@ -527,7 +525,6 @@ int edg_apply_diagop_dev_f64(const edg_sector* s, int kind, int site, int site2,
 
 int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* dout) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_apply_current_dev_f64"));
   EDG_ARG(din && dout && din != dout, "edg_apply_current: bad vectors");
   EDG_CHECK(ensure_device(s));
   return apply_current(s, din, dout, s->stream);
@@ -535,7 +532,6 @@ int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* do
 
 int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double* eknot, double* ehartree) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_energy"));
   if (!s->has_state) {
     set_error("edg_energy: the sector holds no state");
     return EDG_ERR_STATE;
@@ -548,7 +544,6 @@ int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double*
 int edg_observables(const edg_sector* s, double weight, double* dens, double* dens_up, double* dens_dw, double* docc,
                     double* magz) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_observables"));
   if (!s->has_state) {
     set_error("edg_observables: the sector holds no state");
     return EDG_ERR_STATE;
@@ -593,14 +588,13 @@ int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int s
                  int precision, double ei, double* poles, double* weights, double* norm2, int* nout) {
   EDG_CHECK(check_sector(from));
   EDG_CHECK(check_sector(to));
-  EDG_CHECK(real_only(from, "edg_gf_chain"));
-  EDG_CHECK(real_only(to, "edg_gf_chain"));
+  EDG_ARG(from->cplx == to->cplx, "edg_gf_chain: the two sectors come from models of different Hij types");
   EDG_ARG(poles && weights && norm2 && nout, "edg_gf_chain: NULL output");
   if (!from->has_state) {
     set_error("edg_gf_chain: origin sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(to->w64[3].alloc(to->dim, to->stream, "excitation vector"));
+  EDG_CHECK(to->w64[3].alloc(to->vlen, to->stream, "excitation vector"));
   EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, site, spin, 1.0, 0, from->state.p, to->w64[3].p));
   if (site2 > 0)
     EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, site2, spin, 1.0, 1, from->state.p, to->w64[3].p));
@@ -610,13 +604,12 @@ int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int s
 int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qcos, int nlanc, int precision,
                   double ei, double* poles, double* weights, double* norm2, int* nout) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_chi_chain"));
   EDG_ARG(poles && weights && norm2 && nout, "edg_chi_chain: NULL output");
   if (!s->has_state) {
     set_error("edg_chi_chain: sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(s->w64[3].alloc(s->dim, s->stream, "excitation vector"));
+  EDG_CHECK(s->w64[3].alloc(s->vlen, s->stream, "excitation vector"));
   EDG_CHECK(edg_apply_diagop_dev_f64(s, kind, site, site2, qcos, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);
 }
@@ -624,13 +617,12 @@ int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qc
 int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* poles, double* weights, double* norm2,
                  int* nout) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_oc_chain"));
   EDG_ARG(poles && weights && norm2 && nout, "edg_oc_chain: NULL output");
   if (!s->has_state) {
     set_error("edg_oc_chain: sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(s->w64[3].alloc(s->dim, s->stream, "excitation vector"));
+  EDG_CHECK(s->w64[3].alloc(s->vlen, s->stream, "excitation vector"));
   EDG_CHECK(edg_apply_current_dev_f64(s, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);
 }

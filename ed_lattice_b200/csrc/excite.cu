@@ -8,6 +8,8 @@
 //              optional real site-weight vector for momentum combinations (cos(q.r)).
 //  J         : the current of lanc_ed_build_oc (src/OC/OC_ELECTRONS.f90:139-205).
 //  observables: lanc_observables (src/OBSERVABLES.f90:127-152), per-site moments of |psi|^2.
+// Vectors of a complex-Hij sector hold complex elements interleaved (re, im): the kernels take
+// the element width W (1 real, 2 complex) as a template argument.
 #include "common.cuh"
 
 namespace edg {
@@ -45,17 +47,21 @@ __global__ void k_cop_table(const uint32_t* mapJ, int64_t dimJ, int pos, int op,
   sgn[j] = (__popc(s & (bit - 1u)) & 1) ? -1.0 : 1.0;  // bits below pos (src/AUX_FUNX.f90:84-86)
 }
 
-// spin up: out[jdw][jup] (+)= coef * sgn[jup] * in[jdw][src[jup]]
+// spin up: out[jdw][jup] (+)= coef * sgn[jup] * in[jdw][src[jup]], elements of W reals
+template <int W>
 __global__ void k_cop_up(const double* __restrict__ in, double* __restrict__ out, int64_t dupI, int64_t dupJ,
                          int64_t ddw, const int64_t* __restrict__ src, const double* __restrict__ sg, double coef,
                          int accumulate) {
   for (int64_t row = blockIdx.x; row < ddw; row += gridDim.x) {
-    const double* ir = in + row * dupI;
-    double* orow = out + row * dupJ;
+    const double* ir = in + row * dupI * W;
+    double* orow = out + row * dupJ * W;
     for (int64_t j = threadIdx.x; j < dupJ; j += blockDim.x) {
       const int64_t sidx = src[j];
-      const double v = sidx >= 0 ? coef * sg[j] * ir[sidx] : 0.0;
-      if (accumulate) orow[j] += v; else orow[j] = v;
+#pragma unroll
+      for (int c = 0; c < W; ++c) {
+        const double v = sidx >= 0 ? coef * sg[j] * ir[sidx * W + c] : 0.0;
+        if (accumulate) orow[j * W + c] += v; else orow[j * W + c] = v;
+      }
     }
   }
 }
@@ -86,14 +92,16 @@ __global__ void k_site_sum(const uint32_t* map, int64_t dim, const double* w, in
   f[r] = acc;
 }
 
-// out = (kind 0: (fu - fd)/2 ; kind 1: fu + fd) * in
+// out = (kind 0: (fu - fd)/2 ; kind 1: fu + fd) * in, elements of W reals
+template <int W>
 __global__ void k_diagop(const double* __restrict__ in, double* __restrict__ out, int64_t dup, int64_t ddw,
                          const double* __restrict__ fu, const double* __restrict__ fd, int kind) {
   for (int64_t row = blockIdx.x; row < ddw; row += gridDim.x) {
     const double d = fd[row];
     for (int64_t j = threadIdx.x; j < dup; j += blockDim.x) {
       const double f = kind == 0 ? (fu[j] - d) / 2.0 : fu[j] + d;
-      out[row * dup + j] = f * in[row * dup + j];
+#pragma unroll
+      for (int c = 0; c < W; ++c) out[(row * dup + j) * W + c] = f * in[(row * dup + j) * W + c];
     }
   }
 }
@@ -104,6 +112,7 @@ struct HopOp {
   int a[2 * kMaxSites];
   int b[2 * kMaxSites];
   double c[2 * kMaxSites];
+  double ci[2 * kMaxSites];  // imaginary parts (complex Hij)
 };
 
 __device__ __forceinline__ int parity_between(uint32_t t, int a, int b) {
@@ -112,19 +121,33 @@ __device__ __forceinline__ int parity_between(uint32_t t, int a, int b) {
   return __popc(t & mask) & 1;
 }
 
+// acc += (c + i ci) * x for W = 2 (complex elements), acc += c * x for W = 1
+template <int W>
+__device__ __forceinline__ void hop_acc(double c, double ci, const double* x, double* acc) {
+  if (W == 1) {
+    acc[0] += c * x[0];
+  } else {
+    acc[0] += c * x[0] - ci * x[W - 1];
+    acc[W - 1] += c * x[W - 1] + ci * x[0];
+  }
+}
+
+template <int W>
 __global__ void k_hopop(const double* __restrict__ in, double* __restrict__ out, int64_t dup, int64_t ddw,
                         const uint32_t* mup, const uint32_t* mdw, const uint32_t* C, HopOp hu, HopOp hd) {
   const int64_t n = dup * ddw;
   for (int64_t e = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
     const int64_t idw = e / dup, iup = e - idw * dup;
     const uint32_t tu = mup[iup], td = mdw[idw];
-    double acc = 0.0;
+    double acc[W];
+#pragma unroll
+    for (int c = 0; c < W; ++c) acc[c] = 0.0;
     for (int k = 0; k < hu.nb; ++k) {
       const int a = hu.a[k], b = hu.b[k];
       if (((tu >> a) & 1u) && !((tu >> b) & 1u)) {
         const uint32_t s = (tu & ~(1u << a)) | (1u << b);
         const double sg = parity_between(tu, a, b) ? -1.0 : 1.0;
-        acc += hu.c[k] * sg * in[idw * dup + rank_c(s, C)];
+        hop_acc<W>(hu.c[k] * sg, hu.ci[k] * sg, in + (idw * dup + rank_c(s, C)) * W, acc);
       }
     }
     for (int k = 0; k < hd.nb; ++k) {
@@ -132,15 +155,17 @@ __global__ void k_hopop(const double* __restrict__ in, double* __restrict__ out,
       if (((td >> a) & 1u) && !((td >> b) & 1u)) {
         const uint32_t s = (td & ~(1u << a)) | (1u << b);
         const double sg = parity_between(td, a, b) ? -1.0 : 1.0;
-        acc += hd.c[k] * sg * in[int64_t(rank_c(s, C)) * dup + iup];
+        hop_acc<W>(hd.c[k] * sg, hd.ci[k] * sg, in + (int64_t(rank_c(s, C)) * dup + iup) * W, acc);
       }
     }
-    out[e] = acc;
+#pragma unroll
+    for (int c = 0; c < W; ++c) out[e * W + c] = acc[c];
   }
 }
 
 // Observables: one CTA per row idw; per-site sums of |psi|^2 weighted by the up bits, then
 // combined with the down bits of the row. out layout per block: [5][kMaxSites].
+template <int W>
 __global__ void __launch_bounds__(256) k_obs_rows(const double* __restrict__ psi, int64_t dup, int64_t ddw,
                                                   const uint32_t* mup, const uint32_t* mdw, int ns,
                                                   double* __restrict__ partial) {
@@ -156,8 +181,9 @@ __global__ void __launch_bounds__(256) k_obs_rows(const double* __restrict__ psi
     for (int i = 0; i < kMaxSites; ++i) acc_up[i] = 0.0;
     acc_tot = 0.0;
     for (int64_t j = threadIdx.x; j < dup; j += blockDim.x) {
-      const double p = psi[row * dup + j];
-      const double w = p * p;
+      const double p = psi[(row * dup + j) * W];
+      const double q = psi[(row * dup + j) * W + W - 1];
+      const double w = W == 1 ? p * p : __fma_rn(q, q, p * p);
       const uint32_t u = mup[j];
       acc_tot += w;
 #pragma unroll
@@ -201,6 +227,7 @@ int grid_rows(int64_t rows) { return int(rows < 148 * 8 ? (rows < 1 ? 1 : rows) 
 // Partial sums of psi_i^2 diag(H)_i with diag(H)_i = E_up[iup] + E_dw[idw] + U popc(up & dw),
 // the diagonal the H x v applies; fixed grid and order (deterministic).
 constexpr int kDiagBlocks = 592;
+template <int W>
 __global__ void __launch_bounds__(256) k_diag_dot(const double* __restrict__ psi, int64_t dup, int64_t n,
                                                   const double* __restrict__ eup, const double* __restrict__ edw,
                                                   const uint32_t* __restrict__ mup, const uint32_t* __restrict__ mdw,
@@ -210,7 +237,8 @@ __global__ void __launch_bounds__(256) k_diag_dot(const double* __restrict__ psi
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     const int64_t idw = i / dup, iup = i - idw * dup;
     const double d = eup[iup] + edw[idw] + U * double(__popc(mup[iup] & mdw[idw]));
-    s = __fma_rn(psi[i] * psi[i], d, s);
+    const double p = psi[i * W], q = psi[i * W + W - 1];
+    s = __fma_rn(W == 1 ? p * p : __fma_rn(q, q, p * p), d, s);
   }
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
@@ -234,11 +262,16 @@ int apply_cop(const edg_sector_s* from, const edg_sector_s* to, int op, int site
   EDG_CHECK(sg.alloc(BJ.dim, st, "c-op table"));
   k_cop_table<<<int((BJ.dim + 255) / 256), 256, 0, st>>>(BJ.map.p, BJ.dim, pos, op, to->binom.p, src.p, sg.p);
   EDG_CUDA(cudaGetLastError());
+  const int W = to->cplx ? 2 : 1;
   if (spin == 1) {
-    k_cop_up<<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, from->up.dim, to->up.dim, to->dw.dim, src.p, sg.p,
-                                                    coef, accumulate);
-  } else {
-    k_cop_dw<<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, to->up.dim, to->dw.dim, src.p, sg.p, coef,
+    if (W == 2)
+      k_cop_up<2><<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, from->up.dim, to->up.dim, to->dw.dim, src.p,
+                                                         sg.p, coef, accumulate);
+    else
+      k_cop_up<1><<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, from->up.dim, to->up.dim, to->dw.dim, src.p,
+                                                         sg.p, coef, accumulate);
+  } else {  // whole rows move: a row of W * DimUp reals
+    k_cop_dw<<<grid_rows(to->dw.dim), 256, 0, st>>>(din, dout, W * to->up.dim, to->dw.dim, src.p, sg.p, coef,
                                                     accumulate);
   }
   EDG_CUDA(cudaGetLastError());
@@ -256,7 +289,10 @@ int apply_diagop(const edg_sector_s* s, int kind, const double* wsite, const dou
   EDG_CUDA(cudaMemcpyAsync(w.p, wsite, ns * sizeof(double), cudaMemcpyHostToDevice, st));
   k_site_sum<<<int((s->up.dim + 255) / 256), 256, 0, st>>>(s->up.map.p, s->up.dim, w.p, ns, fu.p);
   k_site_sum<<<int((s->dw.dim + 255) / 256), 256, 0, st>>>(s->dw.map.p, s->dw.dim, w.p, ns, fd.p);
-  k_diagop<<<grid_rows(s->dw.dim), 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, fu.p, fd.p, kind);
+  if (s->cplx)
+    k_diagop<2><<<grid_rows(s->dw.dim), 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, fu.p, fd.p, kind);
+  else
+    k_diagop<1><<<grid_rows(s->dw.dim), 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, fu.p, fd.p, kind);
   EDG_CUDA(cudaGetLastError());
   EDG_CUDA(cudaStreamSynchronize(st));
   return EDG_OK;
@@ -264,7 +300,8 @@ int apply_diagop(const edg_sector_s* s, int kind, const double* wsite, const dou
 
 // J along the site chain 1-2-...-Ns-1 (Norb=1): for each isite, jsite=isite+1 (periodic),
 // + Hij(isite,jsite) c^+_isite c_jsite - conjg(Hij(jsite,isite)) c^+_jsite c_isite, per spin,
-// skipped where Hij is zero (src/OC/OC_ELECTRONS.f90:153-198). Returns r with J|psi> = i r.
+// skipped where Hij is zero (src/OC/OC_ELECTRONS.f90:153-198). Returns r with J|psi> = i r
+// (complex r for complex Hij).
 int apply_current(const edg_sector_s* s, const double* din, double* dout, cudaStream_t st) {
   const edg_model_s& m = s->model;
   const int ns = m.ns;
@@ -272,18 +309,36 @@ int apply_current(const edg_sector_s* s, const double* din, double* dout, cudaSt
   for (int sp = 0; sp < 2; ++sp) {
     const int idx = (m.nspin == 2) ? sp : 0;
     h[sp].nb = 0;
+    auto im = [&](int io, int jo) { return m.him[idx].empty() ? 0.0 : m.him[idx][io * ns + jo]; };
     for (int isite = 0; isite < ns; ++isite) {
       const int jsite = (isite + 1 == ns) ? 0 : isite + 1;
-      const double t1 = m.hre[idx][isite * ns + jsite];  // Hij(io=isite, jo=jsite)
-      if (t1 != 0.0) { h[sp].a[h[sp].nb] = isite; h[sp].b[h[sp].nb] = jsite; h[sp].c[h[sp].nb] = t1; ++h[sp].nb; }
-      const double t2 = m.hre[idx][jsite * ns + isite];  // Hij(io=jsite, jo=isite)
-      if (t2 != 0.0) { h[sp].a[h[sp].nb] = jsite; h[sp].b[h[sp].nb] = isite; h[sp].c[h[sp].nb] = -t2; ++h[sp].nb; }
+      // Hij(io=isite, jo=jsite)
+      const double t1 = m.hre[idx][isite * ns + jsite], t1i = im(isite, jsite);
+      if (t1 != 0.0 || t1i != 0.0) {
+        const int k = h[sp].nb++;
+        h[sp].a[k] = isite;
+        h[sp].b[k] = jsite;
+        h[sp].c[k] = t1;
+        h[sp].ci[k] = t1i;
+      }
+      // -conjg(Hij(io=jsite, jo=isite))
+      const double t2 = m.hre[idx][jsite * ns + isite], t2i = im(jsite, isite);
+      if (t2 != 0.0 || t2i != 0.0) {
+        const int k = h[sp].nb++;
+        h[sp].a[k] = jsite;
+        h[sp].b[k] = isite;
+        h[sp].c[k] = -t2;
+        h[sp].ci[k] = t2i;
+      }
     }
   }
   const int64_t n = s->dim;
   int g = int((n + 255) / 256);
   if (g > 148 * 8) g = 148 * 8;
-  k_hopop<<<g, 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, s->binom.p, h[0], h[1]);
+  if (s->cplx)
+    k_hopop<2><<<g, 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, s->binom.p, h[0], h[1]);
+  else
+    k_hopop<1><<<g, 256, 0, st>>>(din, dout, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, s->binom.p, h[0], h[1]);
   EDG_CUDA(cudaGetLastError());
   EDG_CUDA(cudaStreamSynchronize(st));
   return EDG_OK;
@@ -295,7 +350,10 @@ int observables(const edg_sector_s* s, const double* psi, double weight, double*
   const int g = grid_rows(s->dw.dim);
   DevBuf<double> part;
   EDG_CHECK(part.alloc(size_t(g) * 3 * kMaxSites, st, "observable partials"));
-  k_obs_rows<<<g, 256, 0, st>>>(psi, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, ns, part.p);
+  if (s->cplx)
+    k_obs_rows<2><<<g, 256, 0, st>>>(psi, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, ns, part.p);
+  else
+    k_obs_rows<1><<<g, 256, 0, st>>>(psi, s->up.dim, s->dw.dim, s->up.map.p, s->dw.map.p, ns, part.p);
   EDG_CUDA(cudaGetLastError());
   std::vector<double> h(size_t(g) * 3 * kMaxSites);
   EDG_CUDA(cudaMemcpyAsync(h.data(), part.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -323,7 +381,7 @@ int observables(const edg_sector_s* s, const double* psi, double weight, double*
 int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, double* epot, double* eknot,
            double* ehartree) {
   const int ns = s->model.ns;
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;  // <psi|H psi> over reals = Re <psi|H|psi> for complex psi
   cudaStream_t st = s->stream;
   std::vector<double> dens(ns, 0.0), nup(ns, 0.0), ndw(ns, 0.0), docc(ns, 0.0);
   EDG_CHECK(observables(s, psi, 1.0, dens.data(), nup.data(), ndw.data(), docc.data(), nullptr, st));
@@ -334,8 +392,12 @@ int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, doub
   EDG_CHECK(part.alloc(size_t(kRedBlocks) + kDiagBlocks + 4, st, "energy partials"));
   double* out = part.p + kRedBlocks + kDiagBlocks;
   EDG_CHECK(dot_dev<double>(st, psi, hv, n, part.p, out));
-  k_diag_dot<<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, n, s->up.e64.p, s->dw.e64.p, s->up.map.p, s->dw.map.p,
-                                          s->U, part.p + kRedBlocks);
+  if (s->cplx)
+    k_diag_dot<2><<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, s->dim, s->up.e64.p, s->dw.e64.p, s->up.map.p,
+                                               s->dw.map.p, s->U, part.p + kRedBlocks);
+  else
+    k_diag_dot<1><<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, s->dim, s->up.e64.p, s->dw.e64.p, s->up.map.p,
+                                               s->dw.map.p, s->U, part.p + kRedBlocks);
   EDG_CUDA(cudaGetLastError());
   EDG_CHECK(finish_dev(st, part.p + kRedBlocks, kDiagBlocks, out + 1, 0));
   double h[2] = {0.0, 0.0};
