@@ -90,16 +90,6 @@ int check_sector(const edg_sector_s* s) {
   return EDG_OK;
 }
 
-// Entry points whose complex-Hij form is not built: the lowest-k solver and the dense sector
-// matrix.
-int real_only(const edg_sector_s* s, const char* what) {
-  if (s && s->cplx) {
-    set_error("%s: not available for complex Hij sectors", what);
-    return EDG_ERR_UNSUPPORTED;
-  }
-  return EDG_OK;
-}
-
 // Device vectors of a complex sector hold (re, im) pairs: 2*sizeof(T)-aligned.
 template <typename T>
 int check_vec_align(const edg_sector_s* s, const void* p, const char* what) {
@@ -422,7 +412,6 @@ int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, 
 int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol, double* evals,
                  double* evecs, double* resid, int* niter) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_lowest_k"));
   EDG_ARG(evals && niter, "edg_lowest_k: NULL output");
   EDG_ARG(k >= 1 && k <= 16, "edg_lowest_k: k=%d outside 1..16", k);
   EDG_ARG(maxit >= 1, "edg_lowest_k: maxit=%d", maxit);
@@ -433,7 +422,6 @@ int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxi
 
 int edg_sector_dense(edg_sector* s, double* h) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_sector_dense"));
   EDG_ARG(h, "edg_sector_dense: NULL");
   EDG_CHECK(ensure_device(s));
   return sector_dense(s, h);
@@ -441,7 +429,6 @@ int edg_sector_dense(edg_sector* s, double* h) {
 
 int edg_sector_dense_dev(edg_sector* s, double* dh) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(real_only(s, "edg_sector_dense_dev"));
   EDG_ARG(dh, "edg_sector_dense_dev: NULL");
   EDG_CHECK(ensure_device(s));
   return sector_dense_dev(s, dh);

@@ -92,6 +92,88 @@ int launch_multidot(const double* Q, int m, int64_t n, const double* w, double* 
   return EDG_OK;
 }
 
+// Complex vectors (complex-Hij sectors, elements (re, im)): c_j = <q_j|w> = sum conj(q) w,
+// real parts into partial[j * nsplit + s], imaginary parts into partial[(m + j) * nsplit + s],
+// one read of the basis for both. Complex Gram-Schmidt against Q is real Gram-Schmidt against
+// Q and iQ in the real embedding, so the recurrence is otherwise unchanged.
+template <int G>
+__global__ void __launch_bounds__(kLkThreads) k_multidot_c(const double2* __restrict__ Q, int m, int64_t n,
+                                                           const double2* __restrict__ w, double* __restrict__ partial) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nsplit = gridDim.x * (kLkThreads / 32);
+  const int split = blockIdx.x * (kLkThreads / 32) + warp;
+  int64_t chunk = (n + nsplit - 1) / nsplit;
+  chunk = (chunk + 31) & ~int64_t(31);
+  const int64_t i0 = split * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
+  const int j0 = blockIdx.y * G;
+  const double2* __restrict__ q[G];
+#pragma unroll
+  for (int c = 0; c < G; ++c) q[c] = Q + int64_t(j0 + c < m ? j0 + c : m - 1) * n;
+  double ar[G], ai[G];
+#pragma unroll
+  for (int c = 0; c < G; ++c) ar[c] = ai[c] = 0.0;
+  for (int64_t i = i0 + lane; i < i1; i += 32) {
+    const double2 wi = w[i];
+#pragma unroll
+    for (int c = 0; c < G; ++c) {
+      const double2 x = q[c][i];
+      ar[c] = __fma_rn(x.x, wi.x, ar[c]);
+      ar[c] = __fma_rn(x.y, wi.y, ar[c]);
+      ai[c] = __fma_rn(x.x, wi.y, ai[c]);
+      ai[c] = __fma_rn(-x.y, wi.x, ai[c]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < G; ++c) {
+    double tr = ar[c], ti = ai[c];
+    for (int o = 16; o > 0; o >>= 1) {
+      tr += __shfl_down_sync(0xffffffffu, tr, o);
+      ti += __shfl_down_sync(0xffffffffu, ti, o);
+    }
+    if (lane == 0 && j0 + c < m) {
+      partial[int64_t(j0 + c) * nsplit + split] = tr;
+      partial[int64_t(m + j0 + c) * nsplit + split] = ti;
+    }
+  }
+}
+
+int launch_multidot_c(const double* Q, int m, int64_t n, const double* w, double* partial, cudaStream_t st,
+                      int* nsplit) {
+  const DotShape d = dot_shape(m, n);
+  const dim3 grid(d.gx, (m + d.G - 1) / d.G);
+  const double2* Q2 = reinterpret_cast<const double2*>(Q);
+  const double2* w2 = reinterpret_cast<const double2*>(w);
+  if (d.G == 8)
+    k_multidot_c<8><<<grid, kLkThreads, 0, st>>>(Q2, m, n, w2, partial);
+  else
+    k_multidot_c<4><<<grid, kLkThreads, 0, st>>>(Q2, m, n, w2, partial);
+  *nsplit = d.nsplit();
+  return EDG_OK;
+}
+
+// w[i] -= sum_j (cr[j] + i ci[j]) Q[j][i] on complex elements
+__global__ void __launch_bounds__(kLkThreads) k_multiaxpy_c(const double2* __restrict__ Q, const double* __restrict__ c,
+                                                            int m, int64_t n, double2* __restrict__ w) {
+  __shared__ double sr[kMaxBasis], si[kMaxBasis];
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    sr[j] = c[j];
+    si[j] = c[m + j];
+  }
+  __syncthreads();
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    double2 t = w[i];
+#pragma unroll 4
+    for (int j = 0; j < m; ++j) {
+      const double2 q = Q[int64_t(j) * n + i];
+      t.x = __fma_rn(-sr[j], q.x, t.x);
+      t.x = __fma_rn(si[j], q.y, t.x);
+      t.y = __fma_rn(-sr[j], q.y, t.y);
+      t.y = __fma_rn(-si[j], q.x, t.y);
+    }
+    w[i] = t;
+  }
+}
+
 __global__ void k_copy1(double* __restrict__ dst, const double* __restrict__ src) { *dst = *src; }
 
 // c[j] = sum_blk partial[j * nblk + blk], one warp per column, fixed order
@@ -137,10 +219,13 @@ __global__ void __launch_bounds__(kLkThreads) k_ritz_k(const double* __restrict_
   }
 }
 
-// Dense sector matrix, column-major H[i + j*D]: one thread per row i = iup + idw*DimUp.
+// Dense sector matrix, column-major H[i + j*D] (W = 2: complex, interleaved, with the
+// imaginary hop values vi_*): one thread per row i = iup + idw*DimUp.
+template <int W>
 __global__ void k_dense(const uint32_t* __restrict__ off_up, const uint32_t* __restrict__ src_up,
-                        const double* __restrict__ val_up, const uint32_t* __restrict__ off_dw,
-                        const uint32_t* __restrict__ src_dw, const double* __restrict__ val_dw,
+                        const double* __restrict__ val_up, const double* __restrict__ vi_up,
+                        const uint32_t* __restrict__ off_dw, const uint32_t* __restrict__ src_dw,
+                        const double* __restrict__ val_dw, const double* __restrict__ vi_dw,
                         const double* __restrict__ e_up, const double* __restrict__ e_dw,
                         const uint32_t* __restrict__ map_up, const uint32_t* __restrict__ map_dw, double U,
                         int64_t dimup, int64_t dimdw, double* __restrict__ H) {
@@ -148,14 +233,16 @@ __global__ void k_dense(const uint32_t* __restrict__ off_up, const uint32_t* __r
   const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   if (i >= D) return;
   const int64_t idw = i / dimup, iup = i - idw * dimup;
-  H[i + i * D] += e_up[iup] + e_dw[idw] + U * double(__popc(map_up[iup] & map_dw[idw]));
+  H[(i + i * D) * W] += e_up[iup] + e_dw[idw] + U * double(__popc(map_up[iup] & map_dw[idw]));
   for (uint32_t k = off_up[iup]; k < off_up[iup + 1]; ++k) {
     const int64_t j = int64_t(src_up[k]) + idw * dimup;
-    H[i + j * D] += val_up[k];
+    H[(i + j * D) * W] += val_up[k];
+    if (W == 2) H[(i + j * D) * W + W - 1] += vi_up[k];
   }
   for (uint32_t k = off_dw[idw]; k < off_dw[idw + 1]; ++k) {
     const int64_t j = iup + int64_t(src_dw[k]) * dimup;
-    H[i + j * D] += val_dw[k];
+    H[(i + j * D) * W] += val_dw[k];
+    if (W == 2) H[(i + j * D) * W + W - 1] += vi_dw[k];
   }
 }
 
@@ -177,10 +264,17 @@ int sector_dense_dev(edg_sector_s* s, double* dH) {
     return EDG_ERR_STATE;
   }
   cudaStream_t st = s->stream;
-  EDG_CUDA(cudaMemsetAsync(dH, 0, size_t(D) * D * sizeof(double), st));
-  k_dense<<<int((D + 255) / 256), 256, 0, st>>>(s->up.off.p, s->up.src.p, s->up.val64.p, s->dw.off.p, s->dw.src.p,
-                                                s->dw.val64.p, s->up.e64.p, s->dw.e64.p, s->up.map.p, s->dw.map.p,
-                                                s->U, s->up.dim, s->dw.dim, dH);
+  const int W = s->cplx ? 2 : 1;
+  EDG_CUDA(cudaMemsetAsync(dH, 0, size_t(D) * D * W * sizeof(double), st));
+  if (W == 2)
+    k_dense<2><<<int((D + 255) / 256), 256, 0, st>>>(s->up.off.p, s->up.src.p, s->up.val64.p, s->up.val64i.p,
+                                                     s->dw.off.p, s->dw.src.p, s->dw.val64.p, s->dw.val64i.p,
+                                                     s->up.e64.p, s->dw.e64.p, s->up.map.p, s->dw.map.p, s->U,
+                                                     s->up.dim, s->dw.dim, dH);
+  else
+    k_dense<1><<<int((D + 255) / 256), 256, 0, st>>>(s->up.off.p, s->up.src.p, s->up.val64.p, nullptr, s->dw.off.p,
+                                                     s->dw.src.p, s->dw.val64.p, nullptr, s->up.e64.p, s->dw.e64.p,
+                                                     s->up.map.p, s->dw.map.p, s->U, s->up.dim, s->dw.dim, dH);
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -191,11 +285,12 @@ int sector_dense(edg_sector_s* s, double* H_host) {
     set_error("edg_sector_dense: dimension %lld above %d", (long long)D, kDenseMaxDim);
     return EDG_ERR_ARG;
   }
+  const size_t W = s->cplx ? 2 : 1;
   DevBuf<double> Hd;
-  EDG_CHECK(Hd.alloc(size_t(D) * D, s->stream, "dense sector matrix"));
+  EDG_CHECK(Hd.alloc(size_t(D) * D * W, s->stream, "dense sector matrix"));
   EDG_CHECK(sector_dense_dev(s, Hd.p));
   cudaStream_t st = s->stream;
-  EDG_CUDA(cudaMemcpyAsync(H_host, Hd.p, size_t(D) * D * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaMemcpyAsync(H_host, Hd.p, size_t(D) * D * W * sizeof(double), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));
   return EDG_OK;
 }
@@ -207,14 +302,16 @@ constexpr double kRitzRelGap = 1e-5;
 
 int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, double* evals,
              double* evecs_host, double* resid, int* niter) {
-  const int64_t n = s->dim;
+  const int64_t n = s->vlen;   // reals per vector
+  const int64_t ne = s->dim;   // elements per vector (complex ones for complex Hij)
+  const bool cplx = s->cplx;
   cudaStream_t st = s->stream;
   if (k < 1 || k > kMaxK) {
     set_error("edg_lowest_k: k=%d outside 1..%d", k, kMaxK);
     return EDG_ERR_ARG;
   }
-  if (k > n) k = int(n);
-  int mmax = std::min<int64_t>(std::min(maxit, kMaxBasis), n);
+  if (k > ne) k = int(ne);
+  int mmax = std::min<int64_t>(std::min(maxit, kMaxBasis), ne);
   if (mmax < k) mmax = k;
   {  // the basis takes what HBM allows beyond a 2 GB reserve
     size_t fr = 0, tot = 0;
@@ -233,9 +330,10 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
   EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
   size_t npart = kRedBlocks;  // also the norm's scratch
-  for (int mm = 1; mm <= mmax; ++mm) npart = std::max(npart, size_t(mm) * dot_shape(mm, n).nsplit());
+  for (int mm = 1; mm <= mmax; ++mm)
+    npart = std::max(npart, size_t(cplx ? 2 : 1) * mm * dot_shape(mm, cplx ? ne : n).nsplit());
   EDG_CHECK(part.alloc(npart, st, "multi-dot partials"));
-  EDG_CHECK(coef.alloc(size_t(mmax) + 8, st, "multi-dot coefficients"));
+  EDG_CHECK(coef.alloc(2 * size_t(mmax) + 8, st, "multi-dot coefficients"));
   // start vector
   if (v0_host) {
     EDG_CUDA(cudaMemcpyAsync(Q.p, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -270,19 +368,27 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     EDG_CHECK(hxv_apply<double>(s, qj, w.p));
     for (int pass = 0; pass < 2; ++pass) {
       int nsplit = 0;
-      EDG_CHECK(launch_multidot(Q.p, j + 1, n, w.p, part.p, st, &nsplit));
-      k_multifinish<<<(j + 1 + 7) / 8, 256, 0, st>>>(part.p, nsplit, j + 1, coef.p);
-      if (pass == 0) k_copy1<<<1, 1, 0, st>>>(dA + j, coef.p + j);  // a_j = <q_j, H q_j>
-      k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
+      const int nc = cplx ? 2 * (j + 1) : j + 1;  // coefficients: real parts, then imaginary parts
+      if (cplx)
+        EDG_CHECK(launch_multidot_c(Q.p, j + 1, ne, w.p, part.p, st, &nsplit));
+      else
+        EDG_CHECK(launch_multidot(Q.p, j + 1, n, w.p, part.p, st, &nsplit));
+      k_multifinish<<<(nc + 7) / 8, 256, 0, st>>>(part.p, nsplit, nc, coef.p);
+      if (pass == 0) k_copy1<<<1, 1, 0, st>>>(dA + j, coef.p + j);  // a_j = Re <q_j, H q_j>
+      if (cplx)
+        k_multiaxpy_c<<<grid_n(ne), kLkThreads, 0, st>>>(reinterpret_cast<const double2*>(Q.p), coef.p, j + 1, ne,
+                                                         reinterpret_cast<double2*>(w.p));
+      else
+        k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p, j + 1, n, w.p);
     }
     EDG_CUDA(cudaGetLastError());
     EDG_CHECK(norm_dev(st, w.p, n, part.p, dB + j + 1));
     m = j + 1;
-    if ((m >= k && m >= next_check) || m == mmax || m == n) {
+    if ((m >= k && m >= next_check) || m == mmax || m == ne) {
       EDG_CUDA(cudaMemcpyAsync(hA.data(), dA, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
       EDG_CUDA(cudaMemcpyAsync(hB.data(), dB, size_t(m + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
       EDG_CUDA(cudaStreamSynchronize(st));
-      bool last = m == mmax || m == n;
+      bool last = m == mmax || m == ne;
       for (int t = 0; t < m; ++t)
         if (!(hB[t + 1] >= 1e-12)) {  // invariant subspace reached at step t (or NaN)
           m = t + 1;

@@ -185,10 +185,11 @@ def _dense_lowest(sec: Sector, neigen: int):
         raise L.EdgError(L.EDG_ERR_NODEVICE, "ed_diag_d", "dense branch needs a CUDA device")
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream(dev)
-    h = torch.empty((sec.dim, sec.dim), dtype=torch.float64, device=dev)
+    h = torch.empty((sec.dim, sec.dim), dtype=torch.complex128 if sec.cplx else torch.float64, device=dev)
     sec.set_stream(stream.cuda_stream)
     sec.dense_dev(h.data_ptr())
-    w, z = torch.linalg.eigh(h)
+    # the buffer is column-major: read row-major it is H^T (= H for real, conj(H) for complex)
+    w, z = torch.linalg.eigh(h.mT if sec.cplx else h)
     return w[:neigen].cpu().numpy(), z[:, :neigen].T.contiguous().cpu().numpy()
 
 
@@ -446,7 +447,7 @@ def lanc_observables(model: Model, state_list: StateList, zeta: float, params: D
                 sec = sectors.get(st.sector)
                 if sec is None:
                     sec = sectors[st.sector] = Sector.from_index(model, st.sector)
-                sec.set_state(np.real(st.vec))
+                sec.set_state(st.vec)
                 obs = sec.observables(bw)
             for k in out:
                 out[k] += obs[k]
@@ -485,7 +486,7 @@ def lanc_energy(model: Model, state_list: StateList, zeta: float, params: DiagPa
                 sec = sectors.get(st.sector)
                 if sec is None:
                     sec = sectors[st.sector] = Sector.from_index(model, st.sector)
-                sec.set_state(np.real(st.vec))
+                sec.set_state(st.vec)
                 en = sec.energy(bw)
             for k in out:
                 out[k] += en[k]

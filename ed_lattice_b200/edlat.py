@@ -229,23 +229,29 @@ class Sector:
         kk = min(k, self.dim)
         ev = np.zeros(k)
         rs = np.zeros(k)
-        vecs = np.empty((kk, self.dim)) if want_vectors else None
+        vecs = np.empty((kk, self.vlen)) if want_vectors else None
         it = C.c_int()
-        v0a = _f64(v0) if v0 is not None else None
-        if v0a is not None and v0a.size != self.dim:
-            raise ValueError("v0 size != sector dimension")
+        v0a = self._vec(v0, "v0") if v0 is not None else None
         L.check(L.lib().edg_lowest_k(self.handle, k, _pd(v0a), C.c_uint64(seed), maxit, tol, _pd(ev), _pd(vecs),
                                      _pd(rs), C.byref(it)), "sp_eigh")
+        if vecs is not None and self.cplx:
+            vecs = vecs.view(np.complex128)
         return ev[:kk], vecs, rs[:kk], it.value
 
     def dense(self) -> np.ndarray:
-        """Dense sector matrix of ed_buildh(Hmat) (src/DIAG/HAMILTONIAN_STORED_HxV.f90:81-117)."""
+        """Dense sector matrix of ed_buildh(Hmat) (src/DIAG/HAMILTONIAN_STORED_HxV.f90:81-117),
+        complex for a complex-Hij sector."""
+        if self.cplx:
+            h = np.empty((self.dim, self.dim), dtype=np.complex128, order="F")  # the library writes column-major
+            L.check(L.lib().edg_sector_dense(self.handle, h.ctypes.data_as(L._pd)), "ed_buildh")
+            return h
         h = np.empty((self.dim, self.dim))
         L.check(L.lib().edg_sector_dense(self.handle, _pd(h)), "ed_buildh")
         return h  # symmetric: row- and column-major read the same
 
     def dense_dev(self, dh_ptr: int) -> None:
-        """Dense sector matrix into device memory (dim*dim doubles) on the sector's stream."""
+        """Dense sector matrix into device memory (dim*dim doubles, or dim*dim interleaved
+        complex for a complex-Hij sector; column-major) on the sector's stream."""
         L.check(L.lib().edg_sector_dense_dev(self.handle, C.c_void_p(dh_ptr)), "ed_buildh")
 
     # ---- state buffer (the eigenvector kept on the device)

@@ -80,7 +80,7 @@ class _DeviceChains:
     def load(self, isector: int, vec) -> Sector:
         src = self.sector(isector)
         if self.loaded is None or self.loaded[0] != isector or self.loaded[1] is not vec:
-            src.set_state(np.real(vec))
+            src.set_state(vec)
             self.loaded = (isector, vec)
         return src
 

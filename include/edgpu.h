@@ -88,8 +88,7 @@ int edg_sector_dims(const edg_sector* s, int64_t* dim, int64_t* dimup, int64_t* 
  * reference's vectors are complex(8) throughout; with complex Hij every vector argument of
  * this API (host or device: start vectors, H x v operands, states) holds dim complex
  * elements interleaved (re, im), device ones 2*sizeof(T)-aligned, and the Lanczos scalars
- * stay real. Not built for complex Hij (EDG_ERR_UNSUPPORTED): edg_lowest_k and
- * edg_sector_dense(_dev). */
+ * stay real. edg_sector_dense(_dev) then writes dim x dim complex entries. */
 int edg_sector_vlen(const edg_sector* s, int64_t* vlen);
 /* Copy the device-built maps Hsector%H(1)%map / H(2)%map (bitstrings, ascending). */
 int edg_sector_get_maps(const edg_sector* s, int32_t* map_up, int32_t* map_dw);

@@ -164,18 +164,20 @@ def test_complex_ground_state_vs_dense(mode):
     s.delete()
 
 
-def test_complex_unsupported_entries_and_errors():
+def test_complex_errors():
+    """Real host vectors are refused by edg_hxv_d on a complex sector; state sizes are checked;
+    c/c+ between a complex and a real sector is refused."""
     gm = E.Model(flux_ring(6, 0.5), uloc=1.0)
     s = E.Sector(gm, 3, 3)
     with pytest.raises(E.EdgError) as ei:
         s.hxv_real(np.zeros(s.dim))
     assert ei.value.status == L.EDG_ERR_ARG
+    E.sp_lanc_eigh(s, tol=1e-10)
+    r4 = E.Sector(E.Model(ring(6), uloc=1.0), 4, 3)
     with pytest.raises(E.EdgError) as ei:
-        s.lowest_k(2)
-    assert ei.value.status == L.EDG_ERR_UNSUPPORTED
-    with pytest.raises(E.EdgError) as ei:
-        s.dense()
-    assert ei.value.status == L.EDG_ERR_UNSUPPORTED
+        E.gf_chain(s, r4, +1, 1, 1, 10, 0.0)
+    assert ei.value.status == L.EDG_ERR_ARG
+    r4.delete()
     with pytest.raises(ValueError):
         s.set_state(np.zeros(s.dim + 1))
     s.delete()
@@ -330,3 +332,68 @@ def test_complex_gf_chain_vs_lehmann():
         assert np.abs(g - g_ref).max() <= 1e-8 * np.abs(g_ref).max()
         sJ.delete()
     s.delete()
+
+
+# ----------------------------------------------------------------------------- lowest k, dense, driver
+def test_complex_dense_matrix_vs_oracle():
+    gm, om = models(flux_ring(6, 0.6, seed=12), uloc=2.0, xmu=1.0, hfmode=True)
+    s = E.Sector(gm, 3, 2)
+    Hd = dense_from_matvec(O.Stored(om, 3, 2).matvec_z, s.dim)
+    assert np.abs(s.dense() - Hd).max() < 1e-14
+    s.delete()
+
+
+@pytest.mark.parametrize("seed", [17, 3])
+def test_complex_lowest_k_vs_dense(seed):
+    """Lowest four levels of a complex sector (D = 1568) with their vectors: levels to 1e-10
+    against dense diagonalisation (so no level appears twice: complex Gram-Schmidt keeps the
+    i-rotated copies of the basis out), residuals under the oracle's H x v, orthonormality."""
+    gm, om = models(flux_ring(8, 1.3, seed=5), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(gm, 2, 3)
+    st = O.Stored(om, 2, 3)
+    ref = np.linalg.eigvalsh(dense_from_matvec(st.matvec_z, s.dim))[:4]
+    ev, vecs, resid, m = s.lowest_k(4, seed=seed, tol=1e-11)
+    assert np.abs(ev - ref).max() <= 1e-10 * np.abs(ref).max(), (ev, ref)
+    assert vecs.dtype == np.complex128
+    for r in range(4):
+        x = vecs[r]
+        assert abs(np.vdot(x, x).real - 1.0) < 1e-10
+        assert np.linalg.norm(st.matvec_z(x) - ev[r] * x) < 1e-8
+        for q in range(r):
+            assert abs(np.vdot(vecs[q], x)) < 1e-9
+    s.delete()
+
+
+def test_complex_thermal_driver_vs_brute_force():
+    """diagonalize_lattice + partition_function + lanc_observables on a complex model (6-site
+    ring with flux, all 49 sectors, Lanczos everywhere) against every eigenstate of every
+    sector from dense diagonalisation of the oracle's complex H."""
+    import math
+
+    from ed_lattice_b200.diag import DiagParams, diagonalize_lattice, lanc_observables, partition_function
+
+    ns, temp = 6, 0.3
+    H = flux_ring(ns, 0.9, seed=21)
+    gm, om = models(H, uloc=3.0, xmu=1.5, hfmode=False)
+    p = DiagParams(finite_temp=True, temp=temp, lanc_nstates_sector=4, lanc_dim_threshold=0, lanc_tolerance=1e-11)
+    sl, eigs = diagonalize_lattice(gm, p, seed=7)
+    zeta = partition_function(sl, p)
+    obs = lanc_observables(gm, sl, zeta, p)
+    states = []
+    for nup in range(ns + 1):
+        for ndw in range(ns + 1):
+            D = math.comb(ns, nup) * math.comb(ns, ndw)
+            w, V = np.linalg.eigh(dense_from_matvec(O.Stored(om, nup, ndw).matvec_z, D))
+            states += [(w[i], nup, ndw, V[:, i]) for i in range(min(4, D))]
+    egs = min(st[0] for st in states)
+    kept = sorted((st for st in states if math.exp(-(st[0] - egs) / temp) > p.cutoff), key=lambda st: st[0])
+    zref = sum(math.exp(-(st[0] - egs) / temp) for st in kept)
+    assert sl.emin == pytest.approx(egs, abs=1e-10)
+    assert zeta == pytest.approx(zref, rel=1e-9)
+    ref = {k: np.zeros(ns) for k in ("dens", "dens_up", "dens_dw", "docc")}
+    for e, nup, ndw, v in kept:
+        o = O.observables(ns, nup, ndw, np.abs(v), math.exp(-(e - egs) / temp) / zref)
+        for k in ref:
+            ref[k] += o[k]
+    for k in ref:
+        assert np.allclose(obs[k], ref[k], atol=1e-9), k
