@@ -54,6 +54,7 @@ SIGNATURES = {
     "edg_sector_destroy": (_i, [_p]),
     "edg_sector_dims": (_i, [_p, _pi64, _pi64, _pi64]),
     "edg_sector_vlen": (_i, [_p, _pi64]),
+    "edg_release_cached_memory": (_i, []),
     "edg_sector_get_maps": (_i, [_p, _pi32, _pi32]),
     "edg_sector_get_hops": (_i, [_p, _i, _pi64, _pi32, _pd, _pi64]),
     "edg_sector_set_stream": (_i, [_p, _p]),

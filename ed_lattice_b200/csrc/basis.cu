@@ -43,16 +43,22 @@ const char* get_error() { return g_err; }
 // state and other users of the device.
 static const size_t kReserveBytes = size_t(1) << 30;
 
-// Stream-ordered allocations from a library-owned pool per device that keeps up to a
-// quarter of the device memory (at least kPoolKeepBytes) of freed memory for reuse: above
-// that, every synchronisation hands memory back to the driver, which stalls like cudaFree
-// when several sectors' Lanczos bases are alive at once. A request is refused when it would leave less than
-// kReserveBytes of HBM free (memory held by the pool counts as used); the driver's free-memory query is skipped when the pool already
-// holds enough idle memory for the request.
+// Stream-ordered allocations from a library-owned pool per device. The pool never hands
+// memory back to the driver on its own: with a release threshold, every synchronisation
+// returned the memory above it, and while one large buffer stayed alive (a sector's FP32
+// basis) every solve's freed work space went back to the driver and came again through it,
+// which stalls on a busy driver like cudaMalloc/cudaFree. Instead, freeing a buffer of
+// kTrimBytes or more trims the pool's idle memory (beyond what is in use) to a quarter of the
+// device memory (at least kPoolKeepBytes), and edg_release_cached_memory trims it on request. A request is refused
+// when it would leave less than kReserveBytes of HBM free (memory held by the pool counts as
+// used); the driver's free-memory query is skipped when the pool already holds enough idle
+// memory for it.
 namespace {
 constexpr int kPoolDevices = 64;
 constexpr uint64_t kPoolKeepBytes = uint64_t(8) << 30;
+constexpr size_t kTrimBytes = size_t(1) << 30;
 cudaMemPool_t g_pool[kPoolDevices] = {};
+uint64_t g_pool_keep[kPoolDevices] = {};
 std::mutex g_pool_mu;
 thread_local cudaStream_t t_free_stream = nullptr;
 thread_local bool t_free_override = false;
@@ -88,8 +94,9 @@ int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
       EDG_CUDA(cudaMemPoolCreate(&g_pool[dev], &props));
       size_t fr = 0, total = 0;
       EDG_CUDA(cudaMemGetInfo(&fr, &total));
-      uint64_t keep = std::max<uint64_t>(kPoolKeepBytes, total / 4);
-      EDG_CUDA(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+      g_pool_keep[dev] = std::max<uint64_t>(kPoolKeepBytes, total / 4);
+      uint64_t never = UINT64_MAX;
+      EDG_CUDA(cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &never));
     }
     pool = g_pool[dev];
   }
@@ -115,8 +122,40 @@ int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
   return EDG_OK;
 }
 
-void pool_free(void* p, cudaStream_t st) {
-  if (p) cudaFreeAsync(p, st);
+void pool_free(void* p, cudaStream_t st, size_t bytes) {
+  if (!p) return;
+  cudaFreeAsync(p, st);
+  if (bytes < kTrimBytes) return;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kPoolDevices) return;
+  cudaMemPool_t pool = nullptr;
+  uint64_t keep = 0;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    pool = g_pool[dev];
+    keep = g_pool_keep[dev];
+  }
+  if (!pool) return;
+  // the trim target counts memory in use too: keep `keep` bytes idle on top of it
+  size_t used = 0;
+  if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess)
+    cudaMemPoolTrimTo(pool, used + keep);
+}
+
+int pool_trim(size_t keep) {
+  int dev = 0;
+  EDG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kPoolDevices) return EDG_OK;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    pool = g_pool[dev];
+  }
+  if (pool) {
+    EDG_CUDA(cudaDeviceSynchronize());  // frees still queued on streams become trimmable
+    EDG_CUDA(cudaMemPoolTrimTo(pool, keep));
+  }
+  return EDG_OK;
 }
 
 uint64_t binom_host(int n, int k) {

@@ -242,6 +242,8 @@ int edg_sector_destroy(edg_sector* s) {
   return EDG_OK;
 }
 
+int edg_release_cached_memory(void) { return pool_trim(0); }
+
 int edg_sector_vlen(const edg_sector* s, int64_t* vlen) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(vlen, "edg_sector_vlen: NULL");

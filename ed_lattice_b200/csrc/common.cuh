@@ -39,7 +39,8 @@ const char* get_error();
 // from this pool: on a machine whose driver is busy with other processes, a plain
 // cudaMalloc/cudaFree pair took up to 0.8 s, and a finite-temperature loop makes hundreds.
 int pool_alloc(void** p, size_t bytes, cudaStream_t st, const char* what);
-void pool_free(void* p, cudaStream_t st);
+void pool_free(void* p, cudaStream_t st, size_t bytes);
+int pool_trim(size_t keep);  // hand the pool's idle memory above `keep` back to the driver
 
 // While one of these is alive on a thread, buffers released on that thread go back to the
 // pool on `st` instead of the stream they were last allocated on. The sector destructor
@@ -82,7 +83,7 @@ struct DevBuf {
     return s;
   }
   void reset() {
-    if (p) pool_free(p, free_stream(st));
+    if (p) pool_free(p, free_stream(st), n * sizeof(T));
     p = nullptr;
     n = 0;
   }

@@ -55,6 +55,10 @@ typedef struct edg_sector_s edg_sector;
 
 const char* edg_last_error(void);
 int edg_device_count(int* n);
+/* Hand the device memory that the library's allocation pool holds for reuse (up to a quarter
+ * of the current device's memory, kept between sectors) back to the driver, after waiting for
+ * the device. No counterpart in the reference. */
+int edg_release_cached_memory(void);
 
 /* ------------------------------------------------------------------ model
  * Replaces Hij_init/Hij_add_link/Hij_build/Hij_get (src/GRAPH_MATRIX.f90:79-344) plus the
