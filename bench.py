@@ -210,22 +210,26 @@ def e0_time_to_solution(E, L, sector, seed=2024, maxit=600):
 def thermal_3x4(E):
     """Finite-temperature diagonalisation of the 3x4 disordered lattice (t=1, U=4, XMU=2,
     eps_i ~ uniform[-1,1) quantised to 2^-16, seed 7): lowest 4 levels of all 169 sectors,
-    state list, Z and site observables at beta=20. Wall time of the whole driver."""
+    state list, Z and site observables at beta=20. Wall time of the whole driver: a first
+    call, then the reported one."""
     import torch
     from ed_lattice_b200.diag import DiagParams, diagonalize_lattice, lanc_observables, partition_function
     rng = np.random.default_rng(7)
     H = E.square_lattice(3, 4)
     H[np.diag_indices(12)] = np.round(rng.uniform(-1, 1, 12) * 65536) / 65536
     model = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
-    p = DiagParams(finite_temp=True, temp=0.05, lanc_nstates_sector=4, lanc_dim_threshold=1024)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    sl, eigs = diagonalize_lattice(model, p)
-    zeta = partition_function(sl, p)
-    obs = lanc_observables(model, sl, zeta, p)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
-    return {"seconds": dt, "sectors": len(eigs), "lanczos_sectors": sum(1 for e in eigs if e[2]),
+    runs = []
+    for _ in range(2):  # the first call also loads the solver kernels and the dense eigensolver
+        p = DiagParams(finite_temp=True, temp=0.05, lanc_nstates_sector=4, lanc_dim_threshold=1024)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sl, eigs = diagonalize_lattice(model, p)
+        zeta = partition_function(sl, p)
+        obs = lanc_observables(model, sl, zeta, p)
+        torch.cuda.synchronize()
+        runs.append(time.perf_counter() - t0)
+    return {"seconds": runs[1], "first_call_seconds": runs[0], "sector_threads": p.sector_threads,
+            "sectors": len(eigs), "lanczos_sectors": sum(1 for e in eigs if e[2]),
             "states_kept": sl.trimd_size, "egs": sl.emin, "zeta": zeta, "dens_total": float(obs["dens"].sum()),
             "docc_mean": float(obs["docc"].mean())}
 
