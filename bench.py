@@ -234,6 +234,31 @@ def thermal_3x4(E):
             "docc_mean": float(obs["docc"].mean())}
 
 
+def lowest_k_3x4(E):
+    """The lowest 4 levels and vectors of the largest sector of the 3x4 disordered lattice
+    (the thermal workload's (6,6), D = 853,776) with edg_lowest_k, after one untimed solve.
+    Reorthogonalisation bytes: two Gram-Schmidt passes per step, each reading the j-vector
+    basis twice (multi-dot and multi-axpy): 4 j D 8 bytes at step j."""
+    import torch
+    rng = np.random.default_rng(7)
+    H = E.square_lattice(3, 4)
+    H[np.diag_indices(12)] = np.round(rng.uniform(-1, 1, 12) * 65536) / 65536
+    model = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(model, 6, 6)
+    runs = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev, _, resid, m = s.lowest_k(4, seed=1234, maxit=512, tol=1e-10)
+        torch.cuda.synchronize()
+        runs.append(time.perf_counter() - t0)
+    reorth = sum(4 * j * s.dim * 8 for j in range(1, m + 1))
+    s.delete()
+    return {"seconds": runs[1], "first_call_seconds": runs[0], "dim": s.dim, "basis": m,
+            "ms_per_step": 1e3 * runs[1] / m, "reorth_bytes": reorth, "reorth_GBps": reorth / runs[1] / 1e9,
+            "e0": float(ev[0]), "max_resid": float(np.max(resid))}
+
+
 def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150):
     """Green's function chains on the 4x4 lattice at U=4 (t=1, XMU=2): ground state of the
     half-filled sector (8,8) (FP32+refine, vector kept on the device), then c^+_{i,up} into
@@ -399,6 +424,8 @@ def run_ours(args):
         extra["e0_time_to_1e-8"] = e0_time_to_solution(E, L, sector)
     if rank == 0 and not args.no_thermal and ws == 1:
         extra["thermal_3x4_beta20"] = thermal_3x4(E)
+    if rank == 0 and not args.no_lowk and ws == 1:
+        extra["lowest_k_3x4_sector66"] = lowest_k_3x4(E)
     if rank == 0 and not args.no_gf and ws == 1:
         sector.delete()
         torch.cuda.empty_cache()
@@ -448,6 +475,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-thermal", action="store_true")
     ap.add_argument("--no-gf", action="store_true")
+    ap.add_argument("--no-lowk", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
