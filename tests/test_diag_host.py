@@ -398,3 +398,45 @@ def test_threaded_state_map_contexts_and_errors():
         _map_states(sl, None, "test", bad, 4, Ctx)
     assert all(c.closed for c in made)
     assert _map_states(sl, None, "test", lambda i, st, c: i, 1) == {i: i for i in range(1, 21)}
+
+
+def test_device_chain_cache_eviction(monkeypatch):
+    """gf._DeviceChains keeps the `keep` most recently used sectors, deletes the others, and
+    reloads a state whose source sector was evicted (fake sectors: no device needed)."""
+    from ed_lattice_b200 import gf
+
+    made, deleted, loads = [], [], []
+
+    class FakeSector:
+        def __init__(self, isector):
+            self.isector = isector
+            made.append(isector)
+
+        @classmethod
+        def from_index(cls, model, isector):
+            return cls(isector)
+
+        def delete(self):
+            deleted.append(self.isector)
+
+        def set_state(self, vec):
+            loads.append(self.isector)
+
+    monkeypatch.setattr(gf, "Sector", FakeSector)
+    dc = gf._DeviceChains(model=None, precision=0, keep=3)
+    for i in (1, 2, 3, 4):
+        dc.sector(i)
+    assert list(dc.sectors) == [2, 3, 4] and deleted == [1]
+    v = np.zeros(2)
+    dc.load(2, v)
+    dc.load(2, v)  # same state: no reload
+    assert loads == [2] and list(dc.sectors) == [3, 4, 2]
+    dc.sector(5)
+    dc.sector(6)
+    assert deleted == [1, 3, 4] and list(dc.sectors) == [2, 5, 6]
+    dc.sector(7)  # evicts 2, which held the loaded state
+    assert deleted == [1, 3, 4, 2] and dc.loaded is None
+    dc.load(2, v)
+    assert loads == [2, 2] and made.count(2) == 2
+    dc.close()
+    assert sorted(deleted) == [1, 2, 2, 3, 4, 5, 6, 7] and not dc.sectors

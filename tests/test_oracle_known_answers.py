@@ -244,3 +244,32 @@ def test_energy_terms_add_up_to_e0(hfmode):
             assert abs(eh - (-0.5 * u * 5 if hfmode else 0.0)) < 1e-12
             if u == 0.0:
                 assert epot == eh
+
+
+@pytest.mark.parametrize("phi,nup,ndw", [(0.7, 3, 3), (1.9, 2, 4), (np.pi, 3, 2)])
+def test_complex_flux_ring_free_fermions(phi, nup, ndw):
+    """The oracle's complex H x v (both forms) at U=0 on a 6-site ring threaded by flux phi,
+    Hij(i, i+1) = -e^{i phi/L}: the lowest level of the dense matrix it defines equals the
+    sum of the lowest single-particle energies -2 cos(2 pi m/L + phi/L) (stored form, which
+    keeps conjg(Hij)) and -2 cos(2 pi m/L - phi/L) (direct form, Hij itself): the same set
+    of energies, since the two are the spectra of H and of its complex conjugate."""
+    L = 6
+    H = np.zeros((L, L), complex)
+    for i in range(L):
+        H[i, (i + 1) % L] = -np.exp(1j * phi / L)
+        H[(i + 1) % L, i] = -np.exp(-1j * phi / L)
+    eps = np.sort(np.linalg.eigvalsh(H))
+    ks = 2 * np.pi * np.arange(L) / L
+    assert np.allclose(eps, np.sort(-2 * np.cos(ks + phi / L)), atol=1e-12)
+    exact = eps[:nup].sum() + eps[:ndw].sum()
+    m = O.Model(H, uloc=0.0, xmu=0.0, hfmode=False)
+    D = math.comb(L, nup) * math.comb(L, ndw)
+    st = O.Stored(m, nup, ndw)
+    for matvec in (st.matvec_z, lambda v: O.direct_matvec_z(m, nup, ndw, v)):
+        Hd = np.zeros((D, D), complex)
+        for i in range(D):
+            e = np.zeros(D, complex)
+            e[i] = 1.0
+            Hd[:, i] = matvec(e)
+        assert np.abs(Hd - Hd.conj().T).max() < 1e-13
+        assert abs(np.linalg.eigvalsh(Hd)[0] - exact) < 1e-10
