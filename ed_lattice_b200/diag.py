@@ -213,16 +213,18 @@ def device_solver(model: Model, nup: int, ndw: int, neigen: int, lanc_solve: boo
         sec.delete()
 
 
-def sector_device_bytes(dim: int, neigen: int, lanc_solve: bool, params: DiagParams) -> int:
+def sector_device_bytes(dim: int, neigen: int, lanc_solve: bool, params: DiagParams, cplx: bool = False) -> int:
     """Device memory one sector solve holds at its peak, in bytes: the Lanczos basis of
     edg_lowest_k (min(lanc_niter, dim) vectors) plus its Ritz vectors and work vectors, the
     ground-state vectors of edg_ground_state, or the dense matrix with the eigensolver's
-    copy and workspace. The hop tables of a sector are small beside these."""
+    copy and workspace; twice that for the complex vectors of a complex-Hij model. The hop
+    tables of a sector are small beside these."""
+    w = 16 if cplx else 8
     if not lanc_solve:
-        return 3 * dim * dim * 8 + (1 << 20)
+        return 3 * dim * dim * w + (1 << 20)
     if params.lanc_method == "lanczos":
-        return 8 * dim * 8 + (1 << 20)
-    return (min(params.lanc_niter, dim) + neigen + 4) * dim * 8 + (1 << 20)
+        return 8 * dim * w + (1 << 20)
+    return (min(params.lanc_niter, dim) + neigen + 4) * dim * w + (1 << 20)
 
 
 class SectorScheduler:
@@ -282,12 +284,13 @@ def solve_sectors(model: Model, jobs, params: DiagParams, seed: int, solver=None
         torch.linalg.eigh(torch.ones((1, 1), dtype=torch.float64, device=torch.device("cuda", dev)))
     sched = SectorScheduler(capacity if capacity is not None else _device_capacity())
     ns = model.ns
+    cplx = bool(np.iscomplexobj(model.hij) and np.any(np.imag(model.hij) != 0))
 
     def run(job):
         key, nup, ndw, ne, lz = job
         if on_gpu:
             torch.cuda.set_device(dev)
-        held = sched.acquire(sector_device_bytes(math.comb(ns, nup) * math.comb(ns, ndw), ne, lz, params))
+        held = sched.acquire(sector_device_bytes(math.comb(ns, nup) * math.comb(ns, ndw), ne, lz, params, cplx))
         try:
             return fn(model, nup, ndw, ne, lz, params, seed)
         finally:
