@@ -95,6 +95,37 @@ class _DeviceChains:
         self.sectors.clear()
 
 
+def _device_plan(model: Model, state_list: StateList, threads: int) -> tuple[int, int]:
+    """(threads, sectors cached per thread) for the device builders: each thread keeps at most
+    `keep` sectors of about ten work vectors each, sized by the largest sector a state of the
+    list or a neighbour of it (one electron more or less) can have; thread count and cache
+    shrink until that fits in half of the free HBM."""
+    import math
+
+    ns = model.ns
+    dmax = 1
+    for st in state_list.states:
+        nup, ndw = model.get_nup(st.sector), model.get_ndw(st.sector)
+        for du, dd in ((0, 0), (1, 0), (-1, 0), (0, 1), (0, -1)):
+            a, b = nup + du, ndw + dd
+            if 0 <= a <= ns and 0 <= b <= ns:
+                dmax = max(dmax, math.comb(ns, a) * math.comb(ns, b))
+    cplx = bool(np.iscomplexobj(model.hij) and np.any(np.imag(model.hij) != 0))
+    per_sector = 10 * dmax * (16 if cplx else 8)
+    try:
+        import torch
+
+        free = torch.cuda.mem_get_info()[0] if torch.cuda.is_available() else 1 << 62
+    except Exception:
+        free = 1 << 62
+    keep = 8
+    while keep > 3 and threads * keep * per_sector > free // 2:
+        keep -= 1
+    while threads > 1 and threads * keep * per_sector > free // 2:
+        threads -= 1
+    return threads, keep
+
+
 def _map_states(state_list: StateList, comm, what: str, fn, threads: int, make_ctx=None) -> dict:
     """{istate: fn(istate, state, ctx)} over the states this rank owns. With threads > 1 the
     states are shared out among that many host threads, each with its own ctx = make_ctx()
@@ -170,8 +201,11 @@ def build_gf_electrons(model: Model, state_list: StateList, nlanc: int = LANC_NG
                 out[(ispin, io, jo)] = chans
         return out
 
+    keep = 8
+    if not chain_fn:
+        threads, keep = _device_plan(model, state_list, threads)
     per = _map_states(state_list, comm, "build_gf_electrons", run, threads,
-                      None if chain_fn else (lambda: _DeviceChains(model, precision)))
+                      None if chain_fn else (lambda: _DeviceChains(model, precision, keep)))
     mine = {(ispin, io, jo, istate): chans for istate, res in per.items() for (ispin, io, jo), chans in res.items()}
     gm: dict = {}
     for part in _allgather(mine, comm):
@@ -257,8 +291,11 @@ def build_chi(model: Model, state_list: StateList, kind: int = 0, nlanc: int = L
                 res[io] = [chi_chain(sec, io, min(nlanc, sec.dim), st.e, kind=kind, precision=precision)]
         return res
 
+    keep = 8
+    if not chain_fn:
+        threads, keep = _device_plan(model, state_list, threads)
     per = _per_state(state_list, comm, "build_chi", run, threads,
-                     None if chain_fn else (lambda: _DeviceChains(model, precision)))
+                     None if chain_fn else (lambda: _DeviceChains(model, precision, keep)))
     return {io: [per[k][io] for k in range(state_list.size)] for io in range(1, model.ns + 1)}
 
 
@@ -306,8 +343,11 @@ def build_oc(model: Model, state_list: StateList, nlanc: int = LANC_NGFITER, pre
         sec = dev.load(st.sector, st.vec)
         return [oc_chain(sec, min(nlanc, sec.dim), st.e, precision=precision)]
 
+    keep = 8
+    if not chain_fn:
+        threads, keep = _device_plan(model, state_list, threads)
     return _per_state(state_list, comm, "build_oc", run, threads,
-                      None if chain_fn else (lambda: _DeviceChains(model, precision)))
+                      None if chain_fn else (lambda: _DeviceChains(model, precision, keep)))
 
 
 def eval_oc_electrons(ocmatrix: list, state_list: StateList, zeta: float, temp: float, finite_temp: bool,

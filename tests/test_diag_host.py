@@ -440,3 +440,23 @@ def test_device_chain_cache_eviction(monkeypatch):
     assert loads == [2, 2] and made.count(2) == 2
     dc.close()
     assert sorted(deleted) == [1, 2, 2, 3, 4, 5, 6, 7] and not dc.sectors
+
+
+def test_device_plan_shrinks_with_sector_size(monkeypatch):
+    """gf._device_plan: small sectors keep 4 threads and 8 cached sectors; sectors whose work
+    vectors would overrun half the free memory get fewer threads and a smaller cache."""
+    import types
+
+    from ed_lattice_b200 import gf
+
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(is_available=lambda: True,
+                                                                  mem_get_info=lambda: (100 << 30, 180 << 30)))
+    monkeypatch.setitem(__import__("sys").modules, "torch", fake_torch)
+    small = E.Model(E.square_lattice(3, 4), uloc=4.0)
+    sl = StateList()
+    sl.add_state(-1.0, np.zeros(1), small.get_sector(6, 6), size=10)
+    assert gf._device_plan(small, sl, 4) == (4, 8)
+    big = E.Model(E.square_lattice(4, 4), uloc=4.0)  # neighbours of (8,8): D up to 165,636,900
+    sl2 = StateList()
+    sl2.add_state(-1.0, np.zeros(1), big.get_sector(8, 8), size=10)
+    assert gf._device_plan(big, sl2, 4) == (1, 3)  # 3 sectors of 13.25 GB fit in 50 GB, 6 do not
