@@ -296,6 +296,13 @@ class Sector:
         return dict(zip(("ekin", "epot", "eknot", "ehartree"), (x.value for x in out)))
 
 
+def release_cached_memory() -> None:
+    """Hand the device memory the library keeps for reuse between sectors (up to a quarter of
+    the current device's memory) back to the driver, e.g. before a large torch workload in the
+    same process."""
+    L.check(L.lib().edg_release_cached_memory(), "edg_release_cached_memory")
+
+
 # ----------------------------------------------------------------------------- Lanczos
 def random_vector(seed: int, n: int) -> np.ndarray:
     out = np.empty(n)
