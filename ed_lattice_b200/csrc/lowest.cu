@@ -26,44 +26,14 @@ constexpr int kMaxK = 16;         // eigenpairs per call
 constexpr int kLkThreads = 256;
 constexpr int kDenseMaxDim = 16384;  // 2 GB dense matrix
 
-// partial[j * nsplit + s] = sum over element stream s of Q[j][i] * w[i], j < m. blockIdx.y
-// takes a group of G columns and stream s = blockIdx.x * 8 + warp a contiguous run of
-// elements, so every warp streams G + 1 long coalesced rows; the grid spans all column
-// groups at once (about 7 blocks per SM). On the 853,776-state sector this reads the basis
-// at 5.8-6.2 TB/s for 112-224 columns, where one element chunk per block with the column
-// groups shared out among its warps reached 3.3 TB/s. Fixed summation order.
-template <int G>
-__global__ void __launch_bounds__(kLkThreads) k_multidot(const double* __restrict__ Q, int m, int64_t n,
-                                                         const double* __restrict__ w, double* __restrict__ partial) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nsplit = gridDim.x * (kLkThreads / 32);
-  const int split = blockIdx.x * (kLkThreads / 32) + warp;
-  int64_t chunk = (n + nsplit - 1) / nsplit;
-  chunk = (chunk + 31) & ~int64_t(31);
-  const int64_t i0 = split * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
-  const int j0 = blockIdx.y * G;
-  const double* __restrict__ q[G];
-#pragma unroll
-  for (int c = 0; c < G; ++c) q[c] = Q + int64_t(j0 + c < m ? j0 + c : m - 1) * n;  // tail repeats column m-1
-  double acc[G];
-#pragma unroll
-  for (int c = 0; c < G; ++c) acc[c] = 0.0;
-#pragma unroll 2
-  for (int64_t i = i0 + lane; i < i1; i += 32) {
-    const double wi = w[i];
-#pragma unroll
-    for (int c = 0; c < G; ++c) acc[c] = __fma_rn(q[c][i], wi, acc[c]);
-  }
-#pragma unroll
-  for (int c = 0; c < G; ++c) {
-    double t = acc[c];
-    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-    if (lane == 0 && j0 + c < m) partial[int64_t(j0 + c) * nsplit + split] = t;
-  }
-}
-
-// Two right-hand sides in one read of the basis: partial[j * nsplit + s] for Q[j] . w and
-// partial[(m + j) * nsplit + s] for Q[j] . x, j < m (same streams and order as k_multidot).
+// Two right-hand sides in one read of the basis: partial[j * nsplit + s] = sum over element
+// stream s of Q[j][i] * w[i], and partial[(m + j) * nsplit + s] the same for x, j < m.
+// blockIdx.y takes a group of G columns and stream s = blockIdx.x * 8 + warp a contiguous run
+// of elements, so every warp streams G + 2 long coalesced rows; the grid spans all column
+// groups at once (about 7 blocks per SM). On the 853,776-state sector this shape reads the
+// basis at 5.8-6.2 TB/s for 112-224 columns (one right-hand side), where one element chunk
+// per block with the column groups shared out among its warps reached 3.3 TB/s. Fixed
+// summation order.
 template <int G>
 __global__ void __launch_bounds__(kLkThreads) k_multidot2(const double* __restrict__ Q, int m, int64_t n,
                                                           const double* __restrict__ w, const double* __restrict__ x,
@@ -152,20 +122,6 @@ DotShape dot_shape(int m, int64_t n) {
   return d;
 }
 
-int launch_multidot2(const double* Q, int m, int64_t n, const double* w, const double* x, double* partial,
-                     cudaStream_t st, int* nsplit);
-
-int launch_multidot(const double* Q, int m, int64_t n, const double* w, double* partial, cudaStream_t st,
-                    int* nsplit) {
-  const DotShape d = dot_shape(m, n);
-  const dim3 grid(d.gx, (m + d.G - 1) / d.G);
-  if (d.G == 8)
-    k_multidot<8><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, partial);
-  else
-    k_multidot<4><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, partial);
-  *nsplit = d.nsplit();
-  return EDG_OK;
-}
 
 int launch_multidot2(const double* Q, int m, int64_t n, const double* w, const double* x, double* partial,
                      cudaStream_t st, int* nsplit) {
