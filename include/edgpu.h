@@ -166,7 +166,8 @@ int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64);
 /* Lowest k (1..16) eigenpairs of a sector: the sp_eigh (ARPACK) branch of ed_diag_d,
  * Neigen = min(dim, lanc_nstates_sector) states per sector for the finite-temperature state
  * list (src/DIAG/DIAG.f90:144-146,191-202). FP64 Lanczos with full reorthogonalisation
- * (Gram-Schmidt twice per step) against a basis of at most min(maxit, 1024) device
+ * (classical Gram-Schmidt with its second pass from the Gram matrix of the basis; applied
+ * twice for complex vectors) against a basis of at most min(maxit, 1024) device
  * vectors (fewer if HBM is short); stops when every one of the k lowest Ritz pairs has
  * residual b_{m+1}|z_{m,i}| <= tol*max(1,|theta_i|), or the Krylov space becomes invariant,
  * or the basis is full. evals[k] ascending (NaN beyond dim); evecs (host, may be NULL):
