@@ -330,7 +330,7 @@ def test_threaded_sector_solves_match_sequential_and_respect_capacity():
             state["held"] += b
             state["peak"] = max(state["peak"], state["held"])
             state["starts"].append(math.comb(4, nup) * math.comb(4, ndw))
-        time.sleep(0.01)
+        time.sleep(0.05)  # long enough that the four workers start their first jobs first
         try:
             return base(model, nup, ndw, neigen, lanc_solve, params, seed)
         finally:
