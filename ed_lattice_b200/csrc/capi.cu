@@ -100,13 +100,6 @@ int check_vec_align(const edg_sector_s* s, const void* p, const char* what) {
   return EDG_OK;
 }
 
-int ensure_device(const edg_sector_s* s) {
-  int cur = -1;
-  EDG_CUDA(cudaGetDevice(&cur));
-  if (cur != s->device) EDG_CUDA(cudaSetDevice(s->device));
-  return EDG_OK;
-}
-
 }  // namespace
 
 extern "C" {
@@ -228,7 +221,8 @@ int edg_sector_create(const edg_model* m, int nup, int ndw, int form, edg_sector
 
 int edg_sector_destroy(edg_sector* s) {
   if (!s) return EDG_OK;
-  cudaSetDevice(s->device);
+  DeviceGuard dg;
+  (void)dg.enter(s->device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   cudaStream_t st = s->stream;
   bool own = s->own_stream;
@@ -261,7 +255,7 @@ int edg_sector_dims(const edg_sector* s, int64_t* dim, int64_t* dimup, int64_t* 
 
 int edg_sector_get_maps(const edg_sector* s, int32_t* map_up, int32_t* map_dw) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   cudaStream_t st = s->stream;
   if (map_up)
     EDG_CUDA(cudaMemcpyAsync(map_up, s->up.map.p, s->up.dim * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -278,7 +272,7 @@ int edg_sector_get_hops(const edg_sector* s, int spin, int64_t* rowptr, int32_t*
     set_error("edg_sector_get_hops: the direct form keeps no tables");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   const SpinBasis& B = spin == 1 ? s->up : s->dw;
   if (nnz) *nnz = B.nnz;
   cudaStream_t st = s->stream;
@@ -296,7 +290,7 @@ int edg_sector_get_hops(const edg_sector* s, int spin, int64_t* rowptr, int32_t*
 
 int edg_sector_set_stream(edg_sector* s, void* stream) {
   EDG_CHECK(check_sector(s));
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   if (s->stream) EDG_CUDA(cudaStreamSynchronize(s->stream));
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   s->stream = static_cast<cudaStream_t>(stream);
@@ -309,7 +303,7 @@ int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv) {
   EDG_ARG(dv && dhv && dv != dhv, "edg_hxv_dev_f64: bad vectors");
   EDG_CHECK(check_vec_align<double>(s, dv, "edg_hxv_dev_f64"));
   EDG_CHECK(check_vec_align<double>(s, dhv, "edg_hxv_dev_f64"));
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return hxv_apply<double>(s, dv, dhv);
 }
 
@@ -318,7 +312,7 @@ int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv) {
   EDG_ARG(dv && dhv && dv != dhv, "edg_hxv_dev_f32: bad vectors");
   EDG_CHECK(check_vec_align<float>(s, dv, "edg_hxv_dev_f32"));
   EDG_CHECK(check_vec_align<float>(s, dhv, "edg_hxv_dev_f32"));
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return hxv_apply<float>(s, dv, dhv);
 }
 
@@ -331,7 +325,7 @@ int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv) {
   }
   EDG_ARG(nloc == s->dim, "directMatVec ERROR: Nloc != dim(isector) (%lld vs %lld)", (long long)nloc,
           (long long)s->dim);
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   const int64_t n = s->dim;
   EDG_CHECK(s->w64[0].alloc(n, s->stream, "H x v input"));
   EDG_CHECK(s->w64[1].alloc(n, s->stream, "H x v output"));
@@ -347,7 +341,7 @@ int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv) {
   EDG_ARG(v && hv, "edg_hxv_z: NULL vector");
   EDG_ARG(nloc == s->dim, "directMatVec ERROR: Nloc != dim(isector) (%lld vs %lld)", (long long)nloc,
           (long long)s->dim);
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   const int64_t n = s->dim;
   if (s->cplx) {  // complex H x v straight on the interleaved vector
     EDG_CHECK(s->w64[0].alloc(2 * n, s->stream, "H x v input"));
@@ -380,7 +374,7 @@ int edg_tridiag_dev_f64(edg_sector* s, const double* dvinit, int nlanc, double t
   EDG_ARG(nlanc >= 0, "edg_tridiag: nlanc=%d", nlanc);
   EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_tridiag: precision=%d", precision);
   EDG_CHECK(check_vec_align<double>(s, dvinit, "edg_tridiag_dev_f64"));
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return tridiag_dev(s, dvinit, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
 }
 
@@ -388,7 +382,7 @@ int edg_tridiag_d(edg_sector* s, const double* vvinit, int nlanc, double thresho
                   double* blanc, double* norm2, int* nsteps) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(vvinit, "edg_tridiag_d: NULL start vector");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   EDG_CHECK(s->w64[3].alloc(s->vlen, s->stream, "start vector"));
   EDG_CUDA(cudaMemcpyAsync(s->w64[3].p, vvinit, s->vlen * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   return edg_tridiag_dev_f64(s, s->w64[3].p, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
@@ -400,7 +394,7 @@ int edg_ground_state_keep(edg_sector* s, const double* v0, uint64_t seed, int ma
   EDG_ARG(e0 && niter, "edg_ground_state: NULL output");
   EDG_ARG((mode & 0xff) == EDG_GS_F64 || (mode & 0xff) == EDG_GS_F32_REFINE, "edg_ground_state: mode=%d", mode);
   EDG_ARG(tol >= 0.0, "edg_ground_state: tol < 0");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return ground_state(s, v0, seed, maxit, tol, mode, e0, niter);
 }
 
@@ -418,21 +412,21 @@ int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxi
   EDG_ARG(k >= 1 && k <= 16, "edg_lowest_k: k=%d outside 1..16", k);
   EDG_ARG(maxit >= 1, "edg_lowest_k: maxit=%d", maxit);
   EDG_ARG(tol > 0.0 && std::isfinite(tol), "edg_lowest_k: tol must be > 0");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return lowest_k(s, k, v0, seed, maxit, tol, evals, evecs, resid, niter);
 }
 
 int edg_sector_dense(edg_sector* s, double* h) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(h, "edg_sector_dense: NULL");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return sector_dense(s, h);
 }
 
 int edg_sector_dense_dev(edg_sector* s, double* dh) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(dh, "edg_sector_dense_dev: NULL");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return sector_dense_dev(s, dh);
 }
 
@@ -450,7 +444,7 @@ int edg_state_get(const edg_sector* s, double* evec) {
     set_error("edg_state_get: the sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   EDG_CUDA(cudaMemcpyAsync(evec, s->state.p, s->vlen * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   EDG_CUDA(cudaStreamSynchronize(s->stream));
   return EDG_OK;
@@ -459,7 +453,7 @@ int edg_state_get(const edg_sector* s, double* evec) {
 int edg_state_set(edg_sector* s, const double* evec) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(evec, "edg_state_set: NULL");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   EDG_CHECK(s->state.alloc(s->vlen, s->stream, "state"));
   EDG_CUDA(cudaMemcpyAsync(s->state.p, evec, s->vlen * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   EDG_CUDA(cudaStreamSynchronize(s->stream));
@@ -489,7 +483,7 @@ int edg_apply_cop_dev_f64(const edg_sector* from, const edg_sector* to, int op, 
   const int nupJ = from->nup + (spin == 1 ? op : 0), ndwJ = from->ndw + (spin == 2 ? op : 0);
   EDG_ARG(to->nup == nupJ && to->ndw == ndwJ, "edg_apply_cop: target sector (%d,%d) is not (%d,%d)", to->nup, to->ndw,
           nupJ, ndwJ);
-  EDG_CHECK(ensure_device(to));
+  EDG_ON_DEVICE(to->device);
   return apply_cop(from, to, op, site, spin, coef, accumulate, din, dout, to->stream);
 }
 
@@ -508,14 +502,14 @@ int edg_apply_diagop_dev_f64(const edg_sector* s, int kind, int site, int site2,
     w[site - 1] += 1.0;
     if (site2 > 0) w[site2 - 1] += 1.0;
   }
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return apply_diagop(s, kind, w.data(), din, dout, s->stream);
 }
 
 int edg_apply_current_dev_f64(const edg_sector* s, const double* din, double* dout) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(din && dout && din != dout, "edg_apply_current: bad vectors");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return apply_current(s, din, dout, s->stream);
 }
 
@@ -526,7 +520,7 @@ int edg_energy(edg_sector* s, double weight, double* ekin, double* epot, double*
     return EDG_ERR_STATE;
   }
   EDG_ARG(std::isfinite(weight), "edg_energy: weight is not finite");
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return energy(s, s->state.p, weight, ekin, epot, eknot, ehartree);
 }
 
@@ -537,7 +531,7 @@ int edg_observables(const edg_sector* s, double weight, double* dens, double* de
     set_error("edg_observables: the sector holds no state");
     return EDG_ERR_STATE;
   }
-  EDG_CHECK(ensure_device(s));
+  EDG_ON_DEVICE(s->device);
   return observables(s, s->state.p, weight, dens, dens_up, dens_dw, docc, magz, s->stream);
 }
 
@@ -583,6 +577,7 @@ int edg_gf_chain(const edg_sector* from, edg_sector* to, int op, int site, int s
     set_error("edg_gf_chain: origin sector holds no state");
     return EDG_ERR_STATE;
   }
+  EDG_ON_DEVICE(to->device);
   EDG_CHECK(to->w64[3].alloc(to->vlen, to->stream, "excitation vector"));
   EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, site, spin, 1.0, 0, from->state.p, to->w64[3].p));
   if (site2 > 0)
@@ -598,6 +593,7 @@ int edg_chi_chain(edg_sector* s, int kind, int site, int site2, const double* qc
     set_error("edg_chi_chain: sector holds no state");
     return EDG_ERR_STATE;
   }
+  EDG_ON_DEVICE(s->device);
   EDG_CHECK(s->w64[3].alloc(s->vlen, s->stream, "excitation vector"));
   EDG_CHECK(edg_apply_diagop_dev_f64(s, kind, site, site2, qcos, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);
@@ -611,6 +607,7 @@ int edg_oc_chain(edg_sector* s, int nlanc, int precision, double ei, double* pol
     set_error("edg_oc_chain: sector holds no state");
     return EDG_ERR_STATE;
   }
+  EDG_ON_DEVICE(s->device);
   EDG_CHECK(s->w64[3].alloc(s->vlen, s->stream, "excitation vector"));
   EDG_CHECK(edg_apply_current_dev_f64(s, s->state.p, s->w64[3].p));
   return finish_chain(s, s->w64[3].p, nlanc, precision, ei, 1, poles, weights, norm2, nout);

@@ -34,6 +34,35 @@ const char* get_error();
     if (s_ != EDG_OK) return s_; \
   } while (0)
 
+// Makes a sector's device current for the rest of the enclosing scope and gives the caller
+// back its own current device on every return path: a host code that drives several GPUs
+// from one thread must find its current device unchanged after any library call.
+struct DeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  DeviceGuard() = default;
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+  int enter(int dev) {
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e == cudaSuccess && prev != dev) {
+      e = cudaSetDevice(dev);
+      switched = e == cudaSuccess;
+    }
+    if (e != cudaSuccess) {
+      set_error("selecting device %d: %s", dev, cudaGetErrorString(e));
+      return EDG_ERR_CUDA;
+    }
+    return EDG_OK;
+  }
+  ~DeviceGuard() {
+    if (switched) cudaSetDevice(prev);
+  }
+};
+#define EDG_ON_DEVICE(dev)           \
+  ::edg::DeviceGuard edg_dev_guard_; \
+  EDG_CHECK(edg_dev_guard_.enter(dev))
+
 // Stream-ordered buffers from a per-device pool that keeps freed memory for reuse; freed on
 // the same stream when the owner goes out of scope. Every device buffer of the library comes
 // from this pool: on a machine whose driver is busy with other processes, a plain

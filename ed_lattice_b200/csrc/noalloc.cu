@@ -10,8 +10,9 @@
 // __device__ array of fixed size, so the call itself allocates nothing.
 //
 // Limits and sharing:
-//  - sector dimension <= kNoAllocMaxDim (2^20 states) and nlanc <= kNoAllocMaxLanc (1024);
-//    larger requests return EDG_ERR_ARG. The array is 3*2^20 + 4096 doubles (about 25 MB)
+//  - vector length (the sector dimension, or twice it for a complex sector, whose vectors
+//    hold (re, im) pairs) <= kNoAllocMaxDim (2^20 reals) and nlanc <= kNoAllocMaxLanc
+//    (1024); larger requests return EDG_ERR_ARG. The array is 3*2^20 + 4096 doubles (about 25 MB)
 //    and every GPU that loads the library holds it until the process exits.
 //  - every call on a device uses the same array, which keeps the previous call's contents;
 //    the call clears what must start at zero. Two calls that overlap on the GPU (two host
@@ -75,9 +76,11 @@ extern "C" int edg_tridiag_dev_f64_noalloc(edg_sector* s, const double* dvinit, 
               (long long)kNoAllocMaxDim, nlanc, kNoAllocMaxLanc);
     return EDG_ERR_ARG;
   }
-  int cur = -1;
-  EDG_CUDA(cudaGetDevice(&cur));
-  if (cur != s->device) EDG_CUDA(cudaSetDevice(s->device));
+  if (s->cplx && reinterpret_cast<uintptr_t>(dvinit) % (2 * sizeof(double)) != 0) {
+    set_error("edg_tridiag_dev_f64_noalloc: complex vectors must be 16-byte aligned");
+    return EDG_ERR_ARG;
+  }
+  EDG_ON_DEVICE(s->device);
   double* base = nullptr;
   EDG_CHECK(scratch_ptr(s->device, &base));
   const int64_t n = s->vlen;

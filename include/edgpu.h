@@ -138,8 +138,9 @@ int edg_tridiag_dev_f64(edg_sector* s, const double* dvinit, int nlanc, double t
  * host code whose device memory is owned by another runtime's pool or arena, or a loop that
  * must never wait on the allocator. All scratch (three Lanczos vectors, reduction partials,
  * scalar slots) lives in one file-scope device array of about 25 MB that every GPU loading
- * the library holds until exit; the call allocates nothing. Limits: sector dimension <=
- * 2^20 and nlanc <= 1024, else EDG_ERR_ARG. Calls share that array (it keeps the previous
+ * the library holds until exit; the call allocates nothing. Limits: vector length (the
+ * sector dimension, 2*dim for a complex sector) <= 2^20 and nlanc <= 1024, else
+ * EDG_ERR_ARG; a complex start vector must be 16-byte aligned. Calls share that array (it keeps the previous
  * call's contents; the call clears what must start at zero), so calls that overlap on the
  * GPU race and must be serialised by the caller. The first call on a device looks up the
  * array's address (cudaGetSymbolAddress) and should come before any stream capture. */
