@@ -36,6 +36,10 @@ LX, LY, U, NUP, NDW = 4, 4, 8.0, 8, 8
 WORKLOAD = "hubbard_4x4_U8_half_filling_sector(8,8)_D165636900"
 METRIC = "hxv_algorithmic_GBps"
 UNIT = "GB/s"
+# DRAM read + write of the kernels of one FP32 H x v of this sector (dram__bytes_read.sum +
+# dram__bytes_write.sum over the launches of one H x v), a constant taken from an ncu capture
+TRAFFIC_GB = 3.233
+TRAFFIC_SOURCE = "ncu, constant from a capture of the same H x v (not measured in this run)"
 
 
 def peaks():
@@ -115,40 +119,48 @@ def dist_env():
     return ws, rank, local
 
 
-def cpu_baseline_sample(target_seconds: float = 12.0):
-    """The oracle's stored-form spMatVec (FP64, OpenMP on all host threads) on the 4x4 half-filled sector,
-    timed on a bounded sample of output rows. Returns (GB/s in the metric's unit, info)."""
-    from ed_lattice_b200.edlat import square_lattice
+CPU_LOOP_ORDER = ("the reference's spMatVec loop order (src/DIAG/HAMILTONIAN_STORED_HxV.f90:159-220): "
+                  "diagonal sweep, then the DW sweep with iup outer and stride-DimUp access, then the UP sweep")
+
+
+def _oracle_sector():
+    """The oracle's stored form of the benchmarked sector. Imports only the oracle (test
+    infrastructure, CPU): the reference arm and the CPU baseline load none of the engine."""
     from oracle import oracle as O
-    m = O.Model(square_lattice(LX, LY), uloc=U, xmu=U / 2, hfmode=False)
-    st = O.Stored(m, NUP, NDW)
+    m = O.Model(O.square_lattice(LX, LY), uloc=U, xmu=U / 2, hfmode=False)
+    return O, O.Stored(m, NUP, NDW)
+
+
+def cpu_baseline_sample(target_seconds: float = 12.0):
+    """The oracle's stored-form spMatVec (FP64, OpenMP on all host threads, the reference's
+    three-sweep loop order) on the 4x4 half-filled sector, timed on a bounded sample of
+    output rows. Returns (GB/s in the metric's unit, info)."""
+    O, st = _oracle_sector()
     D, ddw = st.dim, st.dimdw
     v = O.random_vector(7, D)
     hv = np.zeros(D)
     rows = max(1, ddw // 256)
     t0 = time.perf_counter()
-    st.matvec_rows_d(v, hv, 0, rows)
+    st.matvec_sweeps_d(v, hv, 0, rows)
     t1 = time.perf_counter()
     per_row = (t1 - t0) / rows
     rows = int(min(ddw, max(rows, target_seconds / max(per_row, 1e-9))))
     t0 = time.perf_counter()
-    st.matvec_rows_d(v, hv, 0, rows)
+    st.matvec_sweeps_d(v, hv, 0, rows)
     dt = time.perf_counter() - t0
     frac = rows / ddw
     hxv_per_s = frac / dt
     return hxv_per_s * 2 * D * 4 / 1e9, {"cores": O.num_threads(), "kind": "port",
                                         "sample": f"stored spMatVec FP64 restatement, output rows 0..{rows} of "
-                                                  f"{ddw} ({frac:.3%} of one H x v, {dt:.1f} s)"}
+                                                  f"{ddw} ({frac:.3%} of one H x v, {dt:.1f} s)",
+                                        "loop_order": CPU_LOOP_ORDER}
 
 
 def run_reference(args):
     ws, rank, local = dist_env()
     if rank != 0:
         return 0
-    from ed_lattice_b200.edlat import square_lattice
-    from oracle import oracle as O
-    m = O.Model(square_lattice(LX, LY), uloc=U, xmu=U / 2, hfmode=False)
-    st = O.Stored(m, NUP, NDW)
+    O, st = _oracle_sector()
     D, ddw = st.dim, st.dimdw
     v = O.random_vector(7, D)
     hv = np.zeros(D)
@@ -157,14 +169,14 @@ def run_reference(args):
     budget = 150.0 / max(1, args.steps + args.warmup)
     rows = max(1, ddw // 512)
     t0 = time.perf_counter()
-    st.matvec_rows_d(v, hv, 0, rows)
+    st.matvec_sweeps_d(v, hv, 0, rows)
     per_row = (time.perf_counter() - t0) / rows
     rows = int(min(ddw, max(1, budget / max(per_row, 1e-9))))
     for _ in range(args.warmup):
-        st.matvec_rows_d(v, hv, 0, rows)
+        st.matvec_sweeps_d(v, hv, 0, rows)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        st.matvec_rows_d(v, hv, 0, rows)
+        st.matvec_sweeps_d(v, hv, 0, rows)
     dt = time.perf_counter() - t0
     hxv_per_s = args.steps * (rows / ddw) / dt
     val = hxv_per_s * 2 * D * 4 / 1e9
@@ -175,7 +187,8 @@ def run_reference(args):
                        "rows_total": ddw},
             "cpu_baseline": {"value": round(val, 4), "unit": UNIT, "cores": O.num_threads(), "kind": "port",
                              "sample": f"output rows 0..{rows} of {ddw} per step (FP64 stored-form restatement; "
-                                       "reference Fortran/SciFortran not buildable here)"},
+                                       "reference Fortran/SciFortran not buildable here)",
+                             "loop_order": CPU_LOOP_ORDER},
             "e2e": {"value": round(val, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -204,6 +217,20 @@ def e0_time_to_solution(E, L, sector, seed=2024, maxit=600):
         out[name] = {"seconds": statistics.median(times), "runs": times, "hxv_applications": it,
                      "hxv_f32": n32.value, "hxv_f64": n64.value, "e0": e0, "rel_err": abs(e0 - e_ref) / abs(e_ref)}
     out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
+    # the vector the FP32+refine path returns (untimed run with the vector kept): its norm,
+    # Rayleigh quotient and residual |H x - E0 x| with one FP64 H x v
+    e0, x, _ = E.sp_lanc_eigh(sector, seed=seed, maxit=maxit, tol=1e-8, mode=E.EDG_GS_F32_REFINE, want_vector=True)
+    xd = torch.from_numpy(x).cuda()
+    hx = torch.empty_like(xd)
+    torch.cuda.synchronize()
+    L.check(L.lib().edg_hxv_dev_f64(sector.handle, C.c_void_p(xd.data_ptr()), C.c_void_p(hx.data_ptr())), "hxv")
+    torch.cuda.synchronize()
+    nrm = float(torch.linalg.vector_norm(xd).item())
+    out["fp32_refine"]["vector"] = {"norm": nrm, "rayleigh_rel_err": abs(float(torch.dot(xd, hx).item()) / nrm ** 2
+                                                                         - e_ref) / abs(e_ref),
+                                    "residual": float(torch.linalg.vector_norm(hx - e0 * xd).item())}
+    del xd, hx
+    torch.cuda.empty_cache()
     return out
 
 
@@ -448,9 +475,8 @@ def run_ours(args):
                          "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_launch_ms,
-                         # DRAM read+write of both kernels of one H x v, GB, from the ncu capture
-                         # summarised in profiles/hxv_f32_hubbard4x4_U8_sector88.md
-                         "traffic": 3.233},
+                         "traffic": TRAFFIC_GB, "traffic_unit": "GB per H x v",
+                         "traffic_source": TRAFFIC_SOURCE},
             "clocks": clk.summary(),
             "gpu_launches": 2 * args.steps,
             "e2e": e2e,

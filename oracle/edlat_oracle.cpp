@@ -345,14 +345,17 @@ int64_t orc_stored_dim(const orc_stored* st) { return st->S.dim; }
 // every output element keeps the serial summation order.
 }  // extern "C"
 
+// The three sweeps restricted to output rows idw in [row_lo,row_hi) (the whole operator for
+// [0,DimDw)): the reference's loop order, with its stride-DimUp DW sweep, so that a bounded
+// sample of rows times the reference's memory-access pattern.
 template <typename T>
-void stored_matvec(const orc_stored* st, const T* v, T* hv) {
-  const int64_t DimUp = st->S.dimup, DimDw = st->S.dimdw, Nloc = st->S.dim;
+void stored_matvec_sweeps(const orc_stored* st, const T* v, T* hv, int64_t row_lo, int64_t row_hi) {
+  const int64_t DimUp = st->S.dimup;
 #pragma omp parallel for schedule(static)
-  for (int64_t i = 0; i < Nloc; ++i) hv[i] = st->d[i] * v[i];
+  for (int64_t i = row_lo * DimUp; i < row_hi * DimUp; ++i) hv[i] = st->d[i] * v[i];
 #pragma omp parallel for schedule(static)
   for (int64_t iup = 0; iup < DimUp; ++iup)
-    for (int64_t idw = 0; idw < DimDw; ++idw) {
+    for (int64_t idw = row_lo; idw < row_hi; ++idw) {
       const int64_t i = iup + idw * DimUp;
       T acc = hv[i];
       for (int64_t jj = st->dw_ptr[idw]; jj < st->dw_ptr[idw + 1]; ++jj) {
@@ -363,7 +366,7 @@ void stored_matvec(const orc_stored* st, const T* v, T* hv) {
       hv[i] = acc;
     }
 #pragma omp parallel for schedule(static)
-  for (int64_t idw = 0; idw < DimDw; ++idw)
+  for (int64_t idw = row_lo; idw < row_hi; ++idw)
     for (int64_t iup = 0; iup < DimUp; ++iup) {
       const int64_t i = iup + idw * DimUp;
       T acc = hv[i];
@@ -374,6 +377,10 @@ void stored_matvec(const orc_stored* st, const T* v, T* hv) {
       }
       hv[i] = acc;
     }
+}
+template <typename T>
+void stored_matvec(const orc_stored* st, const T* v, T* hv) {
+  stored_matvec_sweeps<T>(st, v, hv, 0, st->S.dimdw);
 }
 // The same arithmetic restricted to output rows idw in [row_lo,row_hi): a bounded sample of
 // spMatVec for the CPU baseline. Each output element is computed exactly as above.
@@ -398,6 +405,12 @@ void orc_stored_matvec_rows_d(const orc_stored* st, const double* v, double* hv,
   if (row_lo < 0) row_lo = 0;
   if (row_hi > st->S.dimdw) row_hi = st->S.dimdw;
   stored_matvec_rows(st, v, hv, row_lo, row_hi);
+}
+// Output rows [row_lo,row_hi) in the reference's three-sweep order (CPU baseline).
+void orc_stored_matvec_sweeps_d(const orc_stored* st, const double* v, double* hv, int64_t row_lo, int64_t row_hi) {
+  if (row_lo < 0) row_lo = 0;
+  if (row_hi > st->S.dimdw) row_hi = st->S.dimdw;
+  if (row_hi > row_lo) stored_matvec_sweeps<double>(st, v, hv, row_lo, row_hi);
 }
 int64_t orc_stored_dimdw(const orc_stored* st) { return st->S.dimdw; }
 
@@ -601,29 +614,41 @@ int orc_tridiag_d(const orc_stored* st, const double* vvinit, int nlanc, double 
 // Ground-state Lanczos (contract of sp_lanc_eigh, src/DIAG/DIAG.f90:212-217): run the
 // recurrence from the normalised start vector, after each step diagonalise T_j, stop when
 // |E0(j)-E0(j-1)| <= tol*|E0(j)| or b_{j+1} < 1e-14 or j == maxit; the eigenvector is the
-// Ritz vector sum_j Z(j,1) v_j, normalised. Returns the number of steps.
+// Ritz vector sum_j Z(j,1) v_j, normalised. Returns the number of steps. The basis is kept
+// only when evec is requested (E0-only runs of sectors with 1e8+ states keep three vectors);
+// the vector loops run on all host threads with a static schedule, so a run is reproducible
+// for a given thread count.
+namespace {
+double par_dot(const double* x, const double* y, int64_t n) {
+  double s = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : s)
+  for (int64_t i = 0; i < n; ++i) s += x[i] * y[i];
+  return s;
+}
+}  // namespace
+
 int orc_lanczos_gs_d(const orc_stored* st, const double* v0, int maxit, double tol, double* e0, double* evec,
                      double* alanc, double* blanc) {
   const int64_t D = st->S.dim;
   std::vector<double> v(v0, v0 + D);
-  double n2 = 0.0;
-  for (auto x : v) n2 += x * x;
-  for (auto& x : v) x /= std::sqrt(n2);
+  const double nv = std::sqrt(par_dot(v.data(), v.data(), D));
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < D; ++i) v[i] /= nv;
   std::vector<double> vprev(D, 0.0), w(D);
   std::vector<std::vector<double>> basis;
   std::vector<double> a, b(1, 0.0);
   double eold = 0.0, enew = 0.0;
   int it = 0;
   for (it = 0; it < maxit; ++it) {
-    basis.push_back(v);
+    if (evec) basis.push_back(v);
     orc_stored_matvec_d(st, v.data(), w.data());
-    for (int64_t i = 0; i < D; ++i) w[i] -= b.back() * vprev[i];
-    double ai = 0.0;
-    for (int64_t i = 0; i < D; ++i) ai += v[i] * w[i];
+    const double bj = b.back();
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < D; ++i) w[i] -= bj * vprev[i];
+    const double ai = par_dot(v.data(), w.data(), D);
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < D; ++i) w[i] -= ai * v[i];
-    double bn = 0.0;
-    for (int64_t i = 0; i < D; ++i) bn += w[i] * w[i];
-    bn = std::sqrt(bn);
+    const double bn = std::sqrt(par_dot(w.data(), w.data(), D));
     a.push_back(ai);
     const int m = (int)a.size();
     std::vector<double> ev(m);
@@ -633,6 +658,7 @@ int orc_lanczos_gs_d(const orc_stored* st, const double* v0, int maxit, double t
     eold = enew;
     b.push_back(bn);
     if (conv) { ++it; break; }
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < D; ++i) { vprev[i] = v[i]; v[i] = w[i] / bn; }
   }
   const int m = (int)a.size();

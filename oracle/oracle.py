@@ -50,6 +50,7 @@ _SIG = {
     "orc_stored_matvec_z": (None, [_p, _p, _p]),
     "orc_stored_matvec_d": (None, [_p, _p, _p]),
     "orc_stored_matvec_rows_d": (None, [_p, _p, _p, _i64, _i64]),
+    "orc_stored_matvec_sweeps_d": (None, [_p, _p, _p, _i64, _i64]),
     "orc_stored_dimdw": (_i64, [_p]),
     "orc_dense_h": (None, [_p, _i, _i, _p]),
     "orc_tridiag_eigh": (None, [_i, _p, _p, _p, _p]),
@@ -175,6 +176,11 @@ class Stored:
         """Output rows idw in [row_lo,row_hi) of spMatVec (bounded CPU-baseline sample)."""
         lib().orc_stored_matvec_rows_d(self.h, _ptr(v), _ptr(hv), row_lo, row_hi)
 
+    def matvec_sweeps_d(self, v, hv, row_lo, row_hi):
+        """Output rows idw in [row_lo,row_hi) of spMatVec in the reference's loop order:
+        diagonal, then the DW sweep (iup outer, stride DimUp), then the UP sweep."""
+        lib().orc_stored_matvec_sweeps_d(self.h, _ptr(v), _ptr(hv), row_lo, row_hi)
+
     @property
     def dimdw(self):
         return lib().orc_stored_dimdw(self.h)
@@ -191,9 +197,11 @@ class Stored:
         n = lib().orc_tridiag_d(self.h, _ptr(v), nlanc, threshold, _ptr(a), _ptr(b), C.byref(n2))
         return a, b, n2.value, n
 
-    def ground_state(self, v0, maxit=300, tol=1e-14):
+    def ground_state(self, v0, maxit=300, tol=1e-14, want_vector=True):
+        """Returns (E0, eigenvector or None, a[:m], b[:m]); without the vector the
+        recurrence keeps three vectors only."""
         e0 = C.c_double()
-        evec = np.zeros(self.dim)
+        evec = np.zeros(self.dim) if want_vector else None
         a, b = np.zeros(maxit + 1), np.zeros(maxit + 1)
         v = np.ascontiguousarray(v0, dtype=np.float64)
         m = lib().orc_lanczos_gs_d(self.h, _ptr(v), maxit, tol, C.byref(e0), _ptr(evec), _ptr(a), _ptr(b))
@@ -272,6 +280,20 @@ def energy(m: Model, nup, ndw, psi, bw=1.0):
     lib().orc_energy_d(m.ref, nup, ndw, _ptr(psi), bw, *[C.byref(x) for x in out])
     ekin, epot, eknot, ehartree = (x.value for x in out)
     return ekin, epot + ehartree, eknot, ehartree
+
+
+def square_lattice(lx: int, ly: int, t: float = 1.0) -> np.ndarray:
+    """Hij of the periodic lx x ly square lattice with nearest-neighbour hopping -t, sites
+    numbered x + lx*y (the model mapping of the hot-path workloads)."""
+    ns = lx * ly
+    h = np.zeros((ns, ns))
+    for y in range(ly):
+        for x in range(lx):
+            i = x + lx * y
+            for j in ((x + 1) % lx + lx * y, x + lx * ((y + 1) % ly)):
+                if j != i:
+                    h[i, j] = h[j, i] = -t
+    return h
 
 
 def num_threads() -> int:
