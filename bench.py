@@ -286,12 +286,14 @@ def lowest_k_3x4(E):
             "e0": float(ev[0]), "max_resid": float(np.max(resid))}
 
 
-def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150):
+def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150, widths=(1, 4, 8, 16)):
     """Green's function chains on the 4x4 lattice at U=4 (t=1, XMU=2): ground state of the
     half-filled sector (8,8) (FP32+refine, vector kept on the device), then c^+_{i,up} into
     (9,8) and c_{i,up} into (7,8) (D = 147,232,800 each) for the 16 sites: 32 chains of 150
     steps with FP32 vectors, G_ii(iw_n) on 4096 Matsubara frequencies at beta=50 and on the
-    real axis (eta=0.05). Also the first `nchains_f64` chains with FP64 vectors for the ratio."""
+    real axis (eta=0.05). The 16 chains of each sector run as blocks of width w (block H x V,
+    edg_gf_chain_block; w = 1 is one chain after another through edg_gf_chain); all 32 chains
+    are 2 sectors x 16. Also the first `nchains_f64` chains with FP64 vectors for the ratio."""
     import torch
     model = E.Model(E.square_lattice(4, 4), uloc=4.0, xmu=2.0, hfmode=False)
     gs = E.Sector(model, 8, 8)
@@ -304,27 +306,96 @@ def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150):
     torch.cuda.synchronize()
     t_gs = time.perf_counter() - t0
     out = {"e0": e0.value, "gs_seconds": t_gs, "gs_hxv": it.value, "dim_gs": gs.dim, "dim_excited": part.dim}
-    for prec, name, nch in ((E.EDG_PREC_F32, "f32", 32), (E.EDG_PREC_F64, "f64", nchains_f64)):
-        chans = []
+    sites = np.arange(1, 17)
+    ref = None
+    for w in widths:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for c in range(nch):
-            site = c // 2 + 1
-            # particle chains (op=+1) and hole chains (op=-1, poles already -(theta-E0))
-            to, op = (part, +1) if c % 2 == 0 else (hole, -1)
-            chans.append(E.gf_chain(gs, to, op, site, 1, nlanc, e0.value, precision=prec))
+        chans = []
+        for to, op in ((part, +1), (hole, -1)):
+            if w == 1:
+                chans += [E.gf_chain(gs, to, op, int(i), 1, nlanc, e0.value, precision=E.EDG_PREC_F32) for i in sites]
+            else:
+                for c0 in range(0, 16, w):
+                    chans += E.gf_chain_block(gs, to, op, sites[c0:c0 + w], 1, nlanc, e0.value,
+                                              precision=E.EDG_PREC_F32)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         steps = sum(len(ch.poles) for ch in chans)
-        out[name] = {"chains": nch, "seconds": dt, "lanczos_steps": steps, "ms_per_step": 1e3 * dt / steps,
-                     "sum_rule_site1": chans[0].norm2 + chans[1].norm2}
-        if name == "f32":
+        key = "f32" if w == 1 else f"f32_block{w}"
+        out[key] = {"chains": len(chans), "width": w, "seconds": dt, "lanczos_steps": steps,
+                    "ms_per_step": 1e3 * dt / steps, "sum_rule_site1": chans[0].norm2 + chans[16].norm2}
+        if ref is None:
+            ref = chans
             wm, _, wr, _, _ = E.grids(1.0 / 50.0, lmats=4096, lreal=5000)
-            gm, gr = E.eval_gf(chans[:2], wm, wr, 0.05)
-            out[name]["G11_iw0"] = [gm[0].real, gm[0].imag]
+            gm, gr = E.eval_gf([chans[0], chans[16]], wm, wr, 0.05)
+            out[key]["G11_iw0"] = [gm[0].real, gm[0].imag]
+        else:  # the block's columns carry the single chains' coefficients: same spectra
+            out[key]["max_pole_diff_vs_width1"] = max(float(np.abs(a.poles - b.poles).max()) for a, b in zip(chans, ref))
+            out[key]["max_weight_diff_vs_width1"] = max(float(np.abs(a.weight - b.weight).max())
+                                                        for a, b in zip(chans, ref))
+    chans = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for c in range(nchains_f64):
+        site = c // 2 + 1
+        to, op = (part, +1) if c % 2 == 0 else (hole, -1)
+        chans.append(E.gf_chain(gs, to, op, site, 1, nlanc, e0.value, precision=E.EDG_PREC_F64))
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    steps = sum(len(ch.poles) for ch in chans)
+    out["f64"] = {"chains": nchains_f64, "seconds": dt, "lanczos_steps": steps, "ms_per_step": 1e3 * dt / steps,
+                  "sum_rule_site1": chans[0].norm2 + chans[1].norm2}
     out["f32_speedup_per_step"] = out["f64"]["ms_per_step"] / out["f32"]["ms_per_step"]
     for sct in (gs, part, hole):
         sct.delete()
+    return out
+
+
+def chi_q_6x3(E, L, nlanc=200, width=4):
+    """Config 5: the 6x3 periodic lattice (18 sites), t=1, U=4, XMU=2, sector (9,9)
+    (D = 2,363,904,400; 9.46 GB per FP32 vector). FP32+refine ground state to 1e-8, then the
+    spin (S^z_q) and charge (n_q) susceptibility chains of all 18 momenta, O_q = sum_i
+    cos(q.r_i) O_i, 200 steps each with FP32 vectors, run as blocks of `width` chains (the block
+    is split further when its 3*width work vectors do not fit in free HBM). Sum rule: the
+    cos and sin combinations of every q together carry N * sum_i <O_i^2> (one-step chains give
+    their norms)."""
+    import torch
+    lx, ly = 6, 3
+    model = E.Model(E.square_lattice(lx, ly), uloc=4.0, xmu=2.0, hfmode=False)
+    s = E.Sector(model, 9, 9)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, _, it = E.sp_lanc_eigh(s, seed=2024, maxit=600, tol=1e-8, mode=E.EDG_GS_F32_REFINE)
+    torch.cuda.synchronize()
+    out = {"dim": s.dim, "e0": e0, "gs_seconds": time.perf_counter() - t0, "gs_hxv": it, "width": width,
+           "steps_per_chain": nlanc}
+    s.release_work()
+    obs = s.observables()
+    xs, ys = np.meshgrid(np.arange(lx), np.arange(ly), indexing="xy")
+    r = np.stack([xs.ravel(), ys.ravel()], 1)
+    qs = [(2 * np.pi * m / lx, 2 * np.pi * n / ly) for n in range(ly) for m in range(lx)]
+    phase = np.array([q[0] * r[:, 0] + q[1] * r[:, 1] for q in qs])
+    qcos, qsin = np.cos(phase), np.sin(phase)
+    for kind, name in ((0, "spin"), (1, "charge")):
+        o2 = obs["dens"] - 2 * obs["docc"] if kind == 0 else obs["dens"] + 2 * obs["docc"]
+        if kind == 0:
+            o2 = o2 / 4.0
+        one = E.chi_chain_block(s, 1, e0, kind=kind, qcos=np.concatenate([qcos, qsin[np.abs(qsin).max(1) > 0]]))
+        total = sum(ch.norm2 for ch in one)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        chans = []
+        for c0 in range(0, len(qs), width):
+            chans += E.chi_chain_block(s, nlanc, e0, kind=kind, qcos=qcos[c0:c0 + width], precision=E.EDG_PREC_F32)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        steps = sum(len(ch.poles) for ch in chans)
+        out[name] = {"chains": len(chans), "seconds": dt, "lanczos_steps": steps, "ms_per_step": 1e3 * dt / steps,
+                     "sum_rule_rel_err": abs(total - lx * ly * o2.sum()) / (lx * ly * o2.sum()),
+                     "chi_q0_weight": float(chans[0].weight.sum())}
+        s.release_work()
+    s.delete()
     return out
 
 
@@ -344,6 +415,8 @@ def run_ours(args):
     D = sector.dim
     stream = torch.cuda.current_stream()
     L.check(lib.edg_sector_set_stream(sector.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
+    # the autotuner picks the H x v kernel pair of this sector for each precision (untimed)
+    tune = {"f32": sector.autotune(E.EDG_PREC_F32, reps=5), "f64": sector.autotune(E.EDG_PREC_F64, reps=3)}
     g = torch.Generator(device="cuda")
     g.manual_seed(1234 + rank)
     v = torch.rand(D, device="cuda", dtype=torch.float32, generator=g) * 2 - 1
@@ -453,6 +526,11 @@ def run_ours(args):
         extra["thermal_3x4_beta20"] = thermal_3x4(E)
     if rank == 0 and not args.no_lowk and ws == 1:
         extra["lowest_k_3x4_sector66"] = lowest_k_3x4(E)
+    if rank == 0 and args.config5 and ws == 1:
+        sector.delete()
+        torch.cuda.empty_cache()
+        extra["chi_q_6x3_U4"] = chi_q_6x3(E, L)
+        sector = E.Sector(model, NUP, NDW, E.EDG_FORM_STORED)
     if rank == 0 and not args.no_gf and ws == 1:
         sector.delete()
         torch.cuda.empty_cache()
@@ -471,13 +549,16 @@ def run_ours(args):
                        "ndw": NDW, "dim": D, "form": "stored", "vector_bytes": D * 4,
                        "l2_policy": "inputs larger than L2 (662 MB per vector), no flush",
                        "parallelism": f"replicas x{ws}"},
-            "roofline": {"bound": "hbm", "kernel": "hxv_f32 (k_dw_grp + k_up_smem, one H x v)",
+            "roofline": {"bound": "hbm", "kernel": "hxv_f32 (down pass + up pass of one H x v, the autotuner's pair)",
                          "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_launch_ms,
                          "traffic": TRAFFIC_GB, "traffic_unit": "GB per H x v",
                          "traffic_source": TRAFFIC_SOURCE},
             "clocks": clk.summary(),
+            "autotune": {"candidates": "3*down + up; down: 0 row groups, 1 block-staged 1 CTA/SM, 2 block-staged "
+                                       "2 CTAs/SM; up (FP32): 0 SELL-32, 1 packed 16-bit negated copies, 2 packed "
+                                       "16-bit sign bits", **tune},
             "gpu_launches": 2 * args.steps,
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -502,6 +583,8 @@ def main():
     ap.add_argument("--no-thermal", action="store_true")
     ap.add_argument("--no-gf", action="store_true")
     ap.add_argument("--no-lowk", action="store_true")
+    ap.add_argument("--config5", action="store_true",
+                    help="also run the 6x3 susceptibility sweep (36 chains of 200 steps on 2.36e9 states, minutes)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -58,8 +58,10 @@ SIGNATURES = {
     "edg_sector_get_maps": (_i, [_p, _pi32, _pi32]),
     "edg_sector_get_hops": (_i, [_p, _i, _pi64, _pi32, _pd, _pi64]),
     "edg_sector_set_stream": (_i, [_p, _p]),
+    "edg_sector_release_work": (_i, [_p]),
     "edg_hxv_z": (_i, [_p, _i64, _pd, _pd]),
     "edg_hxv_d": (_i, [_p, _i64, _pd, _pd]),
+    "edg_sector_autotune": (_i, [_p, _i, _i, _pd, _pi, _pi]),
     "edg_hxv_dev_f64": (_i, [_p, _p, _p]),
     "edg_hxv_dev_f32": (_i, [_p, _p, _p]),
     "edg_tridiag_d": (_i, [_p, _pd, _i, _d, _i, _pd, _pd, _pd, _pi]),
@@ -87,6 +89,9 @@ SIGNATURES = {
     "edg_tridiag_eigh": (_i, [_i, _pd, _pd, _pd, _pd]),
     "edg_tridiag_lowest": (_i, [_i, _pd, _pd, _i, _pd, _pd]),
     "edg_poles_weights": (_i, [_i, _pd, _pd, _d, _d, _i, _pd, _pd]),
+    "edg_gf_chain_block": (_i, [_p, _p, _i, _i, _pi, _pi, _i, _i, _i, _d, _pd, _pd, _pd, _pi]),
+    "edg_chi_chain_block": (_i, [_p, _i, _i, _pi, _pi, _pd, _i, _i, _d, _pd, _pd, _pd, _pi]),
+    "edg_poles_weights_block": (_i, [_i, _i, _pd, _pd, _pd, _pi, _d, _i, _pd, _pd]),
 }
 
 

@@ -17,8 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libedgpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-SOURCES = ["basis.cu", "hxv.cu", "vecops.cu", "lanczos.cu", "excite.cu", "capi.cu", "noalloc.cu", "lowest.cu", "evalgrid.cu", "tridiag_host.cpp"]
-HEADERS = ["common.cuh"]
+SOURCES = ["basis.cu", "hxv.cu", "vecops.cu", "lanczos.cu", "excite.cu", "capi.cu", "noalloc.cu", "lowest.cu", "evalgrid.cu", "chains.cu", "tridiag_host.cpp"]
+HEADERS = ["common.cuh", "reduce.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

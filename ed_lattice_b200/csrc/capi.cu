@@ -238,6 +238,24 @@ int edg_sector_destroy(edg_sector* s) {
 
 int edg_release_cached_memory(void) { return pool_trim(0); }
 
+int edg_sector_release_work(edg_sector* s) {
+  EDG_CHECK(check_sector(s));
+  EDG_ON_DEVICE(s->device);
+  if (s->stream) EDG_CUDA(cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 4; ++k) {
+    s->w64[k].reset();
+    s->w32[k].reset();
+  }
+  s->zstage.reset();
+  s->basis32.reset();
+  s->basis32_cols = 0;
+  s->blk64.reset();
+  s->blk32.reset();
+  s->blkred.reset();
+  s->blkact.reset();
+  return EDG_OK;
+}
+
 int edg_sector_vlen(const edg_sector* s, int64_t* vlen) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(vlen, "edg_sector_vlen: NULL");
@@ -296,6 +314,15 @@ int edg_sector_set_stream(edg_sector* s, void* stream) {
   s->stream = static_cast<cudaStream_t>(stream);
   s->own_stream = false;
   return EDG_OK;
+}
+
+int edg_sector_autotune(edg_sector* s, int precision, int reps, double* ms, int* ncand, int* best) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_sector_autotune: precision=%d", precision);
+  EDG_ARG(reps >= 1 && reps <= 1000, "edg_sector_autotune: reps=%d", reps);
+  EDG_ON_DEVICE(s->device);
+  return precision == EDG_PREC_F32 ? hxv_autotune<float>(s, reps, ms, ncand, best)
+                                   : hxv_autotune<double>(s, reps, ms, ncand, best);
 }
 
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv) {
@@ -630,10 +657,79 @@ int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc,
                           double* alanc, double* blanc, double* norm2, int* nsteps) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(k >= 1 && dvinit && alanc && blanc && norm2 && nsteps, "edg_tridiag_block_dev: bad arguments");
+  EDG_ARG(nlanc >= 0, "edg_tridiag_block_dev: nlanc=%d", nlanc);
+  EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_tridiag_block_dev: precision=%d", precision);
+  EDG_CHECK(check_vec_align<double>(s, dvinit, "edg_tridiag_block_dev"));
+  EDG_ON_DEVICE(s->device);
+  return tridiag_block(s, k, dvinit, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
+}
+
+int edg_gf_chain_block(const edg_sector* from, edg_sector* to, int op, int k, const int* sites, const int* sites2,
+                       int spin, int nlanc, int precision, double ei, double* poles, double* weights, double* norm2,
+                       int* nout) {
+  EDG_CHECK(check_sector(from));
+  EDG_CHECK(check_sector(to));
+  EDG_ARG(k >= 1 && sites && poles && weights && norm2 && nout, "edg_gf_chain_block: bad arguments");
+  EDG_ARG(nlanc >= 1, "edg_gf_chain_block: nlanc=%d", nlanc);
+  EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_gf_chain_block: precision=%d", precision);
+  if (!from->has_state) {
+    set_error("edg_gf_chain_block: origin sector holds no state");
+    return EDG_ERR_STATE;
+  }
+  for (int c = 0; c < k; ++c) {
+    EDG_ARG(sites[c] >= 1 && sites[c] <= from->model.ns, "edg_gf_chain_block: sites[%d]=%d", c, sites[c]);
+    EDG_ARG(!sites2 || sites2[c] <= from->model.ns, "edg_gf_chain_block: sites2[%d]=%d", c, sites2[c]);
+  }
+  EDG_ON_DEVICE(to->device);
+  // one excitation vector at a time, each normalised into the block's own vectors
+  DevBuf<double> X;
+  EDG_CHECK(X.alloc(size_t(to->vlen), to->stream, "excitation vector"));
+  StartFn start = [&](int c, const double** x) -> int {
+    EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, sites[c], spin, 1.0, 0, from->state.p, X.p));
+    if (sites2 && sites2[c] > 0)
+      EDG_CHECK(edg_apply_cop_dev_f64(from, to, op, sites2[c], spin, 1.0, 1, from->state.p, X.p));
+    *x = X.p;
+    return EDG_OK;
+  };
+  return chains_block(to, k, start, nlanc, precision, ei, op, poles, weights, norm2, nout);
+}
+
+int edg_chi_chain_block(edg_sector* s, int kind, int k, const int* sites, const int* sites2, const double* qcos,
+                        int nlanc, int precision, double ei, double* poles, double* weights, double* norm2,
+                        int* nout) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(k >= 1 && (sites || qcos) && poles && weights && norm2 && nout, "edg_chi_chain_block: bad arguments");
+  EDG_ARG(nlanc >= 1, "edg_chi_chain_block: nlanc=%d", nlanc);
+  EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_chi_chain_block: precision=%d", precision);
+  if (!s->has_state) {
+    set_error("edg_chi_chain_block: sector holds no state");
+    return EDG_ERR_STATE;
+  }
+  EDG_ON_DEVICE(s->device);
+  DevBuf<double> X;
+  EDG_CHECK(X.alloc(size_t(s->vlen), s->stream, "excitation vector"));
+  const int ns = s->model.ns;
+  StartFn start = [&](int c, const double** x) -> int {
+    EDG_CHECK(edg_apply_diagop_dev_f64(s, kind, sites ? sites[c] : 1, sites2 ? sites2[c] : 0,
+                                       qcos ? qcos + size_t(c) * ns : nullptr, s->state.p, X.p));
+    *x = X.p;
+    return EDG_OK;
+  };
+  return chains_block(s, k, start, nlanc, precision, ei, 1, poles, weights, norm2, nout);
+}
+
+int edg_poles_weights_block(int k, int nlanc, const double* alanc, const double* blanc, const double* norm2,
+                            const int* nsteps, double ei, int isign, double* poles, double* weights) {
+  EDG_ARG(k >= 0 && nlanc >= 0, "edg_poles_weights_block: negative size");
+  EDG_ARG(k == 0 || nlanc == 0 || (alanc && blanc && norm2 && nsteps && poles && weights),
+          "edg_poles_weights_block: NULL array");
   for (int c = 0; c < k; ++c)
-    EDG_CHECK(edg_tridiag_dev_f64(s, dvinit + size_t(c) * s->vlen, nlanc, threshold, precision,
-                                  alanc + size_t(c) * nlanc, blanc + size_t(c) * nlanc, norm2 + c, nsteps + c));
-  return EDG_OK;
+    EDG_ARG(nsteps[c] >= 0 && nsteps[c] <= nlanc, "edg_poles_weights_block: nsteps[%d]=%d", c, nsteps[c]);
+  int dev = 0;
+  EDG_CUDA(cudaGetDevice(&dev));
+  cudaStream_t st = nullptr;
+  EDG_CUDA(pooled_stream(dev, &st));
+  return poles_block(st, k, nlanc, alanc, blanc, norm2, nsteps, ei, isign, poles, weights);
 }
 
 }  // extern "C"

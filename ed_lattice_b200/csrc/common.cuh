@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -153,6 +154,16 @@ struct SpinBasis {
   DevBuf<uint32_t> sched_ent;
   DevBuf<uint32_t> sched_off;
   int sched_rt = 0;             // rows-per-CTA of the FP32 up pass the schedule was built for
+  // Packed FP32 schedule (uniform tables, 2 * (DimUp + 32) <= 32768 slots): the conflict-free
+  // slot schedule for two rows per CTA with slot counts rounded to 2 instead of 8, two 16-bit
+  // entries per 32-bit word (entry 2k of a row in the low half of word k, 2k+1 in the high
+  // half). An entry is the shared-memory slot of its source: src for a positive term,
+  // p16_negoff + src for a negative one, where the up pass keeps the negated copy of the
+  // staged rows, so no term applies a sign.
+  DevBuf<uint32_t> p16_ent;     // words in SELL-32 slices, word-major
+  DevBuf<uint32_t> p16_off;     // [nslices+1] word offsets, multiples of 32
+  DevBuf<uint32_t> p16f_ent;    // the same words with the sign as bit 15 of each entry
+  uint32_t p16_negoff = 0;      // 0: no packed schedule
   // Column-split copy of the SELL table for rows too long to stage whole in shared memory
   // (FP64 rows above 227 KB): part p lists, per slice, the entries whose source lies in
   // columns [split_col[p], split_col[p+1]), stored as source - split_col[p] (padding: the
@@ -168,6 +179,15 @@ struct SpinBasis {
   int max_row = 0;              // longest hop list of any configuration
   // Down-spin pass work split: rows grouped into `groups` CTAs with near-equal total hop
   // counts (longest-processing-time-first assignment), CSR: group_off[groups+1], group_rows.
+  // Contiguous row blocks for the block-staged down pass, one CTA each: block g owns rows
+  // [off[g], off[g+1]), blocks balanced by hop count; rowblk[0] for 1024-thread CTAs (about
+  // one per SM), rowblk[1] for 512-thread CTAs (about two per SM).
+  struct RowBlocks {
+    DevBuf<uint32_t> off;
+    int count = 0;
+    int max_rows = 0;
+  };
+  RowBlocks rowblk[2];
   DevBuf<uint32_t> group_off;
   DevBuf<uint32_t> group_rows;
   int groups = 0;
@@ -218,9 +238,19 @@ struct edg_sector_s {
   edg::DevBuf<double> state;      // FP64 eigenvector kept on the device (ground_state_keep)
   edg::DevBuf<double> zstage;     // interleaved complex staging of the dd_sparse_HxV entry
   edg::DevBuf<float> basis32;     // FP32 Lanczos basis for Ritz vectors
+  edg::DevBuf<double> blk64;      // block Lanczos: 3 blocks of k vectors (FP64 or FP32)
+  edg::DevBuf<float> blk32;
+  edg::DevBuf<double> blkred;     // block Lanczos scalars and reduction scratch
+  edg::DevBuf<int> blkact;        // block Lanczos: active flag per column
   size_t basis32_cols = 0;
   bool has_state = false;
   int last_n32 = 0, last_n64 = 0;  // H x v applications of the last ground-state run per precision
+  // H x v kernel choice per vector precision ([0] FP64, [1] FP32), set by edg_sector_autotune:
+  // down pass 0 = hop-balanced row groups, 1 = block-staged (one CTA per SM), 2 = block-staged
+  // (two CTAs per SM); up pass (FP32) 0 = 32-bit SELL schedule, 1 = packed 16-bit schedule
+  // with negated copies, 2 = packed 16-bit schedule with sign bits. 0/0 until tuned.
+  int hxv_dw[2] = {0, 0};
+  int hxv_up[2] = {0, 0};
 };
 
 namespace edg {
@@ -253,12 +283,31 @@ template <typename T>
 int hxv_apply(edg_sector_s* s, const T* v, T* hv);
 template <typename T>
 int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double* bn, int j, double* partial,
-                 int* nblocks);
+                 double* aout);
 bool hxv_lz_available(const edg_sector_s* s, size_t elem);
+template <typename T>
+int hxv_autotune(edg_sector_s* s, int reps, double* ms, int* nc, int* best);
+// Block forms over ncols vectors of the sector (column c at v + c*vlen): one launch per pass
+// for all columns; columns whose device flag active[c] is 0 are skipped (active may be null).
+// Available where the fused single-vector step is (hxv_lz_available).
+template <typename T>
+int hxv_block(edg_sector_s* s, int ncols, const int* active, const T* v, T* hv);
+// Fused block step: per column, v_c = u_c / bn[c*sstride + j]; writes
+// w_c = H v_c - (bn_j / bn_{j-1}) uprev_c and <v_c, w_c> into aout[c*sstride] (reduction
+// scratch: partial + c*kRedSlots).
+template <typename T>
+int hxv_block_lz(edg_sector_s* s, int ncols, const int* active, const T* u, const T* uprev, T* w, const double* bn,
+                 int64_t sstride, int j, double* partial, double* aout);
 
 // ---- vecops.cu
 constexpr int kRedBlocks = 592;  // 148 SMs x 4: fixed reduction grid (deterministic sums)
 constexpr int kRedThreads = 256;
+// A reduction scratch holds kRedBlocks partials and, at index kRedBlocks, the arrival counter
+// of the fused finish (the last block of a reduction sums the partials and resets it to 0):
+// kRedSlots doubles. The counter must be zero when the scratch is first used
+// (red_scratch_reset).
+constexpr int kRedSlots = kRedBlocks + 2;
+int red_scratch_reset(cudaStream_t st, double* partial);
 template <typename T>
 int dot_dev(cudaStream_t st, const T* x, const T* y, int64_t n, double* partial, double* out);
 template <typename T>
@@ -273,6 +322,27 @@ template <typename T>
 int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
                     double* bn_next);
 int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, int do_sqrt);
+// block forms (ncols columns: vectors vstride elements apart, device scalars sstride apart,
+// reduction scratch kRedSlots apart; columns whose active[c] is 0 are skipped)
+template <typename T>
+int dot_cols(cudaStream_t st, int ncols, const T* x, const T* y, int64_t n, int64_t vstride, double* partial,
+             double* out, int64_t sstride, int do_sqrt);
+template <typename TD, typename TS>
+int normalise_cols(cudaStream_t st, int ncols, TD* dst, int64_t dstride, const TS* src, int64_t srcstride,
+                   const double* norm2, int64_t sstride, int64_t n);
+template <typename T>
+int lanczos_step_a_cols(cudaStream_t st, int ncols, const int* active, T* w, const T* vprev, const T* v,
+                        int64_t vstride, const double* bprev, double* partial, double* aout, int64_t sstride, int64_t n);
+template <typename T>
+int lanczos_step_b_cols(cudaStream_t st, int ncols, const int* active, T* w, const T* v, int64_t vstride,
+                        const double* a, double* partial, double* bout, int64_t sstride, int64_t n);
+template <typename T>
+int lanczos_step_b2_cols(cudaStream_t st, int ncols, const int* active, T* w, const T* u, int64_t vstride,
+                         const double* a, const double* bn, double* partial, double* bn_next, int64_t sstride,
+                         int64_t n);
+template <typename T>
+int scale_into_cols(cudaStream_t st, int ncols, const int* active, T* dst, const T* src, int64_t vstride,
+                    const double* b, int64_t sstride, int64_t n);
 // *out = |x| (FP64, fixed reduction grid; partial holds kRedBlocks values)
 int norm_dev(cudaStream_t st, const double* x, int64_t n, double* partial, double* out);
 // dst = TD(src * scale); dst and src must not overlap (scale_inplace_dev scales in place)
@@ -289,6 +359,26 @@ uint64_t splitmix64(uint64_t x);
 // ---- lanczos.cu
 int tridiag_dev(edg_sector_s* s, const double* dv0, int nlanc, double threshold, int precision,
                 double* alanc, double* blanc, double* norm2, int* nsteps);
+// k chains of one sector in lockstep (block H x V); start vectors dv0 + c*vlen (FP64, device);
+// alanc/blanc [k][nlanc] on the host; falls back to one chain after another where the fused
+// step is not available, and splits k into blocks that fit in free HBM.
+int tridiag_block(edg_sector_s* s, int k, const double* dv0, int nlanc, double threshold, int precision,
+                  double* alanc, double* blanc, double* norm2, int* nsteps);
+// Same with the start vectors produced on demand: start(c, &x) points x at column c's FP64
+// device vector, which need only stay valid until the next call (one shared buffer does).
+using StartFn = std::function<int(int, const double**)>;
+int tridiag_block_fn(edg_sector_s* s, int k, const StartFn& start, int nlanc, double threshold, int precision,
+                     double* alanc, double* blanc, double* norm2, int* nsteps);
+
+// ---- chains.cu
+// k chains from the excitation vectors start(c) (FP64, device) of sector `to`: block
+// tridiagonalisation (threshold 1e-9) and the poles isign*(theta_j - ei) / weights
+// norm2*Z(1,j)^2 of each on the device; poles/weights [k][nlanc] on the host.
+int chains_block(edg_sector_s* to, int k, const StartFn& start, int nlanc, int precision, double ei, int isign,
+                 double* poles, double* weights, double* norm2, int* nout);
+// poles and weights of k chains from host coefficients [k][nlanc] (one launch)
+int poles_block(cudaStream_t st, int k, int nlanc, const double* alanc, const double* blanc, const double* norm2,
+                const int* nsteps, double ei, int isign, double* poles, double* weights);
 int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
                  double* e0, int* niter);
 

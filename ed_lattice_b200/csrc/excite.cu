@@ -389,17 +389,18 @@ int energy(edg_sector_s* s, const double* psi, double weight, double* ekin, doub
   double* hv = s->w64[0].p;
   EDG_CHECK(hxv_apply<double>(s, psi, hv));
   DevBuf<double> part;
-  EDG_CHECK(part.alloc(size_t(kRedBlocks) + kDiagBlocks + 4, st, "energy partials"));
-  double* out = part.p + kRedBlocks + kDiagBlocks;
+  EDG_CHECK(part.alloc(size_t(kRedSlots) + kDiagBlocks + 4, st, "energy partials"));
+  double* out = part.p + kRedSlots + kDiagBlocks;
+  EDG_CHECK(red_scratch_reset(st, part.p));
   EDG_CHECK(dot_dev<double>(st, psi, hv, n, part.p, out));
   if (s->cplx)
     k_diag_dot<2><<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, s->dim, s->up.e64.p, s->dw.e64.p, s->up.map.p,
-                                               s->dw.map.p, s->U, part.p + kRedBlocks);
+                                               s->dw.map.p, s->U, part.p + kRedSlots);
   else
     k_diag_dot<1><<<kDiagBlocks, 256, 0, st>>>(psi, s->up.dim, s->dim, s->up.e64.p, s->dw.e64.p, s->up.map.p,
-                                               s->dw.map.p, s->U, part.p + kRedBlocks);
+                                               s->dw.map.p, s->U, part.p + kRedSlots);
   EDG_CUDA(cudaGetLastError());
-  EDG_CHECK(finish_dev(st, part.p + kRedBlocks, kDiagBlocks, out + 1, 0));
+  EDG_CHECK(finish_dev(st, part.p + kRedSlots, kDiagBlocks, out + 1, 0));
   double h[2] = {0.0, 0.0};
   EDG_CUDA(cudaMemcpyAsync(h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));

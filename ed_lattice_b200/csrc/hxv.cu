@@ -12,8 +12,11 @@
 //  DIRECT (directMatVec, src/DIAG/HAMILTONIAN_DIRECT_HxV.f90:19-59): diag, UP, DW;
 // inside each spin part sources are added in ascending rank, as the reference's loops do.
 #include <algorithm>
+#include <cstdlib>
+#include <type_traits>
 
 #include "common.cuh"
+#include "reduce.cuh"
 
 namespace edg {
 namespace {
@@ -39,8 +42,34 @@ struct HxvArgs {
   const double* __restrict__ bn = nullptr;
   int jstep = 0;
   const T* __restrict__ uprev = nullptr;
-  double* __restrict__ partial = nullptr;
+  double* __restrict__ partial = nullptr;  // reduction scratch [kRedSlots]
+  double* __restrict__ red_out = nullptr;  // receives <v, w>
+  // Block mode (several vectors of the sector in one launch, blockIdx.y = column c): column c
+  // reads v + c*vstride, writes hv + c*vstride, uses uprev + c*vstride, bn + c*sstride,
+  // red_out + c*sstride and the scratch partial + c*kRedSlots; a column whose active[c] is 0
+  // is skipped. ncols is the launch's gridDim.y (1 for a single vector).
+  int64_t vstride = 0, sstride = 0;
+  const int* __restrict__ active = nullptr;
+  int ncols = 1;
+  int dwv = 0, upv = 0;  // kernel choice (edg_sector_s::hxv_dw / hxv_up)
 };
+
+// Points a block-mode launch's arguments at this CTA's column; false when the column has
+// stopped. A single-vector launch (gridDim.y == 1, active == nullptr) is left as it is.
+template <typename T>
+__device__ __forceinline__ bool select_column(HxvArgs<T>& a) {
+  const int64_t c = blockIdx.y;
+  if (a.active && !a.active[c]) return false;
+  if (c) {
+    a.v += c * a.vstride;
+    a.hv += c * a.vstride;
+    if (a.uprev) a.uprev += c * a.vstride;
+    if (a.bn) a.bn += c * a.sstride;
+    if (a.partial) a.partial += c * kRedSlots;
+    if (a.red_out) a.red_out += c * a.sstride;
+  }
+  return true;
+}
 
 template <typename T>
 __device__ __forceinline__ T fmaT(T a, T b, T c);
@@ -138,6 +167,7 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 // applied.
 template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE>
 __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+  if (!select_column(a)) return;
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
@@ -256,6 +286,119 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, Sel
       for (int q = 0; q < int(blockDim.x >> 5); ++q) t += s_red[q];
       a.partial[blockIdx.x] = t;
     }
+    finish_in_last_block(a.partial, gridDim.x, a.red_out, 0);
+  }
+}
+
+// FP32 up pass over the packed 16-bit schedule (SpinBasis::p16_*). A CTA stages RT rows
+// interleaved in shared memory as in k_up_smem and, when NEG, their negated copy at slot
+// offset negoff, so that every term is one shared load and one FMA with the uniform hopping
+// value: the entry is the slot itself (src, or negoff + src for a negative term). Without NEG
+// the entry carries the sign in bit 15 and the value's sign bit is flipped per term. Entries
+// come two per 32-bit word; a warp walks its slice in batches of four words (eight terms)
+// with warp-uniform bounds (all 32 lanes of a warp share one slice). Slot counts are rounded
+// to 2 instead of 8, and the slot order is the bank-conflict-free schedule of k_up_smem, so
+// each half-warp's shared loads hit 16 distinct 8-byte bank pairs.
+struct P16Args {
+  const uint32_t* __restrict__ ent;
+  const uint32_t* __restrict__ off;
+  float h;
+  uint32_t negoff;
+};
+
+__device__ __forceinline__ void ffma2_acc(uint64_t& acc, uint64_t h2, uint64_t x) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(h2), "l"(x));
+}
+
+template <bool NEG, bool ONE, bool LZ>
+__global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_p16(HxvArgs<float> a, P16Args q, int64_t nrowblk) {
+  if (!select_column(a)) return;
+  extern __shared__ __align__(16) unsigned char smem_p16[];
+  float2* S = reinterpret_cast<float2*>(smem_p16);
+  const uint64_t* S64 = reinterpret_cast<const uint64_t*>(smem_p16);
+  const int64_t dimup = a.dimup;
+  double sc = 1.0, cc = 0.0, pa = 0.0;
+  if (LZ) {
+    sc = 1.0 / a.bn[a.jstep];
+    cc = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+  }
+  const float hs = LZ ? float(double(q.h) * sc) : q.h;
+  const uint64_t hh = (uint64_t(__float_as_uint(hs)) << 32) | __float_as_uint(hs);
+  for (int zq = threadIdx.x; zq < kUpZeroSlots; zq += blockDim.x) {  // padding targets
+    S[dimup + zq] = make_float2(0.f, 0.f);
+    if (NEG) S[q.negoff + dimup + zq] = make_float2(0.f, 0.f);
+  }
+  for (int64_t rb = blockIdx.x; rb < nrowblk; rb += gridDim.x) {
+    const int64_t r0 = rb * 2;
+    const bool two = r0 + 1 < a.dimdw;
+    const float* __restrict__ v0 = a.v + r0 * dimup;
+    const float* __restrict__ v1 = two ? v0 + dimup : v0;
+    for (int64_t j = threadIdx.x; j < dimup; j += blockDim.x) {
+      const float2 x = make_float2(v0[j], two ? v1[j] : 0.f);
+      S[j] = x;
+      if (NEG) S[q.negoff + j] = make_float2(-x.x, -x.y);
+    }
+    __syncthreads();
+    float* __restrict__ h0 = a.hv + r0 * dimup;
+    float* __restrict__ h1 = h0 + dimup;
+    for (int64_t iup = threadIdx.x; iup < dimup; iup += blockDim.x) {
+      const uint32_t o1 = q.off[(iup >> 5) + 1];
+      uint32_t p = q.off[iup >> 5] + uint32_t(iup & 31);
+      uint64_t acc = (uint64_t(__float_as_uint(two ? h1[iup] : 0.f)) << 32) | __float_as_uint(h0[iup]);
+      for (; p < o1; p += 32 * 4) {
+        uint32_t w[4];  // the table carries 128 words of padding after its last slice
+#pragma unroll
+        for (int u = 0; u < 4; ++u) w[u] = __ldg(q.ent + p + 32u * u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (p + 32u * u < o1) {
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+              const uint32_t e = half ? (w[u] >> 16) : (w[u] & 0xffffu);
+              if (NEG) {
+                ffma2_acc(acc, hh, S64[e]);
+              } else {
+                const uint64_t x = S64[e & 0x7fffu];
+                const float hf = __uint_as_float(__float_as_uint(hs) ^ ((e & 0x8000u) << 16));
+                float lo = __uint_as_float(uint32_t(acc)), hi = __uint_as_float(uint32_t(acc >> 32));
+                lo = __fmaf_rn(hf, __uint_as_float(uint32_t(x)), lo);
+                hi = __fmaf_rn(hf, __uint_as_float(uint32_t(x >> 32)), hi);
+                acc = (uint64_t(__float_as_uint(hi)) << 32) | __float_as_uint(lo);
+              }
+            }
+          }
+        }
+      }
+      const float acc0 = __uint_as_float(uint32_t(acc)), acc1 = __uint_as_float(uint32_t(acc >> 32));
+      if (LZ) {
+        const float2 xc = S[iup];
+        const int64_t e0 = r0 * dimup + iup;
+        const float w0 = float(double(acc0) - cc * double(a.uprev[e0]));
+        pa = __fma_rn(double(xc.x) * sc, double(w0), pa);
+        __stcs(h0 + iup, w0);
+        if (two) {
+          const float w1 = float(double(acc1) - cc * double(a.uprev[e0 + dimup]));
+          pa = __fma_rn(double(xc.y) * sc, double(w1), pa);
+          __stcs(h1 + iup, w1);
+        }
+      } else {
+        __stcs(h0 + iup, acc0);
+        if (two) __stcs(h1 + iup, acc1);
+      }
+    }
+    __syncthreads();
+  }
+  if (LZ) {  // block partial of <v, w>, fixed order, then the fused finish
+    __shared__ double s_red[32];
+    for (int o = 16; o > 0; o >>= 1) pa += __shfl_down_sync(0xffffffffu, pa, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = pa;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) t += s_red[w];
+      a.partial[blockIdx.x] = t;
+    }
+    finish_in_last_block(a.partial, gridDim.x, a.red_out, 0);
   }
 }
 
@@ -419,6 +562,7 @@ constexpr int kDwHops = 32;  // hop-list capacity per row held in shared memory
 template <typename T, int VEC, int NSEG, int KU, bool FIRST, bool SCALED>
 __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t* __restrict__ goff,
                                                 const uint32_t* __restrict__ grows, int64_t nslab) {
+  if (!select_column(a)) return;
   extern __shared__ __align__(16) unsigned char smem_dw[];
   const double sc = SCALED ? 1.0 / a.bn[a.jstep] : 1.0;
   __shared__ int s_ctr;
@@ -495,6 +639,154 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
 #pragma unroll
           for (int g = 0; g < NSEG; ++g)
             if (act[g]) VecLd<T, VEC>::load(src + g * SEGW, x[u][g]);
+        }
+#pragma unroll
+        for (int u = 0; u < KU; ++u) {
+          if (k + u < cnt) {
+            const T h = hvv[k + u];
+#pragma unroll
+            for (int g = 0; g < NSEG; ++g)
+              if (act[g]) Fma<T, VEC>::run(h, x[u][g], acc[g]);
+          }
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < NSEG; ++g)
+        if (act[g]) {
+#pragma unroll
+          for (int r = 0; r < VEC; ++r) __stcs(a.hv + e0 + g * SEGW + r, acc[g][r]);
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// Down-spin pass over contiguous row blocks. CTA g owns the rows of block g (consecutive
+// ranks, blocks balanced by hop count) and sweeps the column slabs (32*VEC*NSEG columns) in
+// the order of k_dw_grp. For each slab it first stages its own rows' slab segments in shared
+// memory; a hop whose source row lies in the block (about a third of them on square
+// lattices: hops among the low-order sites keep the high-order part of the bitstring, hence
+// the rank range) reads the source there, every other hop reads it from L2 as k_dw_grp does.
+// The choice is per (row, hop), uniform over the warp, and the terms keep k_dw_grp's order,
+// so results are bit-identical to it.
+template <typename T, int VEC>
+struct VecLds {  // VEC-wide shared-memory load
+  static __device__ __forceinline__ void load(const T* p, T* x) {
+#pragma unroll
+    for (int r = 0; r < VEC; ++r) x[r] = p[r];
+  }
+};
+template <>
+struct VecLds<float, 2> {
+  static __device__ __forceinline__ void load(const float* p, float* x) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    x[0] = t.x;
+    x[1] = t.y;
+  }
+};
+template <>
+struct VecLds<double, 2> {
+  static __device__ __forceinline__ void load(const double* p, double* x) {
+    const double2 t = *reinterpret_cast<const double2*>(p);
+    x[0] = t.x;
+    x[1] = t.y;
+  }
+};
+
+template <typename T, int VEC, int NSEG, int KU, bool FIRST, bool SCALED, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_dw_blk(HxvArgs<T> a, const uint32_t* __restrict__ boff, int64_t nslab) {
+  if (!select_column(a)) return;
+  extern __shared__ __align__(16) unsigned char smem_dwb[];
+  constexpr int SEGW = 32 * VEC, SLAB = SEGW * NSEG;
+  const double sc = SCALED ? 1.0 / a.bn[a.jstep] : 1.0;
+  __shared__ int s_ctr;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t r0 = boff[blockIdx.x];
+  const int nr = int(boff[blockIdx.x + 1] - r0);
+  T* tile = reinterpret_cast<T*>(smem_dwb);                 // [nr][SLAB]
+  T* s_val = tile + size_t(nr) * SLAB;                      // [nr][kDwHops]
+  T* s_edw = s_val + size_t(nr) * kDwHops;                  // [nr]
+  uint32_t* s_src = reinterpret_cast<uint32_t*>(s_edw + nr);  // [nr][kDwHops]
+  uint32_t* s_mdw = s_src + size_t(nr) * kDwHops;           // [nr]
+  int* s_cnt = reinterpret_cast<int*>(s_mdw + nr);          // [nr]
+  for (int rr = wib; rr < nr; rr += nw) {
+    const uint32_t row = r0 + rr;
+    const uint32_t k0 = a.off_dw[row];
+    const int cnt = int(a.off_dw[row + 1] - k0);
+    if (lane < cnt) {
+      s_src[rr * kDwHops + lane] = a.src_dw[k0 + lane];
+      s_val[rr * kDwHops + lane] = SCALED ? T(double(a.val_dw[k0 + lane]) * sc) : a.val_dw[k0 + lane];
+    }
+    if (lane == 0) {
+      s_cnt[rr] = cnt;
+      s_edw[rr] = a.e_dw[row];
+      s_mdw[rr] = a.map_dw[row];
+    }
+  }
+  const int64_t dimup = a.dimup;
+  for (int64_t slab = 0; slab < nslab; ++slab) {
+    const int64_t col0 = slab * SLAB + int64_t(lane) * VEC;
+    bool act[NSEG];
+#pragma unroll
+    for (int g = 0; g < NSEG; ++g) act[g] = col0 + g * SEGW < dimup;
+    // stage the block's own rows of this slab
+    for (int rr = wib; rr < nr; rr += nw) {
+      const T* __restrict__ src = a.v + int64_t(r0 + rr) * dimup + col0;
+#pragma unroll
+      for (int g = 0; g < NSEG; ++g)
+        if (act[g]) VecLd<T, VEC>::load(src + g * SEGW, tile + size_t(rr) * SLAB + g * SEGW + lane * VEC);
+    }
+    if (threadIdx.x == 0) s_ctr = 0;
+    __syncthreads();
+    for (;;) {
+      int rr = 0;
+      if (lane == 0) rr = atomicAdd(&s_ctr, 1);
+      rr = __shfl_sync(0xffffffffu, rr, 0);
+      if (rr >= nr) break;
+      const int64_t idw = r0 + rr;
+      const T* __restrict__ vcol = a.v + col0;  // + src*dimup per external hop
+      const T* tcol = tile + lane * VEC;
+      const int64_t e0 = idw * dimup + col0;
+      const int cnt = s_cnt[rr];
+      const uint32_t* hs = s_src + rr * kDwHops;
+      const T* hvv = s_val + rr * kDwHops;
+      T acc[NSEG][VEC];
+#pragma unroll
+      for (int g = 0; g < NSEG; ++g) {
+        if (!act[g]) continue;
+        const int64_t c = col0 + g * SEGW;
+        if (FIRST) {
+          const T edw = s_edw[rr];
+          const uint32_t mdw = s_mdw[rr];
+          T x[VEC];
+          VecLds<T, VEC>::load(tcol + size_t(rr) * SLAB + g * SEGW, x);
+#pragma unroll
+          for (int r = 0; r < VEC; ++r) {
+            const T d = a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw));
+            acc[g][r] = (SCALED ? T(double(d) * sc) : d) * x[r];
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < VEC; ++r) acc[g][r] = a.hv[e0 + g * SEGW + r];
+        }
+      }
+      for (int k = 0; k < cnt; k += KU) {
+        T x[KU][NSEG][VEC];
+#pragma unroll
+        for (int u = 0; u < KU; ++u) {
+          const int kk = k + u < cnt ? k + u : k;
+          const uint32_t sr = hs[kk];
+          const uint32_t lr = sr - r0;
+          if (lr < uint32_t(nr)) {
+            const T* t = tcol + size_t(lr) * SLAB;
+#pragma unroll
+            for (int g = 0; g < NSEG; ++g) VecLds<T, VEC>::load(t + g * SEGW, x[u][g]);
+          } else {
+            const T* __restrict__ src = vcol + int64_t(sr) * dimup;
+#pragma unroll
+            for (int g = 0; g < NSEG; ++g)
+              if (act[g]) VecLd<T, VEC>::load(src + g * SEGW, x[u][g]);
+          }
         }
 #pragma unroll
         for (int u = 0; u < KU; ++u) {
@@ -804,8 +1096,9 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   auto kern = per_sm == 2 ? k_up_smem<T, RT, FIRST, UNIFORM, LZ, false> : k_up_smem<T, RT, FIRST, UNIFORM, LZ, true>;
   if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
-  const int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
-  kern<<<int(g), 1024, smem, st>>>(a, sl, nrb);
+  int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
+  if (LZ && g > kRedBlocks) g = kRedBlocks;  // one partial per block in the reduction scratch
+  kern<<<dim3(int(g), a.ncols), 1024, smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   if (grid) *grid = int(g);
   return EDG_OK;
@@ -819,6 +1112,23 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
   const bool v2 = (a.dimup % 2 == 0) && (reinterpret_cast<uintptr_t>(a.v) % (2 * sizeof(T)) == 0) &&
                   (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
   const int vec = v2 ? 2 : 1;
+  const SpinBasis::RowBlocks* rb = (a.dwv == 1 || a.dwv == 2) ? &Bdw.rowblk[a.dwv - 1] : nullptr;
+  if (rb && Bdw.max_row <= kDwHops && rb->count > 0) {
+    constexpr int NSEG = sizeof(T) == 4 ? 4 : 2;
+    constexpr int KU = sizeof(T) == 4 ? 3 : 4;
+    const int slabw = 32 * vec * NSEG;
+    const size_t smem = size_t(rb->max_rows) * (size_t(slabw) * sizeof(T) + kDwHops * (sizeof(T) + 4) + sizeof(T) + 8) + 16;
+    const int nt = a.dwv == 2 ? 512 : 1024;
+    if (smem <= (nt == 512 ? kUpSmemTwoPerSM : kUpSmemOnePerSM)) {
+      auto kern = nt == 512 ? (v2 ? k_dw_blk<T, 2, NSEG, KU, FIRST, SCALED, 512> : k_dw_blk<T, 1, NSEG, KU, FIRST, SCALED, 512>)
+                            : (v2 ? k_dw_blk<T, 2, NSEG, KU, FIRST, SCALED, 1024> : k_dw_blk<T, 1, NSEG, KU, FIRST, SCALED, 1024>);
+      EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      const int64_t nslab = (a.dimup + slabw - 1) / slabw;
+      kern<<<dim3(rb->count, a.ncols), nt, smem, st>>>(a, rb->off.p, nslab);
+      EDG_CUDA(cudaGetLastError());
+      return EDG_OK;
+    }
+  }
   if (Bdw.max_row <= kDwHops && Bdw.groups > 0) {
     // FP32: 4 float2 segments per lane (256 columns per slab); FP64: 2 double2 segments
     constexpr int NSEG = sizeof(T) == 4 ? 4 : 2;
@@ -827,12 +1137,12 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
     const size_t smem = size_t(Bdw.group_max) * (kDwHops * (sizeof(T) + 4) + sizeof(T) + 12) + 16;
     if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const int64_t nslab = (a.dimup + 32 * vec * NSEG - 1) / (32 * vec * NSEG);
-    kern<<<Bdw.groups, 256, smem, st>>>(a, Bdw.group_off.p, Bdw.group_rows.p, nslab);
+    kern<<<dim3(Bdw.groups, a.ncols), 256, smem, st>>>(a, Bdw.group_off.p, Bdw.group_rows.p, nslab);
     EDG_CUDA(cudaGetLastError());
     return EDG_OK;
   }
-  if (SCALED) {
-    set_error("fused Lanczos H x v needs the grouped down pass");
+  if (SCALED || a.ncols > 1) {
+    set_error("fused Lanczos and block H x V need the grouped down pass");
     return EDG_ERR_UNSUPPORTED;
   }
   const int64_t nslab = (a.dimup + 32 * vec - 1) / (32 * vec);
@@ -845,11 +1155,50 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
   return EDG_OK;
 }
 
+// Packed-schedule FP32 up pass (k_up_p16); returns false when the sector has no packed table.
+template <bool LZ>
+bool launch_up_p16(const HxvArgs<float>& a, const SpinBasis& B, cudaStream_t st, int sms, int* status) {
+  if (B.p16_negoff == 0 || (a.upv != 1 && a.upv != 2)) return false;
+  const bool neg = a.upv == 1;
+  P16Args q;
+  q.ent = neg ? B.p16_ent.p : B.p16f_ent.p;
+  q.off = B.p16_off.p;
+  q.h = float(B.sell_h);
+  q.negoff = B.p16_negoff;
+  const size_t smem = neg ? size_t(B.p16_negoff + a.dimup + kUpZeroSlots) * sizeof(float2)
+                          : size_t(a.dimup + kUpZeroSlots) * sizeof(float2);
+  if (smem > kUpSmemOnePerSM) return false;
+  const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
+  auto kern = neg ? (per_sm == 2 ? k_up_p16<true, false, LZ> : k_up_p16<true, true, LZ>)
+                  : (per_sm == 2 ? k_up_p16<false, false, LZ> : k_up_p16<false, true, LZ>);
+  *status = EDG_OK;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) {
+    set_error("k_up_p16: %s", cudaGetErrorString(e));
+    *status = EDG_ERR_CUDA;
+    return true;
+  }
+  const int64_t nrb = (a.dimdw + 1) / 2;
+  int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
+  if (LZ && g > kRedBlocks) g = kRedBlocks;
+  kern<<<dim3(int(g), a.ncols), 1024, smem, st>>>(a, q, nrb);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("k_up_p16: %s", cudaGetErrorString(e));
+    *status = EDG_ERR_CUDA;
+  }
+  return true;
+}
+
 template <typename T, bool FIRST, bool LZ>
 int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms, int* grid) {
+  if constexpr (std::is_same<T, float>::value && !FIRST) {
+    int status = EDG_OK;
+    if (launch_up_p16<LZ>(a, B, st, sms, &status)) return status;
+  }
   const int rt = up_rows_per_cta(a.dimup, sizeof(T));
   if (rt == 0) {
-    if (LZ) {
+    if (LZ || a.ncols > 1) {
       set_error("fused Lanczos H x v needs the shared-memory up pass");
       return EDG_ERR_UNSUPPORTED;
     }
@@ -915,6 +1264,8 @@ HxvArgs<T> make_args(edg_sector_s* s, const T* v, T* hv) {
   a.map_up = s->up.map.p;
   a.map_dw = s->dw.map.p;
   a.U = T(s->U);
+  a.dwv = s->hxv_dw[sizeof(T) == 4];
+  a.upv = sizeof(T) == 4 ? s->hxv_up[1] : 0;
   return a;
 }
 
@@ -983,11 +1334,11 @@ template int hxv_apply<float>(edg_sector_s*, const float*, float*);
 template int hxv_apply<double>(edg_sector_s*, const double*, double*);
 
 // Lanczos-fused H x v (stored form): with v = u / bn[j], writes w = H v - (bn[j]/bn[j-1]) uprev
-// into `w` and per-block partials of <v, w> into `partial` (*nblocks of them). Returns
+// into `w` and <v, w> into *aout (`partial`: a reduction scratch of kRedSlots doubles). Returns
 // EDG_ERR_UNSUPPORTED when the sector needs one of the general kernels instead.
 template <typename T>
 int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double* bn, int j, double* partial,
-                 int* nblocks) {
+                 double* aout) {
   if (s->cplx || s->form != EDG_FORM_STORED || up_rows_per_cta(s->up.dim, sizeof(T)) == 0 ||
       s->dw.max_row > kDwHops || s->dw.groups == 0) {
     set_error("fused Lanczos H x v not available for this sector");
@@ -998,17 +1349,130 @@ int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double
   a.jstep = j;
   a.uprev = uprev;
   a.partial = partial;
+  a.red_out = aout;
   const int sms = sm_count();
   EDG_CHECK((dw_pass<T, true, true>(a, s->dw, s->stream, sms)));
-  EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nblocks)));
+  EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nullptr)));
   return EDG_OK;
 }
 bool hxv_lz_available(const edg_sector_s* s, size_t elem) {
   return !s->cplx && s->form == EDG_FORM_STORED && up_rows_per_cta(s->up.dim, elem) > 0 &&
          s->dw.max_row <= kDwHops && s->dw.groups > 0;
 }
-template int hxv_apply_lz<float>(edg_sector_s*, const float*, const float*, float*, const double*, int, double*, int*);
+template <typename T>
+int hxv_block(edg_sector_s* s, int ncols, const int* active, const T* v, T* hv) {
+  if (!hxv_lz_available(s, sizeof(T))) {
+    set_error("block H x V not available for this sector");
+    return EDG_ERR_UNSUPPORTED;
+  }
+  HxvArgs<T> a = make_args<T>(s, v, hv);
+  a.vstride = s->vlen;
+  a.active = active;
+  a.ncols = ncols;
+  const int sms = sm_count();
+  EDG_CHECK((dw_pass<T, true, false>(a, s->dw, s->stream, sms)));
+  EDG_CHECK((up_pass<T, false, false>(a, s->up, s->stream, sms, nullptr)));
+  return EDG_OK;
+}
+
+template <typename T>
+int hxv_block_lz(edg_sector_s* s, int ncols, const int* active, const T* u, const T* uprev, T* w, const double* bn,
+                 int64_t sstride, int j, double* partial, double* aout) {
+  if (!hxv_lz_available(s, sizeof(T))) {
+    set_error("block H x V not available for this sector");
+    return EDG_ERR_UNSUPPORTED;
+  }
+  HxvArgs<T> a = make_args<T>(s, u, w);
+  a.bn = bn;
+  a.jstep = j;
+  a.uprev = uprev;
+  a.partial = partial;
+  a.red_out = aout;
+  a.vstride = s->vlen;
+  a.sstride = sstride;
+  a.active = active;
+  a.ncols = ncols;
+  const int sms = sm_count();
+  EDG_CHECK((dw_pass<T, true, true>(a, s->dw, s->stream, sms)));
+  EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nullptr)));
+  return EDG_OK;
+}
+// Autotuner: every down-pass x up-pass pair (3 x 3 for FP32, 3 x 1 for FP64; a pair whose
+// kernel does not apply to the sector falls back to the default kernel and times like it) on
+// `reps` H x v of scratch vectors after one untimed application, timed with CUDA events on
+// the sector's stream; the fastest pair becomes the sector's choice for precision T. Its
+// arithmetic is unchanged in FP64 (every pair gives the same bits); in FP32 the packed up
+// passes sum the terms of a row in another order.
+template <typename T>
+int hxv_autotune(edg_sector_s* s, int reps, double* ms, int* nc, int* best) {
+  if (s->cplx || s->form != EDG_FORM_STORED) {
+    set_error("edg_sector_autotune: only the real stored form has kernel variants");
+    return EDG_ERR_UNSUPPORTED;
+  }
+  const int nup = sizeof(T) == 4 ? 3 : 1;
+  const int ncand = 3 * nup;
+  cudaStream_t st = s->stream;
+  DevBuf<T> x, y;
+  EDG_CHECK(x.alloc(size_t(s->vlen), st, "autotune vectors"));
+  EDG_CHECK(y.alloc(size_t(s->vlen), st, "autotune vectors"));
+  DevBuf<double> r;
+  EDG_CHECK(r.alloc(size_t(s->vlen), st, "autotune vectors"));
+  EDG_CHECK(random_dev(st, r.p, s->vlen, 12345));
+  EDG_CHECK((convert_dev<T, double>(st, x.p, r.p, s->vlen, 1.0)));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EDG_CUDA(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    set_error("edg_sector_autotune: cudaEventCreate failed");
+    return EDG_ERR_CUDA;
+  }
+  const int keep_dw = s->hxv_dw[sizeof(T) == 4], keep_up = s->hxv_up[sizeof(T) == 4];
+  int status = EDG_OK, arg = 0;
+  double tbest = 1e300;
+  for (int cnd = 0; cnd < ncand && status == EDG_OK; ++cnd) {
+    s->hxv_dw[sizeof(T) == 4] = cnd / nup;
+    s->hxv_up[sizeof(T) == 4] = cnd % nup;
+    status = hxv_apply<T>(s, x.p, y.p);  // untimed: first launch of the pair
+    float t = 0.f;
+    if (status == EDG_OK && cudaEventRecord(e0, st) != cudaSuccess) status = EDG_ERR_CUDA;
+    for (int k = 0; k < reps && status == EDG_OK; ++k) status = hxv_apply<T>(s, x.p, y.p);
+    if (status == EDG_OK && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                             cudaEventElapsedTime(&t, e0, e1) != cudaSuccess))
+      status = EDG_ERR_CUDA;
+    const double per = double(t) / (reps > 0 ? reps : 1);
+    if (ms) ms[cnd] = per;
+    if (status == EDG_OK && per < tbest) {
+      tbest = per;
+      arg = cnd;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status != EDG_OK) {
+    s->hxv_dw[sizeof(T) == 4] = keep_dw;
+    s->hxv_up[sizeof(T) == 4] = keep_up;
+    if (status == EDG_ERR_CUDA) set_error("edg_sector_autotune: timing failed");
+    return status;
+  }
+  s->hxv_dw[sizeof(T) == 4] = arg / nup;
+  s->hxv_up[sizeof(T) == 4] = arg % nup;
+  if (nc) *nc = ncand;
+  if (best) *best = arg;
+  return EDG_OK;
+}
+template int hxv_autotune<float>(edg_sector_s*, int, double*, int*, int*);
+template int hxv_autotune<double>(edg_sector_s*, int, double*, int*, int*);
+
+template int hxv_block<float>(edg_sector_s*, int, const int*, const float*, float*);
+template int hxv_block<double>(edg_sector_s*, int, const int*, const double*, double*);
+template int hxv_block_lz<float>(edg_sector_s*, int, const int*, const float*, const float*, float*, const double*,
+                                 int64_t, int, double*, double*);
+template int hxv_block_lz<double>(edg_sector_s*, int, const int*, const double*, const double*, double*,
+                                  const double*, int64_t, int, double*, double*);
+
+template int hxv_apply_lz<float>(edg_sector_s*, const float*, const float*, float*, const double*, int, double*,
+                                 double*);
 template int hxv_apply_lz<double>(edg_sector_s*, const double*, const double*, double*, const double*, int, double*,
-                                  int*);
+                                  double*);
 
 }  // namespace edg

@@ -29,7 +29,7 @@ namespace edg {
 namespace {
 
 struct Scalars {
-  double* partial;  // [kRedBlocks]
+  double* partial;  // [kRedSlots]: reduction partials and the fused finish's counter
   double* a;        // [cap+2]
   double* b;        // [cap+2], b[0] = 0 (Lanczos b's)
   double* bn;       // [cap+2], norms of the unnormalised vectors, bn[0] = 1 (fused form)
@@ -38,10 +38,10 @@ struct Scalars {
 };
 
 int scalars(edg_sector_s* s, int cap, Scalars* sc) {
-  const size_t need = size_t(kRedBlocks) + 3 * size_t(cap + 2) + 8;
+  const size_t need = size_t(kRedSlots) + 3 * size_t(cap + 2) + 8;
   EDG_CHECK(s->red.alloc(need, s->stream, "reduction scratch"));
   sc->partial = s->red.p;
-  sc->a = sc->partial + kRedBlocks;
+  sc->a = sc->partial + kRedSlots;
   sc->b = sc->a + cap + 2;
   sc->bn = sc->b + cap + 2;
   sc->tmp = sc->bn + cap + 2;
@@ -52,6 +52,13 @@ int scalars(edg_sector_s* s, int cap, Scalars* sc) {
   EDG_CUDA(cudaStreamSynchronize(s->stream));  // `one` is a stack value
   return EDG_OK;
 }
+
+template <typename T>
+DevBuf<T>* block_buf(edg_sector_s* s);
+template <>
+DevBuf<double>* block_buf<double>(edg_sector_s* s) { return &s->blk64; }
+template <>
+DevBuf<float>* block_buf<float>(edg_sector_s* s) { return &s->blk32; }
 
 template <typename T>
 DevBuf<T>* work(edg_sector_s* s);
@@ -110,9 +117,7 @@ struct Recurrence {
     const int64_t n = s->vlen;
     cudaStream_t st = s->stream;
     if (fused) {
-      int nb = 0;
-      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, &nb));
-      EDG_CHECK(finish_dev(st, sc.partial, nb, sc.a + j, 0));
+      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, sc.a + j));
       EDG_CHECK(lanczos_step_b2<T>(st, W, U, sc.a + j, sc.bn + j, n, sc.partial, sc.bn + j + 1));
     } else {
       EDG_CHECK(hxv_apply<T>(s, U, W));
@@ -128,9 +133,7 @@ struct Recurrence {
     const int64_t n = s->vlen;
     cudaStream_t st = s->stream;
     if (fused) {
-      int nb = 0;
-      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, &nb));
-      EDG_CHECK(finish_dev(st, sc.partial, nb, sc.a + j, 0));
+      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, sc.a + j));
       EDG_CHECK(lanczos_step_b2<T>(st, W, U, sc.a + j, sc.bn + j, n, sc.partial, sc.bn + j + 1));
     } else {
       EDG_CHECK(hxv_apply<T>(s, U, W));
@@ -211,6 +214,103 @@ int tridiag_t(edg_sector_s* s, const double* dv0, int nlanc, double threshold, d
         if (j + 1 < nlanc) blanc[j + 1] = 0.0;
         return EDG_OK;
       }
+    }
+  }
+  return EDG_OK;
+}
+
+// k chains in lockstep with the fused recurrence of Recurrence<T> applied to every column:
+// one launch per pass for all columns (block H x V, then the per-column w/a and u/b passes).
+// Column c's arithmetic is that of a single chain, so its coefficients equal
+// tridiag_t<T>'s bit for bit. A column stops at its first b below threshold: the host reads
+// every column's scalars once per kChunk steps and clears the column's device flag, and
+// the steps queued after the stop in that chunk are discarded.
+// start(c) returns column c's FP64 start vector on the device (valid until the next call).
+template <typename T, typename Start>
+int tridiag_block_t(edg_sector_s* s, int k, const Start& start, int nlanc, double threshold, double* alanc,
+                    double* blanc, double* norm2, int* nsteps) {
+  const int64_t n = s->vlen;
+  cudaStream_t st = s->stream;
+  const int64_t sstride = nlanc + 2;  // per-column scalar arrays a[], bn[]
+  DevBuf<T>& blk = *block_buf<T>(s);
+  EDG_CHECK(blk.alloc(size_t(3) * k * n, st, "block Lanczos vectors"));
+  const size_t nred = size_t(k) * kRedSlots + 2 * size_t(k) * sstride + size_t(k);
+  EDG_CHECK(s->blkred.alloc(nred, st, "block Lanczos scalars"));
+  EDG_CHECK(s->blkact.alloc(size_t(k), st, "block Lanczos flags"));
+  double* partial = s->blkred.p;
+  double* A = partial + size_t(k) * kRedSlots;
+  double* BN = A + size_t(k) * sstride;
+  double* N2 = BN + size_t(k) * sstride;
+  EDG_CUDA(cudaMemsetAsync(s->blkred.p, 0, nred * sizeof(double), st));
+  for (int c = 0; c < k; ++c) {
+    nsteps[c] = 0;
+    for (int j = 0; j < nlanc; ++j) alanc[size_t(c) * nlanc + j] = blanc[size_t(c) * nlanc + j] = 0.0;
+  }
+  T* U = blk.p;
+  T* P = U + size_t(k) * n;
+  T* W = P + size_t(k) * n;
+  // each column's norm, then v_0 = start / |start| in precision T, one column at a time (the
+  // start vectors may be produced into one shared buffer)
+  for (int c = 0; c < k; ++c) {
+    const double* x0 = nullptr;
+    EDG_CHECK(start(c, &x0));
+    EDG_CHECK(dot_dev<double>(st, x0, x0, n, partial, N2 + c));
+    EDG_CHECK((normalise_cols<T, double>(st, 1, U + size_t(c) * n, n, x0, n, N2 + c, 1, n)));
+  }
+  std::vector<double> n2(k), one(k, 1.0);
+  EDG_CUDA(cudaMemcpyAsync(n2.data(), N2, k * sizeof(double), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  std::vector<int> act(k);
+  int nact = 0;
+  for (int c = 0; c < k; ++c) {
+    norm2[c] = n2[c];
+    act[c] = (n2[c] > 0.0 && nlanc > 0) ? 1 : 0;
+    nact += act[c];
+  }
+  if (nact == 0) return EDG_OK;
+  EDG_CUDA(cudaMemsetAsync(P, 0, size_t(k) * n * sizeof(T), st));
+  EDG_CUDA(cudaMemcpy2DAsync(BN, sstride * sizeof(double), one.data(), sizeof(double), sizeof(double), k,
+                             cudaMemcpyHostToDevice, st));  // bn[c][0] = 1
+  EDG_CUDA(cudaMemcpyAsync(s->blkact.p, act.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+  EDG_CUDA(cudaStreamSynchronize(st));  // host staging arrays are read by the copies above
+  constexpr int kChunk = 16;
+  std::vector<double> ha(size_t(k) * kChunk), hb(size_t(k) * kChunk);
+  for (int j0 = 0; j0 < nlanc && nact > 0; j0 += kChunk) {
+    const int j1 = std::min(nlanc, j0 + kChunk);
+    for (int j = j0; j < j1; ++j) {
+      EDG_CHECK(hxv_block_lz<T>(s, k, s->blkact.p, U, P, W, BN, sstride, j, partial, A + j));
+      EDG_CHECK(lanczos_step_b2_cols<T>(st, k, s->blkact.p, W, U, n, A + j, BN + j, partial, BN + j + 1, sstride, n));
+      T* t = P;
+      P = U;
+      U = W;
+      W = t;
+    }
+    const int m = j1 - j0;
+    EDG_CUDA(cudaMemcpy2DAsync(ha.data(), m * sizeof(double), A + j0, sstride * sizeof(double), m * sizeof(double), k,
+                               cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaMemcpy2DAsync(hb.data(), m * sizeof(double), BN + j0 + 1, sstride * sizeof(double),
+                               m * sizeof(double), k, cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+    bool changed = false;
+    for (int c = 0; c < k; ++c) {
+      if (!act[c]) continue;
+      for (int j = j0; j < j1; ++j) {
+        const double b = hb[size_t(c) * m + (j - j0)];
+        alanc[size_t(c) * nlanc + j] = ha[size_t(c) * m + (j - j0)];
+        nsteps[c] = j + 1;
+        if (j + 1 < nlanc) blanc[size_t(c) * nlanc + j + 1] = b;
+        if (!(b >= threshold)) {  // also stops on NaN
+          if (j + 1 < nlanc) blanc[size_t(c) * nlanc + j + 1] = 0.0;
+          act[c] = 0;
+          --nact;
+          changed = true;
+          break;
+        }
+      }
+    }
+    if (changed && nact > 0) {
+      EDG_CUDA(cudaMemcpyAsync(s->blkact.p, act.data(), k * sizeof(int), cudaMemcpyHostToDevice, st));
+      EDG_CUDA(cudaStreamSynchronize(st));
     }
   }
   return EDG_OK;
@@ -353,6 +453,49 @@ int tridiag_dev(edg_sector_s* s, const double* dv0, int nlanc, double threshold,
                 double* blanc, double* norm2, int* nsteps) {
   if (precision == EDG_PREC_F32) return tridiag_t<float>(s, dv0, nlanc, threshold, alanc, blanc, norm2, nsteps);
   return tridiag_t<double>(s, dv0, nlanc, threshold, alanc, blanc, norm2, nsteps);
+}
+
+int tridiag_block_fn(edg_sector_s* s, int k, const StartFn& start, int nlanc, double threshold, int precision,
+                     double* alanc, double* blanc, double* norm2, int* nsteps) {
+  const size_t elem = precision == EDG_PREC_F32 ? sizeof(float) : sizeof(double);
+  if (k <= 0) return EDG_OK;
+  if (!hxv_lz_available(s, elem) || nlanc <= 0) {  // one chain after another
+    for (int c = 0; c < k; ++c) {
+      const double* x0 = nullptr;
+      EDG_CHECK(start(c, &x0));
+      EDG_CHECK(tridiag_dev(s, x0, nlanc, threshold, precision, alanc + size_t(c) * nlanc, blanc + size_t(c) * nlanc,
+                            norm2 + c, nsteps + c));
+    }
+    return EDG_OK;
+  }
+  // columns per block: three vectors each, within the free HBM less 2 GB
+  size_t fr = 0, tot = 0;
+  EDG_CUDA(cudaMemGetInfo(&fr, &tot));
+  const size_t per = 3 * size_t(s->vlen) * elem;
+  const size_t reserve = size_t(2) << 30;
+  int kb = fr > reserve ? int(std::min<size_t>(size_t(k), (fr - reserve) / per)) : 0;
+  if (kb < 1) kb = 1;
+  for (int c0 = 0; c0 < k; c0 += kb) {
+    const int kk = std::min(kb, k - c0);
+    auto sub = [&](int c, const double** x) -> int { return start(c0 + c, x); };
+    double* a = alanc + size_t(c0) * nlanc;
+    double* b = blanc + size_t(c0) * nlanc;
+    if (precision == EDG_PREC_F32)
+      EDG_CHECK(tridiag_block_t<float>(s, kk, sub, nlanc, threshold, a, b, norm2 + c0, nsteps + c0));
+    else
+      EDG_CHECK(tridiag_block_t<double>(s, kk, sub, nlanc, threshold, a, b, norm2 + c0, nsteps + c0));
+  }
+  return EDG_OK;
+}
+
+int tridiag_block(edg_sector_s* s, int k, const double* dv0, int nlanc, double threshold, int precision,
+                  double* alanc, double* blanc, double* norm2, int* nsteps) {
+  const int64_t n = s->vlen;
+  StartFn start = [dv0, n](int c, const double** x) -> int {
+    *x = dv0 + size_t(c) * n;
+    return EDG_OK;
+  };
+  return tridiag_block_fn(s, k, start, nlanc, threshold, precision, alanc, blanc, norm2, nsteps);
 }
 
 int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,

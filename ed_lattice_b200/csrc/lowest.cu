@@ -369,13 +369,15 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   }
   // device: basis Q[mmax][n], w, scratch
   DevBuf<double> Q, X;
-  DevBuf<double> w, part, coef, Zd;
+  DevBuf<double> w, part, coef, Zd, nred;
   EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
   EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
-  size_t npart = kRedBlocks;  // also the norm's scratch
+  size_t npart = 1;
   for (int mm = 1; mm <= mmax; ++mm)
     npart = std::max(npart, size_t(2) * mm * dot_shape(mm, cplx ? ne : n).nsplit());
   EDG_CHECK(part.alloc(npart, st, "multi-dot partials"));
+  EDG_CHECK(nred.alloc(kRedSlots, st, "norm reduction scratch"));  // the norms' own scratch
+  EDG_CHECK(red_scratch_reset(st, nred.p));
   EDG_CHECK(coef.alloc(3 * size_t(mmax) + 8, st, "multi-dot coefficients"));
   DevBuf<double> Gm;  // Gram matrix Q^T Q of the basis (real sectors)
   if (!cplx) EDG_CHECK(Gm.alloc(size_t(mmax) * mmax, st, "Gram matrix"));
@@ -389,7 +391,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
   EDG_CHECK(dab.alloc(2 * size_t(mmax) + 4, st, "Lanczos scalars"));
   double* dA = dab.p;
   double* dB = dab.p + mmax + 1;
-  EDG_CHECK(norm_dev(st, Q.p, n, part.p, dB));
+  EDG_CHECK(norm_dev(st, Q.p, n, nred.p, dB));
   double nrm = 0.0;
   EDG_CUDA(cudaMemcpyAsync(&nrm, dB, sizeof(double), cudaMemcpyDeviceToHost, st));
   EDG_CUDA(cudaStreamSynchronize(st));
@@ -436,7 +438,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
       k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p + 2 * m1, m1, n, w.p);
     }
     EDG_CUDA(cudaGetLastError());
-    EDG_CHECK(norm_dev(st, w.p, n, part.p, dB + j + 1));
+    EDG_CHECK(norm_dev(st, w.p, n, nred.p, dB + j + 1));
     m = j + 1;
     if ((m >= k && m >= next_check) || m == mmax || m == ne) {
       EDG_CUDA(cudaMemcpyAsync(hA.data(), dA, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));

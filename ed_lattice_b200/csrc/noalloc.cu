@@ -30,8 +30,8 @@ namespace {
 
 constexpr int64_t kNoAllocMaxDim = int64_t(1) << 20;
 constexpr int kNoAllocMaxLanc = 1024;
-constexpr int64_t kNoAllocScalars = 4096;  // partials [kRedBlocks] + a [cap] + b [cap+1] + slots
-static_assert(kRedBlocks + 2 * (kNoAllocMaxLanc + 1) + 8 <= kNoAllocScalars, "scalar area too small");
+constexpr int64_t kNoAllocScalars = 4096;  // reduction scratch [kRedSlots] + a [cap] + b [cap+1] + slots
+static_assert(kRedSlots + 2 * (kNoAllocMaxLanc + 1) + 8 <= kNoAllocScalars, "scalar area too small");
 
 // The scratch: [V | P | W] vectors of kNoAllocMaxDim doubles, then the scalar area.
 __device__ __align__(256) double g_noalloc_scratch[3 * kNoAllocMaxDim + kNoAllocScalars];
@@ -89,12 +89,14 @@ extern "C" int edg_tridiag_dev_f64_noalloc(edg_sector* s, const double* dvinit, 
   double* P = base + kNoAllocMaxDim;
   double* W = base + 2 * kNoAllocMaxDim;
   double* partial = base + 3 * kNoAllocMaxDim;
-  double* A = partial + kRedBlocks;
+  double* A = partial + kRedSlots;
   double* B = A + nlanc + 1;  // b[0] = 0, b[j+1] written by step j; B[nlanc+1] holds norm2
   for (int j = 0; j < nlanc; ++j) { alanc[j] = 0.0; blanc[j] = 0.0; }
   *nsteps = 0;
   // the array keeps the previous call's contents: clear the scalar slots read before written
+  // and the reduction's arrival counter
   EDG_CUDA(cudaMemsetAsync(A, 0, size_t(2 * (nlanc + 1) + 2) * sizeof(double), st));
+  EDG_CHECK(red_scratch_reset(st, partial));
   EDG_CHECK(dot_dev<double>(st, dvinit, dvinit, n, partial, B + nlanc + 1));
   double n2 = 0.0;
   EDG_CUDA(cudaMemcpyAsync(&n2, B + nlanc + 1, sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -13,6 +13,7 @@
 #include <cstdint>
 
 #include "common.cuh"
+#include "reduce.cuh"
 
 namespace edg {
 namespace {
@@ -31,6 +32,18 @@ __device__ __forceinline__ double block_sum(double v) {
   return r;  // valid in thread 0
 }
 
+// Block mode: blockIdx.y is a column of a block of vectors (vectors vstride elements apart,
+// device scalars sstride apart, reduction scratch kRedSlots apart); a column whose active[c]
+// is 0 is skipped. Single-vector launches pass Cols{} (gridDim.y == 1).
+struct Cols {
+  int64_t vstride = 0, sstride = 0;
+  const int* active = nullptr;
+};
+__device__ __forceinline__ bool col_on(const Cols& k) { return !k.active || k.active[blockIdx.y]; }
+__device__ __forceinline__ int64_t col_v(const Cols& k) { return int64_t(blockIdx.y) * k.vstride; }
+__device__ __forceinline__ int64_t col_s(const Cols& k) { return int64_t(blockIdx.y) * k.sstride; }
+__device__ __forceinline__ int64_t col_r(const Cols&) { return int64_t(blockIdx.y) * kRedSlots; }
+
 // Grid-stride loops below take kUnr elements per thread per trip (indices i + u*stride, each
 // coalesced across the warp) with all loads issued before the arithmetic, so that every
 // thread keeps several HBM requests in flight; the order of the partial sums is fixed.
@@ -38,7 +51,13 @@ constexpr int kUnr = 4;
 
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ x, const T* __restrict__ y, int64_t n,
-                                                     double* __restrict__ partial) {
+                                                     double* __restrict__ partial, double* __restrict__ out,
+                                                     int do_sqrt, Cols cl) {
+  if (!col_on(cl)) return;
+  x += col_v(cl);
+  y += col_v(cl);
+  partial += col_r(cl);
+  out += col_s(cl);
   const int64_t st = int64_t(gridDim.x) * blockDim.x;
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
   double s = 0.0;
@@ -55,6 +74,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dot(const T* __restrict__ x, co
   for (; i < n; i += st) s = __fma_rn(double(x[i]), double(y[i]), s);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  finish_in_last_block(partial, gridDim.x, out, do_sqrt);
 }
 
 // out = sum(partial) (do_sqrt: sqrt of the sum)
@@ -69,7 +89,15 @@ __global__ void __launch_bounds__(kRedThreads) k_finish(const double* __restrict
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_step_a(T* __restrict__ w, const T* __restrict__ vprev,
                                                         const T* __restrict__ v, const double* __restrict__ bprev,
-                                                        int64_t n, double* __restrict__ partial) {
+                                                        int64_t n, double* __restrict__ partial,
+                                                        double* __restrict__ out, Cols cl) {
+  if (!col_on(cl)) return;
+  w += col_v(cl);
+  vprev += col_v(cl);
+  v += col_v(cl);
+  bprev += col_s(cl);
+  partial += col_r(cl);
+  out += col_s(cl);
   const double b = *bprev;
   const int64_t st = int64_t(gridDim.x) * blockDim.x;
   int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
@@ -96,6 +124,7 @@ __global__ void __launch_bounds__(kRedThreads) k_step_a(T* __restrict__ w, const
   }
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  finish_in_last_block(partial, gridDim.x, out, 0);
 }
 
 // w <- w - coef * x, returning this thread's partial sum of |w|^2
@@ -205,20 +234,36 @@ __device__ __forceinline__ double dot_v(const T* __restrict__ x, const T* __rest
 
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_dot_v(const T* __restrict__ x, const T* __restrict__ y, int64_t nv,
-                                                       double* __restrict__ partial) {
+                                                       double* __restrict__ partial, double* __restrict__ out,
+                                                       int do_sqrt, Cols cl) {
+  if (!col_on(cl)) return;
+  x += col_v(cl);
+  y += col_v(cl);
+  partial += col_r(cl);
+  out += col_s(cl);
   double s = dot_v<T>(x, y, nv);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  finish_in_last_block(partial, gridDim.x, out, do_sqrt);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_step_b2_v(T* __restrict__ w, const T* __restrict__ u,
                                                            const double* __restrict__ a,
                                                            const double* __restrict__ bn, int64_t nv,
-                                                           double* __restrict__ partial) {
+                                                           double* __restrict__ partial, double* __restrict__ out,
+                                                           Cols cl) {
+  if (!col_on(cl)) return;
+  w += col_v(cl);
+  u += col_v(cl);
+  a += col_s(cl);
+  bn += col_s(cl);
+  partial += col_r(cl);
+  out += col_s(cl);
   double s = axpy_norm_v<T>(w, u, *a / *bn, nv);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  finish_in_last_block(partial, gridDim.x, out, 1);
 }
 
 template <typename T>
@@ -229,10 +274,18 @@ bool vec16_ok(int64_t n, const void* p, const void* q) {
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_step_b(T* __restrict__ w, const T* __restrict__ v,
                                                         const double* __restrict__ a, int64_t n,
-                                                        double* __restrict__ partial) {
+                                                        double* __restrict__ partial, double* __restrict__ out,
+                                                        Cols cl) {
+  if (!col_on(cl)) return;
+  w += col_v(cl);
+  v += col_v(cl);
+  a += col_s(cl);
+  partial += col_r(cl);
+  out += col_s(cl);
   double s = axpy_norm<T>(w, v, *a, n);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  finish_in_last_block(partial, gridDim.x, out, 1);
 }
 
 // Fused recurrence, second half: u_{j+1} = w - (a_j / bn_j) u_j in place on w, and the
@@ -240,10 +293,19 @@ __global__ void __launch_bounds__(kRedThreads) k_step_b(T* __restrict__ w, const
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_step_b2(T* __restrict__ w, const T* __restrict__ u,
                                                          const double* __restrict__ a, const double* __restrict__ bn,
-                                                         int64_t n, double* __restrict__ partial) {
+                                                         int64_t n, double* __restrict__ partial,
+                                                         double* __restrict__ out, Cols cl) {
+  if (!col_on(cl)) return;
+  w += col_v(cl);
+  u += col_v(cl);
+  a += col_s(cl);
+  bn += col_s(cl);
+  partial += col_r(cl);
+  out += col_s(cl);
   double s = axpy_norm<T>(w, u, *a / *bn, n);
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  finish_in_last_block(partial, gridDim.x, out, 1);
 }
 
 // dst[i] = T(src[i] * scale); dst and src do not overlap
@@ -262,7 +324,12 @@ __device__ __forceinline__ void scale_copy(TD* __restrict__ dst, const TS* __res
 }
 
 template <typename T>
-__global__ void k_scale_into(T* __restrict__ dst, const T* __restrict__ src, const double* __restrict__ b, int64_t n) {
+__global__ void k_scale_into(T* __restrict__ dst, const T* __restrict__ src, const double* __restrict__ b, int64_t n,
+                             Cols cl) {
+  if (!col_on(cl)) return;
+  dst += col_v(cl);
+  src += col_v(cl);
+  b += col_s(cl);
   const double bb = *b;
   scale_copy<T, T>(dst, src, n, bb != 0.0 ? 1.0 / bb : 0.0);
 }
@@ -270,6 +337,15 @@ __global__ void k_scale_into(T* __restrict__ dst, const T* __restrict__ src, con
 template <typename TD, typename TS>
 __global__ void k_convert(TD* __restrict__ dst, const TS* __restrict__ src, int64_t n, double scale) {
   scale_copy<TD, TS>(dst, src, n, scale);
+}
+
+// dst_c = TD(src_c / sqrt(norm2[c])) for every column (zero when norm2[c] is 0)
+template <typename TD, typename TS>
+__global__ void k_normalise_cols(TD* __restrict__ dst, int64_t dstride, const TS* __restrict__ src, int64_t sstride_v,
+                                 const double* __restrict__ norm2, int64_t sstride, int64_t n) {
+  const double n2 = norm2[int64_t(blockIdx.y) * sstride];
+  scale_copy<TD, TS>(dst + int64_t(blockIdx.y) * dstride, src + int64_t(blockIdx.y) * sstride_v, n,
+                     n2 > 0.0 ? 1.0 / sqrt(n2) : 0.0);
 }
 
 // x[i] *= scale in place
@@ -345,10 +421,9 @@ uint64_t splitmix64(uint64_t x) { return splitmix64_d(x); }
 template <typename T>
 int dot_dev(cudaStream_t st, const T* x, const T* y, int64_t n, double* partial, double* out) {
   if (vec16_ok<T>(n, x, y))
-    k_dot_v<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n / V16<T>::K, partial);
+    k_dot_v<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n / V16<T>::K, partial, out, 0, Cols{});
   else
-    k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n, partial);
-  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, out, 0);
+    k_dot<T><<<kRedBlocks, kRedThreads, 0, st>>>(x, y, n, partial, out, 0, Cols{});
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -356,16 +431,14 @@ int dot_dev(cudaStream_t st, const T* x, const T* y, int64_t n, double* partial,
 template <typename T>
 int lanczos_step_a(cudaStream_t st, T* w, const T* vprev, const T* v, const double* bprev, int64_t n, double* partial,
                    double* aout) {
-  k_step_a<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, vprev, v, bprev, n, partial);
-  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, aout, 0);
+  k_step_a<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, vprev, v, bprev, n, partial, aout, Cols{});
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
 
 template <typename T>
 int lanczos_step_b(cudaStream_t st, T* w, const T* v, const double* a, int64_t n, double* partial, double* bout) {
-  k_step_b<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, v, a, n, partial);
-  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, bout, 1);
+  k_step_b<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, v, a, n, partial, bout, Cols{});
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -374,21 +447,24 @@ template <typename T>
 int lanczos_step_b2(cudaStream_t st, T* w, const T* u, const double* a, const double* bn, int64_t n, double* partial,
                     double* bn_next) {
   if (vec16_ok<T>(n, w, u))
-    k_step_b2_v<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n / V16<T>::K, partial);
+    k_step_b2_v<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n / V16<T>::K, partial, bn_next, Cols{});
   else
-    k_step_b2<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n, partial);
-  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, bn_next, 1);
+    k_step_b2<T><<<kRedBlocks, kRedThreads, 0, st>>>(w, u, a, bn, n, partial, bn_next, Cols{});
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
 
 int norm_dev(cudaStream_t st, const double* x, int64_t n, double* partial, double* out) {
   if (vec16_ok<double>(n, x, x))
-    k_dot_v<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n / V16<double>::K, partial);
+    k_dot_v<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n / V16<double>::K, partial, out, 1, Cols{});
   else
-    k_dot<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n, partial);
-  k_finish<<<1, kRedThreads, 0, st>>>(partial, kRedBlocks, out, 1);
+    k_dot<double><<<kRedBlocks, kRedThreads, 0, st>>>(x, x, n, partial, out, 1, Cols{});
   EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+int red_scratch_reset(cudaStream_t st, double* partial) {
+  EDG_CUDA(cudaMemsetAsync(partial + kRedBlocks, 0, sizeof(double), st));
   return EDG_OK;
 }
 
@@ -400,7 +476,7 @@ int finish_dev(cudaStream_t st, const double* partial, int nblk, double* out, in
 
 template <typename T>
 int scale_into(cudaStream_t st, T* dst, const T* src, const double* b, int64_t n) {
-  k_scale_into<T><<<grid_for(n), 256, 0, st>>>(dst, src, b, n);
+  k_scale_into<T><<<grid_for(n), 256, 0, st>>>(dst, src, b, n, Cols{});
   EDG_CUDA(cudaGetLastError());
   return EDG_OK;
 }
@@ -445,6 +521,74 @@ int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed) {
   return EDG_OK;
 }
 
+// ---- block forms: ncols columns, vectors vstride elements apart, device scalars sstride
+// apart, reduction scratch kRedSlots apart per column; inactive columns skipped
+inline dim3 col_grid(int nblk, int ncols) { return dim3(nblk, ncols); }
+
+template <typename T>
+int dot_cols(cudaStream_t st, int ncols, const T* x, const T* y, int64_t n, int64_t vstride, double* partial,
+             double* out, int64_t sstride, int do_sqrt) {
+  Cols cl{vstride, sstride, nullptr};
+  if (vec16_ok<T>(n, x, y) && vstride % V16<T>::K == 0)
+    k_dot_v<T><<<col_grid(kRedBlocks, ncols), kRedThreads, 0, st>>>(x, y, n / V16<T>::K, partial, out, do_sqrt, cl);
+  else
+    k_dot<T><<<col_grid(kRedBlocks, ncols), kRedThreads, 0, st>>>(x, y, n, partial, out, do_sqrt, cl);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename TD, typename TS>
+int normalise_cols(cudaStream_t st, int ncols, TD* dst, int64_t dstride, const TS* src, int64_t srcstride,
+                   const double* norm2, int64_t sstride, int64_t n) {
+  int g = grid_for(n) / ncols;
+  if (g < 1) g = 1;
+  k_normalise_cols<TD, TS><<<col_grid(g, ncols), 256, 0, st>>>(dst, dstride, src, srcstride, norm2, sstride, n);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int lanczos_step_a_cols(cudaStream_t st, int ncols, const int* active, T* w, const T* vprev, const T* v,
+                        int64_t vstride, const double* bprev, double* partial, double* aout, int64_t sstride, int64_t n) {
+  k_step_a<T><<<col_grid(kRedBlocks, ncols), kRedThreads, 0, st>>>(w, vprev, v, bprev, n, partial, aout,
+                                                                  Cols{vstride, sstride, active});
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int lanczos_step_b_cols(cudaStream_t st, int ncols, const int* active, T* w, const T* v, int64_t vstride,
+                        const double* a, double* partial, double* bout, int64_t sstride, int64_t n) {
+  k_step_b<T><<<col_grid(kRedBlocks, ncols), kRedThreads, 0, st>>>(w, v, a, n, partial, bout,
+                                                                  Cols{vstride, sstride, active});
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int lanczos_step_b2_cols(cudaStream_t st, int ncols, const int* active, T* w, const T* u, int64_t vstride,
+                         const double* a, const double* bn, double* partial, double* bn_next, int64_t sstride,
+                         int64_t n) {
+  const Cols cl{vstride, sstride, active};
+  if (vec16_ok<T>(n, w, u) && vstride % V16<T>::K == 0)
+    k_step_b2_v<T><<<col_grid(kRedBlocks, ncols), kRedThreads, 0, st>>>(w, u, a, bn, n / V16<T>::K, partial, bn_next,
+                                                                       cl);
+  else
+    k_step_b2<T><<<col_grid(kRedBlocks, ncols), kRedThreads, 0, st>>>(w, u, a, bn, n, partial, bn_next, cl);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
+template <typename T>
+int scale_into_cols(cudaStream_t st, int ncols, const int* active, T* dst, const T* src, int64_t vstride,
+                    const double* b, int64_t sstride, int64_t n) {
+  int g = grid_for(n) / ncols;
+  if (g < 1) g = 1;
+  k_scale_into<T><<<col_grid(g, ncols), 256, 0, st>>>(dst, src, b, n, Cols{vstride, sstride, active});
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
 #define EDG_INST(T)                                                                                        \
   template int dot_dev<T>(cudaStream_t, const T*, const T*, int64_t, double*, double*);                   \
   template int lanczos_step_a<T>(cudaStream_t, T*, const T*, const T*, const double*, int64_t, double*,   \
@@ -453,7 +597,19 @@ int random_dev(cudaStream_t st, double* dst, int64_t n, uint64_t seed) {
   template int scale_into<T>(cudaStream_t, T*, const T*, const double*, int64_t);                         \
   template int lanczos_step_b2<T>(cudaStream_t, T*, const T*, const double*, const double*, int64_t,      \
                                   double*, double*);                                                      \
-  template int axpy_accum_dev<T>(cudaStream_t, double*, const T*, double, int64_t);
+  template int axpy_accum_dev<T>(cudaStream_t, double*, const T*, double, int64_t);                         \
+  template int dot_cols<T>(cudaStream_t, int, const T*, const T*, int64_t, int64_t, double*, double*, int64_t,  \
+                           int);                                                                           \
+  template int lanczos_step_a_cols<T>(cudaStream_t, int, const int*, T*, const T*, const T*, int64_t,     \
+                                      const double*, double*, double*, int64_t, int64_t);                  \
+  template int lanczos_step_b_cols<T>(cudaStream_t, int, const int*, T*, const T*, int64_t, const double*, \
+                                      double*, double*, int64_t, int64_t);                                 \
+  template int lanczos_step_b2_cols<T>(cudaStream_t, int, const int*, T*, const T*, int64_t, const double*, \
+                                       const double*, double*, double*, int64_t, int64_t);                 \
+  template int scale_into_cols<T>(cudaStream_t, int, const int*, T*, const T*, int64_t, const double*,     \
+                                  int64_t, int64_t);                                                       \
+  template int normalise_cols<T, double>(cudaStream_t, int, T*, int64_t, const double*, int64_t,           \
+                                         const double*, int64_t, int64_t);
 EDG_INST(float)
 EDG_INST(double)
 #undef EDG_INST

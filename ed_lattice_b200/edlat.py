@@ -218,6 +218,20 @@ class Sector:
         L.check(L.lib().edg_hxv_d(self.handle, v.size, _pd(v), _pd(hv)), "spHtimesV")
         return hv
 
+    def autotune(self, precision: int = L.EDG_PREC_F32, reps: int = 5) -> dict:
+        """Time the H x v kernel variants on this sector and keep the fastest for `precision`
+        (edg_sector_autotune): {"ms": per-candidate ms per H x v, "best": index kept}."""
+        ms = np.zeros(9)
+        nc, best = C.c_int(), C.c_int()
+        L.check(L.lib().edg_sector_autotune(self.handle, precision, reps, _pd(ms), C.byref(nc), C.byref(best)),
+                "edg_sector_autotune")
+        return {"ms": ms[: nc.value].tolist(), "best": best.value}
+
+    def release_work(self) -> None:
+        """Hand the sector's work buffers (Lanczos vectors, FP32 basis, block vectors) back to
+        the library's pool; tables and the state buffer stay."""
+        L.check(L.lib().edg_sector_release_work(self.handle), "edg_sector_release_work")
+
     def set_stream(self, stream: int | None) -> None:
         """Run the sector's device work on `stream` (a cudaStream_t as an int; None = the legacy default stream)."""
         L.check(L.lib().edg_sector_set_stream(self.handle, C.c_void_p(stream)), "edg_sector_set_stream")
@@ -396,6 +410,48 @@ def gf_chain(from_sector: Sector, to_sector: Sector, op: int, site: int, spin: i
     L.check(L.lib().edg_gf_chain(from_sector.handle, to_sector.handle, op, site, site2, spin, nlanc, precision, ei,
                                  _pd(p), _pd(w), C.byref(n2), C.byref(n)), "gf_chain")
     return Spectrum(p[: n.value].copy(), w[: n.value].copy(), n2.value)
+
+
+def _block_out(k, nlanc):
+    return (np.zeros(k * nlanc), np.zeros(k * nlanc), np.zeros(k), np.zeros(k, dtype=np.int32))
+
+
+def _spectra(k, nlanc, p, w, n2, n):
+    return [Spectrum(p[c * nlanc: c * nlanc + n[c]].copy(), w[c * nlanc: c * nlanc + n[c]].copy(), float(n2[c]))
+            for c in range(k)]
+
+
+def gf_chain_block(from_sector: Sector, to_sector: Sector, op: int, sites, spin: int, nlanc: int, ei: float,
+                   sites2=None, precision: int = L.EDG_PREC_F64) -> list:
+    """The chains c^+_{sites[c]} (op=+1) or c_{sites[c]} (op=-1) of one state into one target
+    sector as one block (block H x V; edg_gf_chain_block): the inner loop of
+    lanc_build_gf_electrons_diag/_mix over sites (src/GF/GF_ELECTRONS.f90:202-405) with
+    add_to_lanczos_gf_normal per chain (:417-457). Returns one Spectrum per site."""
+    si = np.ascontiguousarray(sites, dtype=np.int32)
+    k = si.size
+    s2 = np.ascontiguousarray(sites2, dtype=np.int32) if sites2 is not None else None
+    p, w, n2, n = _block_out(k, nlanc)
+    L.check(L.lib().edg_gf_chain_block(from_sector.handle, to_sector.handle, op, k, si.ctypes.data_as(L._pi),
+                                       s2.ctypes.data_as(L._pi) if s2 is not None else None, spin, nlanc, precision,
+                                       ei, _pd(p), _pd(w), _pd(n2), n.ctypes.data_as(L._pi)), "gf_chain_block")
+    return _spectra(k, nlanc, p, w, n2, n)
+
+
+def chi_chain_block(sector: Sector, nlanc: int, ei: float, kind: int = 0, sites=None, sites2=None, qcos=None,
+                    precision: int = L.EDG_PREC_F64) -> list:
+    """Susceptibility chains of one state as one block (edg_chi_chain_block): kind 0 = S^z,
+    1 = N, one chain per site of `sites` (+ sites2), or per row of qcos [k, Ns] (momentum
+    combinations). add_to_lanczos_spinChi per chain (src/CHI/CHI_SPIN_ELECTRONS.f90:305-366)."""
+    q = np.ascontiguousarray(qcos, dtype=np.float64) if qcos is not None else None
+    si = np.ascontiguousarray(sites, dtype=np.int32) if sites is not None else None
+    s2 = np.ascontiguousarray(sites2, dtype=np.int32) if sites2 is not None else None
+    k = q.shape[0] if q is not None else si.size
+    p, w, n2, n = _block_out(k, nlanc)
+    L.check(L.lib().edg_chi_chain_block(sector.handle, kind, k, si.ctypes.data_as(L._pi) if si is not None else None,
+                                        s2.ctypes.data_as(L._pi) if s2 is not None else None,
+                                        _pd(q.ravel()) if q is not None else None, nlanc, precision, ei, _pd(p), _pd(w),
+                                        _pd(n2), n.ctypes.data_as(L._pi)), "chi_chain_block")
+    return _spectra(k, nlanc, p, w, n2, n)
 
 
 def chi_chain(sector: Sector, site: int, nlanc: int, ei: float, kind: int = 0, site2: int = 0, qcos=None,

@@ -34,11 +34,12 @@ import numpy as np
 
 from . import _edgpu_lib as L
 from .diag import StateList, _allgather, _rank_world
-from .edlat import (Model, Sector, Spectrum, chi_chain, drude_weight, eval_chi, eval_oc, eval_poles, gf_chain,
-                    oc_chain)
+from .edlat import (Model, Sector, Spectrum, chi_chain, chi_chain_block, drude_weight, eval_chi, eval_oc, eval_poles,
+                    gf_chain, gf_chain_block, oc_chain)
 
 LANC_NGFITER = 200  # LANC_NGFITER default (src/INPUT_VARS.f90:161)
 STATE_THREADS = 4   # host threads that run the chains of different states at once
+BLOCK_WIDTH = 16    # chains of one state and target sector run as blocks of at most this many
 
 
 def get_cdg_sector(model: Model, ispin: int, isector: int) -> int:
@@ -88,6 +89,25 @@ class _DeviceChains:
         src = self.load(isector, vec)
         dst = self.sector(jsector)
         return gf_chain(src, dst, op, io, ispin, min(nlanc, dst.dim), ei, site2=jo, precision=self.precision)
+
+    def gf_block(self, isector, vec, jsector, op, ios, jos, ispin, nlanc, ei) -> list:
+        """The chains (ios[c], jos[c]) of one state into jsector as blocks of BLOCK_WIDTH
+        (block H x V); the same spectra as one __call__ per chain."""
+        src = self.load(isector, vec)
+        dst = self.sector(jsector)
+        out = []
+        for c0 in range(0, len(ios), BLOCK_WIDTH):
+            out += gf_chain_block(src, dst, op, ios[c0:c0 + BLOCK_WIDTH], ispin, min(nlanc, dst.dim), ei,
+                                  sites2=jos[c0:c0 + BLOCK_WIDTH], precision=self.precision)
+        return out
+
+    def chi_block(self, isector, vec, sites, kind, nlanc, ei) -> list:
+        sec = self.load(isector, vec)
+        out = []
+        for c0 in range(0, len(sites), BLOCK_WIDTH):
+            out += chi_chain_block(sec, min(nlanc, sec.dim), ei, kind=kind, sites=sites[c0:c0 + BLOCK_WIDTH],
+                                   precision=self.precision)
+        return out
 
     def close(self):
         for s in self.sectors.values():
@@ -190,6 +210,18 @@ def build_gf_electrons(model: Model, state_list: StateList, nlanc: int = LANC_NG
         out = {}
         for ispin in range(1, model.nspin + 1):
             jp, jh = get_cdg_sector(model, ispin, st.sector), get_c_sector(model, ispin, st.sector)
+            if not chain_fn:  # the device runs the chains of each target sector as blocks
+                ios = [io for io, _ in pairs]
+                jos = [0 if io == jo else jo for io, jo in pairs]
+                per_op = []
+                for jsec, op in ((jp, +1), (jh, -1)):
+                    if jsec == 0:
+                        per_op.append([Spectrum(np.zeros(0), np.zeros(0), 0.0)] * len(pairs))
+                    else:
+                        per_op.append(dev.gf_block(st.sector, st.vec, jsec, op, ios, jos, ispin, nlanc, st.e))
+                for c, (io, jo) in enumerate(pairs):
+                    out[(ispin, io, jo)] = [per_op[0][c], per_op[1][c]]
+                continue
             for io, jo in pairs:
                 chans = []
                 for jsec, op in ((jp, +1), (jh, -1)):
@@ -282,14 +314,10 @@ def build_chi(model: Model, state_list: StateList, kind: int = 0, nlanc: int = L
         threads = 1 if chain_fn else STATE_THREADS
 
     def run(istate, st, dev):
-        res = {}
-        for io in range(1, model.ns + 1):
-            if chain_fn:
-                res[io] = [chain_fn(st.sector, st.vec, io, nlanc, st.e)]
-            else:
-                sec = dev.load(st.sector, st.vec)
-                res[io] = [chi_chain(sec, io, min(nlanc, sec.dim), st.e, kind=kind, precision=precision)]
-        return res
+        if not chain_fn:  # one block of chains over the sites
+            sites = list(range(1, model.ns + 1))
+            return {io: [ch] for io, ch in zip(sites, dev.chi_block(st.sector, st.vec, sites, kind, nlanc, st.e))}
+        return {io: [chain_fn(st.sector, st.vec, io, nlanc, st.e)] for io in range(1, model.ns + 1)}
 
     keep = 8
     if not chain_fn:

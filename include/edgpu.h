@@ -101,6 +101,11 @@ int edg_sector_get_maps(const edg_sector* s, int32_t* map_up, int32_t* map_dw);
  * NULL arrays to get *nnz only. */
 int edg_sector_get_hops(const edg_sector* s, int spin, int64_t* rowptr, int32_t* cols,
                         double* vals, int64_t* nnz);
+/* Hand back the sector's work buffers (Lanczos vectors, the FP32 ground-state basis, block
+ * chain vectors) to the library's pool, keeping its tables and its state buffer: between a
+ * ground state and the response chains of a sector whose vectors take tens of GB. Later
+ * calls allocate again on demand. No counterpart in the reference. */
+int edg_sector_release_work(edg_sector* s);
 /* Run this sector's work on a caller-owned stream (cudaStream_t passed as void*). */
 int edg_sector_set_stream(edg_sector* s, void* stream);
 
@@ -116,6 +121,18 @@ int edg_sector_set_stream(edg_sector* s, void* stream);
 int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv);
 /* Same on real host vectors (real Hij only). */
 int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv);
+/* Autotuner of the stored-form H x v (real Hij): times each candidate pair of down-spin and
+ * up-spin pass kernels (3 x 3 for FP32 vectors, 3 x 1 for FP64) on `reps` applications to
+ * scratch vectors of this sector (after one untimed application each), with CUDA events on
+ * the sector's stream, and keeps the fastest pair for that precision: the H x v, the fused
+ * Lanczos steps and the block chains of this sector then use it. Candidate k = 3*down + up:
+ * down 0 hop-balanced row groups, 1 block-staged rows (one CTA per SM), 2 block-staged rows
+ * (two CTAs per SM); up 0 32-bit SELL schedule, 1 packed 16-bit schedule with negated
+ * copies, 2 packed 16-bit schedule with sign bits. ms (may be NULL) receives each candidate's
+ * ms per H x v, *ncand their number, *best the index kept. FP64 results are the same bits for
+ * every pair; FP32 packed up passes change the order of a row's terms. Untuned sectors use
+ * candidate 0. No counterpart in the reference. */
+int edg_sector_autotune(edg_sector* s, int precision, int reps, double* ms, int* ncand, int* best);
 /* Device-resident forms (vectors in HBM, reference layout); stream-ordered, no sync. */
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv);
 int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv);
@@ -252,12 +269,43 @@ int edg_eval_poles(int64_t npoles, const double* poles, const double* weights, i
                    const double* z_re, const double* z_im, double* out_re, double* out_im);
 
 /* Batched chains: k start vectors of one sector in one call, each tridiagonalised as by
- * edg_tridiag_dev_f64 (one alpha/beta sequence per column). The chains run one after
- * another, each H x v using the whole GPU; a block H x V over several vectors would gather
- * the same bytes per vector, so it is not used. dvinit: k device vectors, column c at
- * dvinit + c*dim. alanc/blanc/norm2: [k][nlanc] row-major per column; nsteps[k]. */
+ * edg_tridiag_dev_f64 (one alpha/beta sequence per column, equal bit for bit to a single
+ * chain's). The k chains run in lockstep as one block: every pass (the H x V and the fused
+ * recurrence) is one launch over all columns still running, a column stops at its first
+ * b < threshold, and k is split into blocks whose 3k work vectors fit in free HBM. Sectors
+ * without the fused stored-form passes (direct form, complex Hij, rows beyond shared memory)
+ * run the chains one after another. Replaces the per-chain calls of tridiag_Hv_sector in the
+ * GF/CHI builders (src/GF/GF_ELECTRONS.f90:202-290, src/CHI/CHI_SPIN_ELECTRONS.f90:189-233).
+ * dvinit: k device vectors, column c at dvinit + c*vlen. alanc/blanc: [k][nlanc] row-major;
+ * norm2[k]; nsteps[k]. */
 int edg_tridiag_block_dev(edg_sector* s, int k, const double* dvinit, int nlanc, double threshold,
                           int precision, double* alanc, double* blanc, double* norm2, int* nsteps);
+/* k Green's-function chains of one state into one target sector as a block: for chain c the
+ * excitation c^+_{sites[c]} (op=+1) or c_{sites[c]} (op=-1) of spin `spin` on the state
+ * buffer of `from`, plus the same operator on sites2[c] when sites2 != NULL and
+ * sites2[c] > 0 (the (c_i + c_j) vectors of lanc_build_gf_electrons_mix,
+ * src/GF/GF_ELECTRONS.f90:343-353); then edg_tridiag_block_dev (threshold 1e-9) and the
+ * poles op*(theta_j - ei) and weights norm2*Z(1,j)^2 of add_to_lanczos_gf_normal
+ * (src/GF/GF_ELECTRONS.f90:417-457), the tridiagonal eigenproblems solved on the device (one
+ * implicit-QL thread per chain). poles/weights: [k][nlanc]; nout[k] entries valid per chain. */
+int edg_gf_chain_block(const edg_sector* from, edg_sector* to, int op, int k, const int* sites,
+                       const int* sites2, int spin, int nlanc, int precision, double ei, double* poles,
+                       double* weights, double* norm2, int* nout);
+/* k susceptibility chains of the state buffer of s as a block (add_to_lanczos_spinChi,
+ * src/CHI/CHI_SPIN_ELECTRONS.f90:305-366): operator of chain c = kind (0 Sz, 1 N) on
+ * sites[c] (+ sites2[c]), or, when qcos != NULL, the momentum combination with site weights
+ * qcos[c*ns .. c*ns+ns) (sites ignored). Poles theta_j - ei, weights norm2*Z(1,j)^2, as
+ * edg_gf_chain_block. */
+int edg_chi_chain_block(edg_sector* s, int kind, int k, const int* sites, const int* sites2,
+                        const double* qcos, int nlanc, int precision, double ei, double* poles,
+                        double* weights, double* norm2, int* nout);
+/* Poles and weights of k chains from their coefficients ([k][nlanc] host arrays in the
+ * blanc(1)-unused convention, nsteps[k] valid steps each): the eigenproblems of
+ * add_to_lanczos_gf_normal solved on the current device, one implicit-QL thread per chain
+ * (src/GF/GF_ELECTRONS.f90:445-456); poles isign*(theta_j - ei), weights norm2[c]*Z(1,j)^2. */
+int edg_poles_weights_block(int k, int nlanc, const double* alanc, const double* blanc,
+                            const double* norm2, const int* nsteps, double ei, int isign,
+                            double* poles, double* weights);
 
 /* Tridiagonal eigenproblem (SF_LINALG eigh(diag,subdiag,Ev) as used at
  * src/GF/GF_ELECTRONS.f90:447): FP64 implicit QL, eigenvalues ascending; z1 receives the
