@@ -11,7 +11,10 @@
 The eigenpairs of each sector come from the device: edg_lowest_k for the sp_eigh (ARPACK)
 branch, edg_ground_state for lanc_method="lanczos", and for dim <= lanc_dim_threshold the dense
 sector matrix of edg_sector_dense_dev handed to the device dense eigensolver (the LAPACK
-branch). ed_twin (twin-sector symmetry) is not supported: every sector is visited.
+branch). With ed_twin (DiagParams.ed_twin) only the sectors with Nup >= Ndw are solved; each
+state of a sector with Nup != Ndw enters the list with a vectorless twin in (Ndw, Nup),
+whose vector is the transpose of its partner's DimDw x DimUp matrix (twin_sector_order,
+src/SECTOR.f90:507-554).
 
 Sectors are independent, so the device solves several at once: a pool of host threads takes
 them largest first, each on its own library stream, and a sector starts only when the HBM
@@ -34,12 +37,33 @@ from .edlat import Model, Sector, sp_lanc_eigh
 
 
 # ----------------------------------------------------------------------------- state list
-@dataclass
 class EState:
-    e: float
-    vec: np.ndarray | None
-    sector: int
-    owner: int = 0  # rank that holds the vector
+    """One entry of the state list (sparse_estate, src/EIGENSPACE.f90:16-25). A twin entry
+    (itwin) carries no vector of its own: its vector is the spin-flipped copy of its partner's,
+    the transpose of the partner's DimDw x DimUp matrix without any sign (es_return_cvector,
+    src/EIGENSPACE.f90:490-510, with twin_sector_order / flip_state, src/SECTOR.f90:507-554),
+    built on first use and kept."""
+
+    __slots__ = ("e", "_vec", "sector", "owner", "twin", "partner", "shape")
+
+    def __init__(self, e: float, vec, sector: int, owner: int = 0, twin: bool = False, partner=None,
+                 shape: tuple[int, int] | None = None):
+        self.e, self._vec, self.sector, self.owner = e, vec, sector, owner
+        self.twin, self.partner, self.shape = twin, partner, shape  # shape: the partner's (DimUp, DimDw)
+
+    @property
+    def vec(self):
+        if self.twin and self._vec is None and self.partner is not None:
+            pv = self.partner.vec
+            if pv is None:
+                return None
+            dup, ddw = self.shape
+            self._vec = np.ascontiguousarray(np.asarray(pv).reshape(ddw, dup).T).ravel()
+        return self._vec
+
+    @vec.setter
+    def vec(self, v):
+        self._vec = v
 
 
 class StateList:
@@ -60,32 +84,47 @@ class StateList:
     def size(self) -> int:
         return len(self.states)
 
-    def insert_state(self, e: float, vec, sector: int, owner: int = 0) -> None:
-        """es_insert_state (src/EIGENSPACE.f90:198-247): before the first entry with e <= E."""
+    def insert_state(self, e: float, vec, sector: int, owner: int = 0, twin=None) -> None:
+        """es_insert_state (src/EIGENSPACE.f90:198-247): before the first entry with e <= E.
+        twin = (twin sector, (DimUp, DimDw) of `sector`) also inserts, right after it, the
+        vectorless twin entry of the same energy."""
         pos = bisect.bisect_left(self._energies, e)
-        self.states.insert(pos, EState(float(e), vec, sector, owner))
+        st = EState(float(e), vec, sector, owner)
+        self.states.insert(pos, st)
         self._energies.insert(pos, float(e))
+        if twin is not None:
+            self.states.insert(pos + 1, EState(float(e), None, twin[0], owner, True, st, twin[1]))
+            self._energies.insert(pos + 1, float(e))
         self.emax = max(self.emax, e)
         self.emin = min(self.emin, e)
 
-    def add_state(self, e: float, vec, sector: int, size: int | None = None, owner: int = 0) -> None:
+    def add_state(self, e: float, vec, sector: int, size: int | None = None, owner: int = 0, twin=None) -> None:
         """es_add_state (src/EIGENSPACE.f90:167-190): with `size`, a full list takes a new state
-        only if it lies below the last one, which is dropped."""
+        only if it lies below the last one, which is dropped (with its twin)."""
         if size is None or self.size < size:
-            self.insert_state(e, vec, sector, owner)
+            self.insert_state(e, vec, sector, owner, twin)
         elif e < self.energy():
             self.pop_state()
-            self.insert_state(e, vec, sector, owner)
+            self.insert_state(e, vec, sector, owner, twin)
 
     def pop_state(self, n: int | None = None) -> None:
-        """es_pop_state: remove the n-th (default last) state (src/EIGENSPACE.f90:260-332)."""
+        """es_pop_state: remove the n-th (default last) state (src/EIGENSPACE.f90:260-332); a
+        twin pair goes together: a twin entry takes its partner (the entry before it) along,
+        and an entry followed by its twin takes the twin along."""
         if self.size == 0:
             raise L.EdgError(L.EDG_ERR_STATE, "es_pop_state", "empty list")
         pos = self.size if n is None else n
         if pos > self.size:
             raise L.EdgError(L.EDG_ERR_ARG, "es_pop_state", "pos > espace.size")
-        del self.states[pos - 1]
-        del self._energies[pos - 1]
+        i = pos - 1
+        if self.states[i].twin:
+            lo, hi = i - 1, i + 1
+        elif i + 1 < self.size and self.states[i + 1].twin:
+            lo, hi = i, i + 2
+        else:
+            lo, hi = i, i + 1
+        del self.states[lo:hi]
+        del self._energies[lo:hi]
 
     def free(self) -> None:
         """es_free_espace (src/EIGENSPACE.f90:136-153)."""
@@ -158,6 +197,7 @@ class DiagParams:
     lanc_tolerance: float = 1e-10    # LANC_TOLERANCE
     lanc_dim_threshold: int = 1024   # LANC_DIM_THRESHOLD
     lanc_nstates_total: int = 1      # set by setup()
+    ed_twin: bool = False            # ED_TWIN: solve Nup >= Ndw only, twins by spin flip
     sector_threads: int = 4          # sectors solved at once on one device (no reference key)
 
     def setup(self, nsectors: int) -> "DiagParams":
@@ -361,9 +401,15 @@ def diagonalize_lattice(model: Model, params: DiagParams, seed: int = 1234, solv
     params.setup(nsectors)
     finite_t = params.finite_temp
     visit = []
+    if params.ed_twin and model.nspin > 1:
+        import warnings
+
+        warnings.warn("using twin_sector with Nspin>1")  # the reference's warning (src/SETUP.f90:197-199)
     for isector in range(1, nsectors + 1):
         nup, ndw = model.get_nup(isector), model.get_ndw(isector)
         if model.ed_filling != 0 and nup + ndw != model.ed_filling:
+            continue
+        if params.ed_twin and nup < ndw:  # twin_mask (src/SETUP.f90:254-260)
             continue
         dim = math.comb(ns, nup) * math.comb(ns, ndw)
         neigen = 1 if params.lanc_method == "lanczos" else min(dim, params.lanc_nstates_sector)
@@ -389,18 +435,21 @@ def diagonalize_lattice(model: Model, params: DiagParams, seed: int = 1234, solv
         evals, owner = solved[isector]
         eig_list.append((isector, evals.copy(), lanc_solve))
         vecs = vectors.get(isector) if owner == rank else None
+        # Tflag (src/DIAG/DIAG.f90:136-137): the twin of a sector with Nup != Ndw
+        twin = (model.get_sector(ndw, nup), (math.comb(ns, nup), math.comb(ns, ndw))) \
+            if params.ed_twin and nup != ndw else None
         for i in range(neigen):
             vec = vecs[i] if vecs is not None else None
             e = float(evals[i])
             if finite_t:
-                state_list.add_state(e, vec, isector, size=params.lanc_nstates_total, owner=owner)
+                state_list.add_state(e, vec, isector, size=params.lanc_nstates_total, owner=owner, twin=twin)
             elif e < oldzero - 10.0 * params.gs_threshold:
                 oldzero = e
                 state_list.free()
-                state_list.add_state(e, vec, isector, owner=owner)
+                state_list.add_state(e, vec, isector, owner=owner, twin=twin)
             elif abs(e - oldzero) <= params.gs_threshold:
                 oldzero = min(oldzero, e)
-                state_list.add_state(e, vec, isector, owner=owner)
+                state_list.add_state(e, vec, isector, owner=owner, twin=twin)
     if finite_t:
         egs, ec = state_list.emin, state_list.emax
         if math.exp(-(ec - egs) / params.temp) > params.cutoff:

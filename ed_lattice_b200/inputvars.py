@@ -91,4 +91,5 @@ def diag_params(cfg: dict, lanc_tolerance: float | None = None) -> DiagParams:
     return DiagParams(finite_temp=bool(cfg["ED_FINITE_TEMP"]), temp=float(cfg["TEMP"]), cutoff=float(cfg["CUTOFF"]),
                       gs_threshold=float(cfg["GS_THRESHOLD"]), lanc_method=str(cfg["LANC_METHOD"]).lower(),
                       lanc_nstates_sector=int(cfg["LANC_NSTATES_SECTOR"]), lanc_niter=int(cfg["LANC_NITER"]),
-                      lanc_tolerance=tol, lanc_dim_threshold=int(cfg["LANC_DIM_THRESHOLD"]))
+                      lanc_tolerance=tol, lanc_dim_threshold=int(cfg["LANC_DIM_THRESHOLD"]),
+                      ed_twin=bool(cfg["ED_TWIN"]))

@@ -460,3 +460,58 @@ def test_device_plan_shrinks_with_sector_size(monkeypatch):
     sl2 = StateList()
     sl2.add_state(-1.0, np.zeros(1), big.get_sector(8, 8), size=10)
     assert gf._device_plan(big, sl2, 4) == (1, 3)  # 3 sectors of 13.25 GB fit in 50 GB, 6 do not
+
+
+def test_state_list_twin_pairs():
+    """es_insert_state with twin=.true. puts a vectorless twin of the same energy right after
+    the state; es_pop_state removes a twin pair together whichever of the two is hit, and a
+    capped list drops the pair at its end (src/EIGENSPACE.f90:198-332)."""
+    sl = StateList()
+    v = np.arange(6.0)  # a (DimUp=3) x (DimDw=2) sector vector, element iup + idw*3
+    sl.add_state(0.2, v, 7, twin=(9, (3, 2)))
+    sl.add_state(-0.1, None, 1)
+    sl.add_state(0.2, None, 4)
+    assert [(s.sector, s.twin) for s in sl.states] == [(1, False), (4, False), (7, False), (9, True)]
+    tw = sl.states[3]
+    assert tw.e == 0.2 and tw.partner is sl.states[2]
+    # twin vector: the transpose of the partner's matrix, element idw + iup*2
+    assert np.array_equal(tw.vec, v.reshape(2, 3).T.ravel())
+    assert np.array_equal(sl.vector(4), [0.0, 3.0, 1.0, 4.0, 2.0, 5.0])
+    sl.pop_state()                      # the last entry is a twin: its partner goes too
+    assert [s.sector for s in sl.states] == [1, 4]
+    sl.add_state(0.5, v, 7, twin=(9, (3, 2)))
+    sl.pop_state(3)                     # a state followed by its twin: both go
+    assert [s.sector for s in sl.states] == [1, 4]
+    sl.add_state(0.3, v, 7, twin=(9, (3, 2)), size=3)  # size 2 < 3: the pair goes in (size 4)
+    assert sl.size == 4
+    sl.add_state(0.0, None, 5, size=4)  # full: the pair at the end is dropped for the newcomer
+    assert [s.sector for s in sl.states] == [1, 5, 4]
+
+
+def test_twin_sectors_thermal_and_vectors():
+    """ED_TWIN: only Nup >= Ndw is solved; Z and the observables equal the run that visits
+    every sector, and each twin vector is an eigenvector of its own sector (spin flip)."""
+    H = _chain4()
+    m = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    om = O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
+    res = {}
+    for twin in (False, True):
+        p = DiagParams(finite_temp=True, temp=0.5, lanc_nstates_sector=36, ed_twin=twin)
+        sl, eigs = diagonalize_lattice(m, p, solver=_oracle_solver(om))
+        zeta = partition_function(sl, p)
+        res[twin] = (sl, eigs, zeta, lanc_observables(m, sl, zeta, p, observer=_oracle_observer))
+    sl, eigs, zeta, obs = res[True]
+    assert len(eigs) == 15  # Nup >= Ndw of the 25 sectors
+    assert all(m.get_nup(isec) >= m.get_ndw(isec) for isec, _, _ in eigs)
+    assert zeta == pytest.approx(res[False][2], rel=1e-12)
+    for k in obs:
+        assert np.allclose(obs[k], res[False][3][k], atol=1e-12), k
+    ntwin = 0
+    for st in sl.states:
+        if not st.twin:
+            continue
+        ntwin += 1
+        nup, ndw = m.get_nup(st.sector), m.get_ndw(st.sector)
+        hb = O.dense_h(om, nup, ndw)
+        assert np.abs(hb @ st.vec - st.e * st.vec).max() <= 1e-10
+    assert ntwin > 0
