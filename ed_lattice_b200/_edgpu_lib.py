@@ -27,6 +27,8 @@ EDG_PREC_F32 = 1
 EDG_GS_F64 = 0
 EDG_GS_F32_REFINE = 1
 EDG_GS_E0_ONLY = 0x100
+EDG_LK_F64 = 0
+EDG_LK_F32_REFINE = 1
 
 _i = C.c_int
 _i64 = C.c_int64
@@ -71,6 +73,7 @@ SIGNATURES = {
     "edg_ground_state_keep": (_i, [_p, _pd, _u64, _i, _d, _i, _pd, _pi]),
     "edg_ground_state_stats": (_i, [_p, _pi, _pi]),
     "edg_lowest_k": (_i, [_p, _i, _pd, _u64, _i, _d, _pd, _pd, _pd, _pi]),
+    "edg_lowest_k_mode": (_i, [_p, _i, _pd, _u64, _i, _d, _i, _pd, _pd, _pd, _pi]),
     "edg_sector_dense": (_i, [_p, _pd]),
     "edg_sector_dense_dev": (_i, [_p, _p]),
     "edg_state_get": (_i, [_p, _pd]),

@@ -432,15 +432,21 @@ int edg_ground_state(edg_sector* s, const double* v0, uint64_t seed, int maxit, 
   return EDG_OK;
 }
 
-int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol, double* evals,
-                 double* evecs, double* resid, int* niter) {
+int edg_lowest_k_mode(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol, int mode,
+                      double* evals, double* evecs, double* resid, int* niter) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(evals && niter, "edg_lowest_k: NULL output");
   EDG_ARG(k >= 1 && k <= 16, "edg_lowest_k: k=%d outside 1..16", k);
   EDG_ARG(maxit >= 1, "edg_lowest_k: maxit=%d", maxit);
   EDG_ARG(tol > 0.0 && std::isfinite(tol), "edg_lowest_k: tol must be > 0");
+  EDG_ARG(mode == EDG_LK_F64 || mode == EDG_LK_F32_REFINE, "edg_lowest_k: mode=%d", mode);
   EDG_ON_DEVICE(s->device);
-  return lowest_k(s, k, v0, seed, maxit, tol, evals, evecs, resid, niter);
+  return lowest_k(s, k, v0, seed, maxit, tol, mode, evals, evecs, resid, niter);
+}
+
+int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol, double* evals,
+                 double* evecs, double* resid, int* niter) {
+  return edg_lowest_k_mode(s, k, v0, seed, maxit, tol, EDG_LK_F64, evals, evecs, resid, niter);
 }
 
 int edg_sector_dense(edg_sector* s, double* h) {

@@ -383,7 +383,8 @@ int ground_state(edg_sector_s* s, const double* v0_host, uint64_t seed, int maxi
                  double* e0, int* niter);
 
 // ---- lowest.cu
-int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, double* evals,
+int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
+             double* evals,
              double* evecs_host, double* resid, int* niter);
 int sector_dense(edg_sector_s* s, double* H_host);
 int sector_dense_dev(edg_sector_s* s, double* dH);

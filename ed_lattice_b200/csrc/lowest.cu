@@ -14,6 +14,7 @@
 // lapack branch of ed_diag_d (src/DIAG/DIAG.f90:229-254).
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -34,9 +35,11 @@ constexpr int kDenseMaxDim = 16384;  // 2 GB dense matrix
 // basis at 5.8-6.2 TB/s for 112-224 columns (one right-hand side), where one element chunk
 // per block with the column groups shared out among its warps reached 3.3 TB/s. Fixed
 // summation order.
-template <int G>
-__global__ void __launch_bounds__(kLkThreads) k_multidot2(const double* __restrict__ Q, int m, int64_t n,
-                                                          const double* __restrict__ w, const double* __restrict__ x,
+// TQ: element type of the basis and of w, x (FP64, or FP32 for the FP32-bulk phase); the
+// products and sums are FP64 either way.
+template <int G, typename TQ>
+__global__ void __launch_bounds__(kLkThreads) k_multidot2(const TQ* __restrict__ Q, int m, int64_t n,
+                                                          const TQ* __restrict__ w, const TQ* __restrict__ x,
                                                           double* __restrict__ partial) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nsplit = gridDim.x * (kLkThreads / 32);
@@ -45,17 +48,17 @@ __global__ void __launch_bounds__(kLkThreads) k_multidot2(const double* __restri
   chunk = (chunk + 31) & ~int64_t(31);
   const int64_t i0 = split * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
   const int j0 = blockIdx.y * G;
-  const double* __restrict__ q[G];
+  const TQ* __restrict__ q[G];
 #pragma unroll
   for (int c = 0; c < G; ++c) q[c] = Q + int64_t(j0 + c < m ? j0 + c : m - 1) * n;
   double aw[G], ax[G];
 #pragma unroll
   for (int c = 0; c < G; ++c) aw[c] = ax[c] = 0.0;
   for (int64_t i = i0 + lane; i < i1; i += 32) {
-    const double wi = w[i], xi = x[i];
+    const double wi = double(w[i]), xi = double(x[i]);
 #pragma unroll
     for (int c = 0; c < G; ++c) {
-      const double qi = q[c][i];
+      const double qi = double(q[c][i]);
       aw[c] = __fma_rn(qi, wi, aw[c]);
       ax[c] = __fma_rn(qi, xi, ax[c]);
     }
@@ -123,14 +126,15 @@ DotShape dot_shape(int m, int64_t n) {
 }
 
 
-int launch_multidot2(const double* Q, int m, int64_t n, const double* w, const double* x, double* partial,
-                     cudaStream_t st, int* nsplit) {
+template <typename TQ>
+int launch_multidot2(const TQ* Q, int m, int64_t n, const TQ* w, const TQ* x, double* partial, cudaStream_t st,
+                     int* nsplit) {
   const DotShape d = dot_shape(m, n);
   const dim3 grid(d.gx, (m + d.G - 1) / d.G);
   if (d.G == 8)
-    k_multidot2<8><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, x, partial);
+    k_multidot2<8, TQ><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, x, partial);
   else
-    k_multidot2<4><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, x, partial);
+    k_multidot2<4, TQ><<<grid, kLkThreads, 0, st>>>(Q, m, n, w, x, partial);
   *nsplit = d.nsplit();
   return EDG_OK;
 }
@@ -229,29 +233,31 @@ __global__ void k_multifinish(const double* __restrict__ partial, int nblk, int 
   if (lane == 0) c[j] = t;
 }
 
-// w[i] -= sum_j c[j] Q[j][i]
-__global__ void __launch_bounds__(kLkThreads) k_multiaxpy(const double* __restrict__ Q, const double* __restrict__ c,
-                                                          int m, int64_t n, double* __restrict__ w) {
+// w[i] -= sum_j c[j] Q[j][i] (sums in FP64, one rounding to TQ per element)
+template <typename TQ>
+__global__ void __launch_bounds__(kLkThreads) k_multiaxpy(const TQ* __restrict__ Q, const double* __restrict__ c,
+                                                          int m, int64_t n, TQ* __restrict__ w) {
   __shared__ double sc[kMaxBasis];
   for (int j = threadIdx.x; j < m; j += blockDim.x) sc[j] = c[j];
   __syncthreads();
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    double t = w[i];
+    double t = double(w[i]);
 #pragma unroll 8
-    for (int j = 0; j < m; ++j) t = __fma_rn(-sc[j], Q[int64_t(j) * n + i], t);
-    w[i] = t;
+    for (int j = 0; j < m; ++j) t = __fma_rn(-sc[j], double(Q[int64_t(j) * n + i]), t);
+    w[i] = TQ(t);
   }
 }
 
 // X[r][i] = sum_j Z[j*m + r] Q[j][i], r < k (Z column-major m x m, first k columns)
-__global__ void __launch_bounds__(kLkThreads) k_ritz_k(const double* __restrict__ Q, const double* __restrict__ Z,
+template <typename TQ>
+__global__ void __launch_bounds__(kLkThreads) k_ritz_k(const TQ* __restrict__ Q, const double* __restrict__ Z,
                                                        int m, int k, int64_t n, double* __restrict__ X) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     double acc[kMaxK];
 #pragma unroll
     for (int r = 0; r < kMaxK; ++r) acc[r] = 0.0;
     for (int j = 0; j < m; ++j) {
-      const double q = Q[int64_t(j) * n + i];
+      const double q = double(Q[int64_t(j) * n + i]);
 #pragma unroll
       for (int r = 0; r < kMaxK; ++r)
         if (r < k) acc[r] = __fma_rn(Z[j + int64_t(r) * m], q, acc[r]);
@@ -338,173 +344,246 @@ int sector_dense(edg_sector_s* s, double* H_host) {
   return EDG_OK;
 }
 
+namespace {
+
 // Eigenvalues of T closer than this fraction of its spectral radius get their Ritz
 // coefficients from the QL eigenvector matrix (the twisted-factorisation vectors of such a
 // pair are accurate to about eps / kRitzRelGap only).
 constexpr double kRitzRelGap = 1e-5;
+// FP32-bulk phase: Ritz pairs to this relative residual before the FP64 refinement (FP32
+// vectors carry about 1e-7 relative rounding per H x v).
+constexpr double kTol32 = 1e-6;
 
-int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, double* evals,
-             double* evecs_host, double* resid, int* niter) {
+template <typename T>
+int norm_vec(cudaStream_t st, const T* x, int64_t n, double* scratch, double* out) {
+  return dot_cols<T>(st, 1, x, x, n, n, scratch, out, 1, 1);
+}
+
+// One Lanczos run with full reorthogonalisation in precision T (T = float only for real
+// sectors): basis Q, the tridiagonal (A, B), the residual data of the last test.
+template <typename T>
+struct LkRun {
+  DevBuf<T> Q, w;
+  DevBuf<double> part, coef, nred, Gm, dab;
+  std::vector<double> A, B, zlast;
+  double blast = 0.0;
+  int m = 0;
+
+  // mmax basis columns at most; start: n FP64 device values (any nonzero norm)
+  int run(edg_sector_s* s, int k, const double* start, int mmax, double tol) {
+    const int64_t n = s->vlen;
+    const int64_t ne = s->dim;
+    const bool cplx = s->cplx;
+    cudaStream_t st = s->stream;
+    EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
+    EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
+    size_t npart = 1;
+    for (int mm = 1; mm <= mmax; ++mm)
+      npart = std::max(npart, size_t(2) * mm * dot_shape(mm, cplx ? ne : n).nsplit());
+    EDG_CHECK(part.alloc(npart, st, "multi-dot partials"));
+    EDG_CHECK(nred.alloc(kRedSlots, st, "norm reduction scratch"));  // the norms' own scratch
+    EDG_CHECK(red_scratch_reset(st, nred.p));
+    EDG_CHECK(coef.alloc(3 * size_t(mmax) + 8, st, "multi-dot coefficients"));
+    if (!cplx) EDG_CHECK(Gm.alloc(size_t(mmax) * mmax, st, "Gram matrix"));  // Q^T Q
+    EDG_CHECK(dab.alloc(2 * size_t(mmax) + 4, st, "Lanczos scalars"));  // a_j at [j], b_{j+1} at [mmax+1+j+1]
+    double* dA = dab.p;
+    double* dB = dab.p + mmax + 1;
+    EDG_CHECK(norm_vec<double>(st, start, n, nred.p, dB));
+    double nrm = 0.0;
+    EDG_CUDA(cudaMemcpyAsync(&nrm, dB, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+    if (!(nrm > 0.0)) {
+      set_error("edg_lowest_k: start vector has zero norm");
+      return EDG_ERR_ARG;
+    }
+    EDG_CHECK((convert_dev<T, double>(st, Q.p, start, n, 1.0 / nrm)));
+    // Steps are queued without waiting on the host: the scalars stay on the device (v_{j+1}
+    // = w / b_{j+1} reads b from there) and the host reads them only when it tests
+    // convergence, every max(1, m/32) steps past the first k (more while far from
+    // convergence). Each step reorthogonalises against the whole basis: one pass of
+    // classical Gram-Schmidt lost orthogonality entirely on small sectors, and the test of
+    // Daniel, Gragg, Kaufman & Stewart (Math. Comp. 30 (1976) 772) asked for the second pass
+    // at nearly every step (|a_j| is well above b_j for the shifted spectra of Hubbard sectors).
+    std::vector<double> hA(size_t(mmax) + 1), hB(size_t(mmax) + 2);
+    int next_check = k;
+    m = 0;
+    for (int j = 0; j < mmax; ++j) {
+      T* qj = Q.p + size_t(j) * n;
+      EDG_CHECK(hxv_apply<T>(s, qj, w.p));
+      if constexpr (std::is_same<T, double>::value) {
+        if (cplx) {
+          for (int pass = 0; pass < 2; ++pass) {
+            int nsplit = 0;
+            const int nc = 2 * (j + 1);  // coefficients: real parts, then imaginary parts
+            EDG_CHECK(launch_multidot_c(Q.p, j + 1, ne, w.p, part.p, st, &nsplit));
+            k_multifinish<<<(nc + 7) / 8, 256, 0, st>>>(part.p, nsplit, nc, coef.p);
+            if (pass == 0) k_copy1<<<1, 1, 0, st>>>(dA + j, coef.p + j);  // a_j = Re <q_j, H q_j>
+            k_multiaxpy_c<<<grid_n(ne), kLkThreads, 0, st>>>(reinterpret_cast<const double2*>(Q.p), coef.p, j + 1,
+                                                             ne, reinterpret_cast<double2*>(w.p));
+          }
+        }
+      }
+      if (!cplx) {
+        // One read of the basis gives c = Q^T w and g = Q^T q_j (row j of the Gram matrix
+        // G = Q^T Q); the second Gram-Schmidt pass is taken from G instead of a second read,
+        // y = c - (G - I) c, and one more read applies w -= Q y. Two reads of the basis per
+        // step instead of four; on the 3x4 sectors (up to D = 853,776) the basis stays as
+        // orthogonal (|Q^T Q - I| below 4e-15) and the levels agree with classical
+        // Gram-Schmidt applied twice to 1e-14.
+        int nsplit = 0;
+        const int m1 = j + 1;
+        EDG_CHECK(launch_multidot2<T>(Q.p, m1, n, w.p, qj, part.p, st, &nsplit));
+        k_multifinish<<<(2 * m1 + 7) / 8, 256, 0, st>>>(part.p, nsplit, 2 * m1, coef.p);
+        k_gram_step<<<(m1 + 7) / 8, 256, 0, st>>>(coef.p, m1, Gm.p, mmax, dA + j);
+        k_multiaxpy<T><<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p + 2 * m1, m1, n, w.p);
+      }
+      EDG_CUDA(cudaGetLastError());
+      EDG_CHECK(norm_vec<T>(st, w.p, n, nred.p, dB + j + 1));
+      m = j + 1;
+      if ((m >= k && m >= next_check) || m == mmax || m == ne) {
+        EDG_CUDA(cudaMemcpyAsync(hA.data(), dA, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        EDG_CUDA(cudaMemcpyAsync(hB.data(), dB, size_t(m + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        EDG_CUDA(cudaStreamSynchronize(st));
+        bool last = m == mmax || m == ne;
+        for (int t = 0; t < m; ++t)
+          if (!(hB[t + 1] >= 1e-12)) {  // invariant subspace reached at step t (or NaN)
+            m = t + 1;
+            last = true;
+            break;
+          }
+        A.assign(hA.begin(), hA.begin() + m);
+        B.assign(1, 0.0);
+        for (int t = 1; t < m; ++t) B.push_back(hB[t]);
+        const double b = hB[m];
+        auto converged = [&](const std::vector<double>& th, const std::vector<double>& zl) {
+          if (m < k) return false;
+          for (int i = 0; i < k; ++i)
+            if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) return false;
+          return true;
+        };
+        // the O(k m) test between steps; the QL eigenvectors confirm it before the loop stops
+        std::vector<double> th(std::max(m, k)), zl(std::max(m, k));
+        bool conv = false;
+        double worst = 0.0;  // largest b|z_i| / (tol max(1,|theta_i|)) over the k pairs
+        if (!last && tridiag_lowest_host(m, A.data(), B.data(), std::min(k, m), th.data(), zl.data()) == EDG_OK) {
+          conv = converged(th, zl);
+          for (int i = 0; i < std::min(k, m); ++i)
+            worst = std::max(worst, b * std::fabs(zl[i]) / (tol * std::max(1.0, std::fabs(th[i]))));
+        }
+        if (conv || last) {
+          EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
+          conv = converged(th, zl);
+          zlast = zl;
+          blast = b;
+        }
+        if (conv || last) break;
+        // Ritz residuals fall by a modest factor per step, so far from the tolerance the
+        // next few steps run without a test (steps past convergence cost less than tests)
+        int gap = std::max(1, m / 32);
+        if (worst > 1e6) gap = std::max(gap, 8);
+        else if (worst > 1e3) gap = std::max(gap, 3);
+        next_check = m + gap;
+      }
+      EDG_CHECK(scale_into<T>(st, Q.p + size_t(m) * n, w.p, dB + m, n));
+    }
+    return EDG_OK;
+  }
+
+  // the kk lowest Ritz values, their residual estimates, and (X != null) the Ritz vectors
+  // X[r] = sum_j Z[j][r] q_j in FP64 on the device
+  int ritz(edg_sector_s* s, int kk, double* evals, double* resid, double* X) {
+    const int64_t n = s->vlen;
+    cudaStream_t st = s->stream;
+    // the kk lowest eigenvectors of T by twisted factorisation, O(kk m), when their
+    // eigenvalues stand apart; the full QL eigenvector matrix, O(m^3), when two are close
+    std::vector<double> th(m), Z(size_t(m) * m);
+    if (tridiag_lowest_vectors(m, A.data(), B.data(), kk, kRitzRelGap, th.data(), Z.data()) != EDG_OK)
+      EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, Z.data()));
+    for (int i = 0; i < kk; ++i) evals[i] = th[i];
+    if (resid)
+      for (int i = 0; i < kk; ++i) resid[i] = blast * std::fabs(zlast[i]);
+    if (X) {
+      DevBuf<double> Zd;
+      EDG_CHECK(Zd.alloc(size_t(m) * kk, st, "Ritz coefficients"));
+      EDG_CUDA(cudaMemcpyAsync(Zd.p, Z.data(), size_t(m) * kk * sizeof(double), cudaMemcpyHostToDevice, st));
+      k_ritz_k<T><<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p, m, kk, n, X);
+      EDG_CUDA(cudaGetLastError());
+      EDG_CUDA(cudaStreamSynchronize(st));  // Z (host) is read by the copy above
+    }
+    return EDG_OK;
+  }
+};
+
+// Basis columns of precision `elem` that fit in HBM beyond a 2 GB reserve, at most mmax.
+int basis_room(int64_t n, size_t elem, int k, int* mmax) {
+  size_t fr = 0, tot = 0;
+  EDG_CUDA(cudaMemGetInfo(&fr, &tot));
+  const size_t reserve = size_t(2) << 30, per = size_t(n) * elem;
+  const size_t extra = size_t(n) * sizeof(double) * (size_t(k) + 4);  // Ritz and start vectors
+  const int64_t fit = fr > reserve + extra ? int64_t((fr - reserve - extra) / per) - 2 : 0;
+  if (fit < *mmax) *mmax = int(fit);
+  if (*mmax < k || *mmax < 1) {
+    set_error("edg_lowest_k: %lld-element basis vectors: no room for %d of them", (long long)n, k);
+    return EDG_ERR_NOMEM;
+  }
+  return EDG_OK;
+}
+
+}  // namespace
+
+int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int maxit, double tol, int mode,
+             double* evals, double* evecs_host, double* resid, int* niter) {
   const int64_t n = s->vlen;   // reals per vector
   const int64_t ne = s->dim;   // elements per vector (complex ones for complex Hij)
-  const bool cplx = s->cplx;
   cudaStream_t st = s->stream;
   if (k < 1 || k > kMaxK) {
     set_error("edg_lowest_k: k=%d outside 1..%d", k, kMaxK);
     return EDG_ERR_ARG;
   }
+  for (int i = 0; i < k; ++i) {
+    evals[i] = NAN;
+    if (resid) resid[i] = NAN;
+  }
   if (k > ne) k = int(ne);
-  int mmax = std::min<int64_t>(std::min(maxit, kMaxBasis), ne);
-  if (mmax < k) mmax = k;
-  {  // the basis takes what HBM allows beyond a 2 GB reserve
-    size_t fr = 0, tot = 0;
-    EDG_CUDA(cudaMemGetInfo(&fr, &tot));
-    const size_t reserve = size_t(2) << 30, per = size_t(n) * sizeof(double);
-    const int64_t fit = fr > reserve + 4 * per ? int64_t((fr - reserve) / per) - 4 : 0;
-    if (fit < mmax) mmax = int(fit);
-    if (mmax < k || mmax < 1) {
-      set_error("edg_lowest_k: %lld-element basis vectors: no room for %d of them", (long long)n, k);
-      return EDG_ERR_NOMEM;
-    }
-  }
-  // device: basis Q[mmax][n], w, scratch
-  DevBuf<double> Q, X;
-  DevBuf<double> w, part, coef, Zd, nred;
-  EDG_CHECK(Q.alloc(size_t(mmax) * n, st, "Lanczos basis (lowest-k)"));
-  EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
-  size_t npart = 1;
-  for (int mm = 1; mm <= mmax; ++mm)
-    npart = std::max(npart, size_t(2) * mm * dot_shape(mm, cplx ? ne : n).nsplit());
-  EDG_CHECK(part.alloc(npart, st, "multi-dot partials"));
-  EDG_CHECK(nred.alloc(kRedSlots, st, "norm reduction scratch"));  // the norms' own scratch
-  EDG_CHECK(red_scratch_reset(st, nred.p));
-  EDG_CHECK(coef.alloc(3 * size_t(mmax) + 8, st, "multi-dot coefficients"));
-  DevBuf<double> Gm;  // Gram matrix Q^T Q of the basis (real sectors)
-  if (!cplx) EDG_CHECK(Gm.alloc(size_t(mmax) * mmax, st, "Gram matrix"));
-  // start vector
+  const int mmax0 = std::max<int>(k, int(std::min<int64_t>(std::min(maxit, kMaxBasis), ne)));
+  DevBuf<double> x0;  // start vector
+  EDG_CHECK(x0.alloc(size_t(n), st, "start vector"));
   if (v0_host) {
-    EDG_CUDA(cudaMemcpyAsync(Q.p, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    EDG_CUDA(cudaMemcpyAsync(x0.p, v0_host, n * sizeof(double), cudaMemcpyHostToDevice, st));
   } else {
-    EDG_CHECK(random_dev(st, Q.p, n, seed));
+    EDG_CHECK(random_dev(st, x0.p, n, seed));
   }
-  DevBuf<double> dab;  // a_j at [j], b_{j+1} at [mmax + 1 + j + 1]
-  EDG_CHECK(dab.alloc(2 * size_t(mmax) + 4, st, "Lanczos scalars"));
-  double* dA = dab.p;
-  double* dB = dab.p + mmax + 1;
-  EDG_CHECK(norm_dev(st, Q.p, n, nred.p, dB));
-  double nrm = 0.0;
-  EDG_CUDA(cudaMemcpyAsync(&nrm, dB, sizeof(double), cudaMemcpyDeviceToHost, st));
-  EDG_CUDA(cudaStreamSynchronize(st));
-  if (!(nrm > 0.0)) {
-    set_error("edg_lowest_k: start vector has zero norm");
-    return EDG_ERR_ARG;
+  int steps32 = 0;
+  if (mode == EDG_LK_F32_REFINE && !s->cplx) {
+    // FP32-bulk phase to residuals kTol32, then its k Ritz vectors, summed, start the FP64 run:
+    // the FP64 Krylov space then holds the wanted eigenvectors to FP32 accuracy from its first
+    // k vectors and refines them in few steps
+    const int kk = k;
+    DevBuf<double> X;
+    EDG_CHECK(X.alloc(size_t(kk) * n, st, "FP32 Ritz vectors"));
+    {
+      int mmax = mmax0;
+      EDG_CHECK(basis_room(n, sizeof(float), k, &mmax));
+      LkRun<float> r32;
+      EDG_CHECK(r32.run(s, k, x0.p, mmax, std::max(tol, kTol32)));
+      steps32 = r32.m;
+      std::vector<double> ev(kk), rs(kk);
+      const int k32 = std::min(kk, r32.m);
+      EDG_CHECK(r32.ritz(s, k32, ev.data(), rs.data(), X.p));
+      EDG_CUDA(cudaMemsetAsync(x0.p, 0, n * sizeof(double), st));
+      for (int r = 0; r < k32; ++r) EDG_CHECK(axpy_accum_dev<double>(st, x0.p, X.p + size_t(r) * n, 1.0, n));
+    }  // the FP32 basis goes back to the pool before the FP64 one is taken
   }
-  EDG_CHECK((scale_inplace_dev<double>(st, Q.p, n, 1.0 / nrm)));
-  // Steps are queued without waiting on the host: the scalars stay on the device (v_{j+1} =
-  // w / b_{j+1} reads b from there) and the host reads them only when it tests convergence,
-  // every max(1, m/32) steps past the first k (more while far from convergence). Each step reorthogonalises against the whole
-  // basis by classical Gram-Schmidt applied twice: one pass lost orthogonality entirely on
-  // small sectors, and the test of Daniel, Gragg, Kaufman & Stewart (Math. Comp. 30 (1976)
-  // 772) asked for the second pass at nearly every step (|a_j| is well above b_j for the
-  // shifted spectra of Hubbard sectors).
-  std::vector<double> A, B, hA(size_t(mmax) + 1), hB(size_t(mmax) + 2), zlast;
-  double blast = 0.0;
-  int m = 0, next_check = k;
-  for (int j = 0; j < mmax; ++j) {
-    double* qj = Q.p + size_t(j) * n;
-    EDG_CHECK(hxv_apply<double>(s, qj, w.p));
-    if (cplx) {
-      for (int pass = 0; pass < 2; ++pass) {
-        int nsplit = 0;
-        const int nc = 2 * (j + 1);  // coefficients: real parts, then imaginary parts
-        EDG_CHECK(launch_multidot_c(Q.p, j + 1, ne, w.p, part.p, st, &nsplit));
-        k_multifinish<<<(nc + 7) / 8, 256, 0, st>>>(part.p, nsplit, nc, coef.p);
-        if (pass == 0) k_copy1<<<1, 1, 0, st>>>(dA + j, coef.p + j);  // a_j = Re <q_j, H q_j>
-        k_multiaxpy_c<<<grid_n(ne), kLkThreads, 0, st>>>(reinterpret_cast<const double2*>(Q.p), coef.p, j + 1, ne,
-                                                         reinterpret_cast<double2*>(w.p));
-      }
-    } else {
-      // One read of the basis gives c = Q^T w and g = Q^T q_j (row j of the Gram matrix
-      // G = Q^T Q); the second Gram-Schmidt pass is taken from G instead of a second read,
-      // y = c - (G - I) c, and one more read applies w -= Q y. Two reads of the basis per
-      // step instead of four; on the 3x4 sectors (up to D = 853,776) the basis stays as
-      // orthogonal (|Q^T Q - I| below 4e-15) and the levels agree with classical
-      // Gram-Schmidt applied twice to 1e-14.
-      int nsplit = 0;
-      const int m1 = j + 1;
-      EDG_CHECK(launch_multidot2(Q.p, m1, n, w.p, qj, part.p, st, &nsplit));
-      k_multifinish<<<(2 * m1 + 7) / 8, 256, 0, st>>>(part.p, nsplit, 2 * m1, coef.p);
-      k_gram_step<<<(m1 + 7) / 8, 256, 0, st>>>(coef.p, m1, Gm.p, mmax, dA + j);
-      k_multiaxpy<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p + 2 * m1, m1, n, w.p);
-    }
-    EDG_CUDA(cudaGetLastError());
-    EDG_CHECK(norm_dev(st, w.p, n, nred.p, dB + j + 1));
-    m = j + 1;
-    if ((m >= k && m >= next_check) || m == mmax || m == ne) {
-      EDG_CUDA(cudaMemcpyAsync(hA.data(), dA, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
-      EDG_CUDA(cudaMemcpyAsync(hB.data(), dB, size_t(m + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
-      EDG_CUDA(cudaStreamSynchronize(st));
-      bool last = m == mmax || m == ne;
-      for (int t = 0; t < m; ++t)
-        if (!(hB[t + 1] >= 1e-12)) {  // invariant subspace reached at step t (or NaN)
-          m = t + 1;
-          last = true;
-          break;
-        }
-      A.assign(hA.begin(), hA.begin() + m);
-      B.assign(1, 0.0);
-      for (int t = 1; t < m; ++t) B.push_back(hB[t]);
-      const double b = hB[m];
-      auto converged = [&](const std::vector<double>& th, const std::vector<double>& zl) {
-        if (m < k) return false;
-        for (int i = 0; i < k; ++i)
-          if (b * std::fabs(zl[i]) > tol * std::max(1.0, std::fabs(th[i]))) return false;
-        return true;
-      };
-      // the O(k m) test between steps; the QL eigenvectors confirm it before the loop stops
-      std::vector<double> th(std::max(m, k)), zl(std::max(m, k));
-      bool conv = false;
-      double worst = 0.0;  // largest b|z_i| / (tol max(1,|theta_i|)) over the k pairs
-      if (!last && tridiag_lowest_host(m, A.data(), B.data(), std::min(k, m), th.data(), zl.data()) == EDG_OK) {
-        conv = converged(th, zl);
-        for (int i = 0; i < std::min(k, m); ++i)
-          worst = std::max(worst, b * std::fabs(zl[i]) / (tol * std::max(1.0, std::fabs(th[i]))));
-      }
-      if (conv || last) {
-        EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, nullptr, zl.data()));
-        conv = converged(th, zl);
-        zlast = zl;
-        blast = b;
-      }
-      if (conv || last) break;
-      // Ritz residuals fall by a modest factor per step, so far from the tolerance the
-      // next few steps run without a test (steps past convergence cost less than tests)
-      int gap = std::max(1, m / 32);
-      if (worst > 1e6) gap = std::max(gap, 8);
-      else if (worst > 1e3) gap = std::max(gap, 3);
-      next_check = m + gap;
-    }
-    EDG_CHECK(scale_into<double>(st, Q.p + size_t(m) * n, w.p, dB + m, n));
-  }
-  if (niter) *niter = m;
-  const int kk = std::min(k, m);
-  // the kk lowest eigenvectors of T by twisted factorisation, O(kk m), when their eigenvalues
-  // stand apart; the full QL eigenvector matrix, O(m^3), when two of them are close
-  std::vector<double> th(m), Z(size_t(m) * m);
-  if (tridiag_lowest_vectors(m, A.data(), B.data(), kk, kRitzRelGap, th.data(), Z.data()) != EDG_OK)
-    EDG_CHECK(tridiag_eigh_host(m, A.data(), B.data(), th.data(), nullptr, Z.data()));
-  for (int i = 0; i < kk; ++i) evals[i] = th[i];
-  for (int i = kk; i < k; ++i) evals[i] = NAN;
-  if (resid) {
-    for (int i = 0; i < kk; ++i) resid[i] = blast * std::fabs(zlast[i]);
-    for (int i = kk; i < k; ++i) resid[i] = NAN;
-  }
+  int mmax = mmax0;
+  EDG_CHECK(basis_room(n, sizeof(double), k, &mmax));
+  LkRun<double> r64;
+  EDG_CHECK(r64.run(s, k, x0.p, mmax, tol));
+  if (niter) *niter = steps32 + r64.m;
+  const int kk = std::min(k, r64.m);
+  DevBuf<double> X;
+  if (evecs_host) EDG_CHECK(X.alloc(size_t(kk) * n, st, "Ritz vectors"));
+  EDG_CHECK(r64.ritz(s, kk, evals, resid, evecs_host ? X.p : nullptr));
   if (evecs_host) {
-    EDG_CHECK(Zd.alloc(size_t(m) * kk, st, "Ritz coefficients"));
-    EDG_CHECK(X.alloc(size_t(kk) * n, st, "Ritz vectors"));
-    EDG_CUDA(cudaMemcpyAsync(Zd.p, Z.data(), size_t(m) * kk * sizeof(double), cudaMemcpyHostToDevice, st));
-    k_ritz_k<<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p, m, kk, n, X.p);
-    EDG_CUDA(cudaGetLastError());
     EDG_CUDA(cudaMemcpyAsync(evecs_host, X.p, size_t(kk) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
     EDG_CUDA(cudaStreamSynchronize(st));
   }

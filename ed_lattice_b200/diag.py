@@ -198,6 +198,7 @@ class DiagParams:
     lanc_dim_threshold: int = 1024   # LANC_DIM_THRESHOLD
     lanc_nstates_total: int = 1      # set by setup()
     ed_twin: bool = False            # ED_TWIN: solve Nup >= Ndw only, twins by spin flip
+    lanc_fp32_bulk: bool = False     # lowest-k sectors: FP32 bulk + FP64 refinement (no reference key)
     sector_threads: int = 4          # sectors solved at once on one device (no reference key)
 
     def setup(self, nsectors: int) -> "DiagParams":
@@ -243,7 +244,8 @@ def device_solver(model: Model, nup: int, ndw: int, neigen: int, lanc_solve: boo
         if params.lanc_method == "lanczos":
             e0, vec, _ = sp_lanc_eigh(sec, seed=seed, maxit=maxit, tol=params.lanc_tolerance)
             return np.array([e0]), vec[None, :]
-        ev, vecs, resid, _ = sec.lowest_k(neigen, seed=seed, maxit=maxit, tol=params.lanc_tolerance)
+        ev, vecs, resid, _ = sec.lowest_k(neigen, seed=seed, maxit=maxit, tol=params.lanc_tolerance,
+                                          mode=L.EDG_LK_F32_REFINE if params.lanc_fp32_bulk else L.EDG_LK_F64)
         bad = resid > params.lanc_tolerance * np.maximum(1.0, np.abs(ev))
         if np.any(bad):
             raise L.EdgError(L.EDG_ERR_NOCONV, "sp_eigh",

@@ -237,8 +237,9 @@ class Sector:
         L.check(L.lib().edg_sector_set_stream(self.handle, C.c_void_p(stream)), "edg_sector_set_stream")
 
     def lowest_k(self, k: int, v0: np.ndarray | None = None, seed: int = 1234, maxit: int = 512,
-                 tol: float = 1e-10, want_vectors: bool = True):
-        """Lowest k eigenpairs (the sp_eigh branch of ed_diag_d, src/DIAG/DIAG.f90:191-202).
+                 tol: float = 1e-10, want_vectors: bool = True, mode: int = L.EDG_LK_F64):
+        """Lowest k eigenpairs (the sp_eigh branch of ed_diag_d, src/DIAG/DIAG.f90:191-202),
+        FP64 (mode EDG_LK_F64) or FP32 bulk + FP64 refinement (EDG_LK_F32_REFINE).
         Returns (evals[k'], evecs[k', dim] or None, resid[k'], basis size), k' = min(k, dim)."""
         kk = min(k, self.dim)
         ev = np.zeros(k)
@@ -246,8 +247,8 @@ class Sector:
         vecs = np.empty((kk, self.vlen)) if want_vectors else None
         it = C.c_int()
         v0a = self._vec(v0, "v0") if v0 is not None else None
-        L.check(L.lib().edg_lowest_k(self.handle, k, _pd(v0a), C.c_uint64(seed), maxit, tol, _pd(ev), _pd(vecs),
-                                     _pd(rs), C.byref(it)), "sp_eigh")
+        L.check(L.lib().edg_lowest_k_mode(self.handle, k, _pd(v0a), C.c_uint64(seed), maxit, tol, mode, _pd(ev),
+                                          _pd(vecs), _pd(rs), C.byref(it)), "sp_eigh")
         if vecs is not None and self.cplx:
             vecs = vecs.view(np.complex128)
         return ev[:kk], vecs, rs[:kk], it.value

@@ -195,6 +195,14 @@ int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64);
  * inside a sector appear once (use edg_sector_dense for small sectors with symmetries). */
 int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol,
                  double* evals, double* evecs, double* resid, int* niter);
+/* Lowest-k modes: FP64 throughout (edg_lowest_k), or FP32 bulk + FP64 refinement: the same
+ * solver with FP32 basis and H x v (FP64 scalars and sums) to Ritz residuals of 1e-6, whose k
+ * Ritz vectors, summed, start the FP64 solve to tol. Real Hij only (complex sectors run FP64). */
+enum { EDG_LK_F64 = 0, EDG_LK_F32_REFINE = 1 };
+/* edg_lowest_k with a mode; *niter counts the basis vectors of both phases. The outputs are
+ * those of the FP64 phase (evals, vectors and residuals to tol). */
+int edg_lowest_k_mode(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol,
+                      int mode, double* evals, double* evecs, double* resid, int* niter);
 /* Dense sector Hamiltonian, column-major dim x dim (the matrix ed_buildh(Hmat) assembles for
  * the LAPACK branch of ed_diag_d, src/DIAG/HAMILTONIAN_STORED_HxV.f90:81-117 and
  * src/DIAG/DIAG.f90:229-235): diag + kron(H_dw, 1) + kron(1, H_up). Stored form only;

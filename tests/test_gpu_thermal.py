@@ -61,13 +61,15 @@ def test_dense_matrix_and_lowest_k_small_sectors(fx):
         s.delete()
 
 
+@pytest.mark.parametrize("mode", [E.EDG_LK_F64, E.EDG_LK_F32_REFINE], ids=["f64", "f32refine"])
 @pytest.mark.parametrize("nup,ndw", [(6, 6), (5, 6), (3, 2), (7, 4)])
-def test_lowest_k_large_sectors(fx, nup, ndw):
-    """Sectors beyond the dense range (D up to 853,776) against ARPACK's levels."""
+def test_lowest_k_large_sectors(fx, nup, ndw, mode):
+    """Sectors beyond the dense range (D up to 853,776) against ARPACK's levels, FP64 and FP32
+    bulk + FP64 refinement (the same tolerances: the refinement is FP64)."""
     H = _hij(fx["eps"])
     gm, om = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False), O.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
     s = E.Sector(gm, nup, ndw)
-    ev, vecs, resid, m = s.lowest_k(4, seed=3, tol=1e-10)
+    ev, vecs, resid, m = s.lowest_k(4, seed=3, tol=1e-10, mode=mode)
     ref = fx["energies"][gm.get_sector(nup, ndw) - 1]
     assert np.allclose(ev, ref, rtol=0, atol=1e-9), (ev, ref)
     assert np.all(resid <= 1e-10 * np.maximum(1.0, np.abs(ev)))
@@ -99,21 +101,26 @@ def test_lowest_k_start_vector_and_argument_checks(fx):
     one.delete()
 
 
-@pytest.mark.parametrize("dim_threshold", [4000, 0])
-def test_thermal_beta20_all_sectors(fx, dim_threshold):
+@pytest.mark.parametrize("dim_threshold,fp32,twin", [(4000, False, False), (0, False, False), (1024, True, False),
+                                                    (1024, True, True)])
+def test_thermal_beta20_all_sectors(fx, dim_threshold, fp32, twin):
     """diagonalize_lattice + partition_function + lanc_observables at T=0.05 over the 169
-    sectors (lowest 4 each), with the dense branch up to D=4000 and with Lanczos everywhere."""
+    sectors (lowest 4 each), with the dense branch up to D=4000, with Lanczos everywhere, with
+    FP32 bulk + FP64 refinement in the Lanczos sectors, and with twin sectors (the 91 sectors
+    with Nup >= Ndw solved, the others taken as spin-flipped copies)."""
     H = _hij(fx["eps"])
     gm = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
     p = DiagParams(finite_temp=True, temp=0.05, cutoff=1e-9, lanc_nstates_sector=4,
-                   lanc_dim_threshold=dim_threshold, lanc_tolerance=1e-10)
+                   lanc_dim_threshold=dim_threshold, lanc_tolerance=1e-10, lanc_fp32_bulk=fp32, ed_twin=twin)
     sl, eigs = diagonalize_lattice(gm, p, seed=1234)
-    assert len(eigs) == 169
+    assert len(eigs) == (91 if twin else 169)
     for isector, ev, _ in eigs:
         ref = fx["energies"][isector - 1]
         assert np.allclose(ev, ref[: ev.size], rtol=0, atol=1e-9), (isector, ev, ref)
     zeta = partition_function(sl, p)
     assert sl.emin == pytest.approx(float(fx["egs"]), abs=1e-10)
+    if twin:  # the twins' levels are copies: the kept list is the same set of states
+        assert all(s.vec is not None for s in sl.states[: sl.trimd_size])
     assert sl.trimd_size == int(fx["nkept"])
     assert sorted(s.sector for s in sl.states[: sl.trimd_size]) == sorted(fx["kept_sectors"].tolist())
     assert zeta == pytest.approx(float(fx["zeta"]), rel=1e-8)
