@@ -237,28 +237,39 @@ def e0_time_to_solution(E, L, sector, seed=2024, maxit=600):
 def thermal_3x4(E):
     """Finite-temperature diagonalisation of the 3x4 disordered lattice (t=1, U=4, XMU=2,
     eps_i ~ uniform[-1,1) quantised to 2^-16, seed 7): lowest 4 levels of all 169 sectors,
-    state list, Z and site observables at beta=20. Wall time of the whole driver: a first
-    call, then the reported one."""
+    state list, Z and site observables at beta=20, with the Lanczos sectors in FP32 bulk +
+    FP64 refinement (the reported figure) and in FP64 throughout. Wall time of the whole
+    driver: a first call, then the reported one."""
     import torch
     from ed_lattice_b200.diag import DiagParams, diagonalize_lattice, lanc_observables, partition_function
     rng = np.random.default_rng(7)
     H = E.square_lattice(3, 4)
     H[np.diag_indices(12)] = np.round(rng.uniform(-1, 1, 12) * 65536) / 65536
     model = E.Model(H, uloc=4.0, xmu=2.0, hfmode=False)
-    runs = []
-    for _ in range(2):  # the first call also loads the solver kernels and the dense eigensolver
-        p = DiagParams(finite_temp=True, temp=0.05, lanc_nstates_sector=4, lanc_dim_threshold=1024)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        sl, eigs = diagonalize_lattice(model, p)
-        zeta = partition_function(sl, p)
-        obs = lanc_observables(model, sl, zeta, p)
-        torch.cuda.synchronize()
-        runs.append(time.perf_counter() - t0)
-    return {"seconds": runs[1], "first_call_seconds": runs[0], "sector_threads": p.sector_threads,
-            "sectors": len(eigs), "lanczos_sectors": sum(1 for e in eigs if e[2]),
-            "states_kept": sl.trimd_size, "egs": sl.emin, "zeta": zeta, "dens_total": float(obs["dens"].sum()),
-            "docc_mean": float(obs["docc"].mean())}
+    out = {}
+    for fp32 in (True, False):
+        runs = []
+        for _ in range(2):  # the first call also loads the solver kernels and the dense eigensolver
+            p = DiagParams(finite_temp=True, temp=0.05, lanc_nstates_sector=4, lanc_dim_threshold=1024,
+                           lanc_fp32_bulk=fp32)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sl, eigs = diagonalize_lattice(model, p)
+            zeta = partition_function(sl, p)
+            obs = lanc_observables(model, sl, zeta, p)
+            torch.cuda.synchronize()
+            runs.append(time.perf_counter() - t0)
+        res = {"seconds": runs[1], "first_call_seconds": runs[0], "sector_threads": p.sector_threads,
+               "sectors": len(eigs), "lanczos_sectors": sum(1 for e in eigs if e[2]),
+               "states_kept": sl.trimd_size, "egs": sl.emin, "zeta": zeta, "dens_total": float(obs["dens"].sum()),
+               "docc_mean": float(obs["docc"].mean())}
+        if fp32:
+            out.update(res)
+            out["lanczos_precision"] = "FP32 bulk + FP64 refinement"
+        else:
+            out["fp64"] = res
+    out["zeta_rel_diff_vs_fp64"] = abs(out["zeta"] - out["fp64"]["zeta"]) / out["fp64"]["zeta"]
+    return out
 
 
 def lowest_k_3x4(E):
@@ -280,10 +291,20 @@ def lowest_k_3x4(E):
         torch.cuda.synchronize()
         runs.append(time.perf_counter() - t0)
     reorth = sum(2 * j * s.dim * 8 for j in range(1, m + 1))
+    out = {"seconds": runs[1], "first_call_seconds": runs[0], "dim": s.dim, "basis": m,
+           "ms_per_step": 1e3 * runs[1] / m, "reorth_bytes": reorth, "reorth_GBps": reorth / runs[1] / 1e9,
+           "e0": float(ev[0]), "max_resid": float(np.max(resid))}
+    runs = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev2, _, resid2, m2 = s.lowest_k(4, seed=1234, maxit=512, tol=1e-10, mode=E.EDG_LK_F32_REFINE)
+        torch.cuda.synchronize()
+        runs.append(time.perf_counter() - t0)
+    out["fp32_refine"] = {"seconds": runs[1], "basis_vectors_both_phases": m2, "max_level_diff": float(np.abs(ev2 - ev).max()),
+                          "max_resid": float(np.max(resid2))}
     s.delete()
-    return {"seconds": runs[1], "first_call_seconds": runs[0], "dim": s.dim, "basis": m,
-            "ms_per_step": 1e3 * runs[1] / m, "reorth_bytes": reorth, "reorth_GBps": reorth / runs[1] / 1e9,
-            "e0": float(ev[0]), "max_resid": float(np.max(resid))}
+    return out
 
 
 def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150, widths=(1, 4, 8, 16)):

@@ -64,6 +64,7 @@ SIGNATURES = {
     "edg_hxv_z": (_i, [_p, _i64, _pd, _pd]),
     "edg_hxv_d": (_i, [_p, _i64, _pd, _pd]),
     "edg_sector_autotune": (_i, [_p, _i, _i, _pd, _pi, _pi]),
+    "edg_sector_set_kernels": (_i, [_p, _i, _i]),
     "edg_hxv_dev_f64": (_i, [_p, _p, _p]),
     "edg_hxv_dev_f32": (_i, [_p, _p, _p]),
     "edg_tridiag_d": (_i, [_p, _pd, _i, _d, _i, _pd, _pd, _pd, _pi]),

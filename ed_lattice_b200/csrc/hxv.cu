@@ -358,12 +358,8 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_p16(HxvArgs<float> a, 
               if (NEG) {
                 ffma2_acc(acc, hh, S64[e]);
               } else {
-                const uint64_t x = S64[e & 0x7fffu];
-                const float hf = __uint_as_float(__float_as_uint(hs) ^ ((e & 0x8000u) << 16));
-                float lo = __uint_as_float(uint32_t(acc)), hi = __uint_as_float(uint32_t(acc >> 32));
-                lo = __fmaf_rn(hf, __uint_as_float(uint32_t(x)), lo);
-                hi = __fmaf_rn(hf, __uint_as_float(uint32_t(x >> 32)), hi);
-                acc = (uint64_t(__float_as_uint(hi)) << 32) | __float_as_uint(lo);
+                const uint64_t sb = uint64_t((e & 0x8000u) << 16);  // the term's sign, both halves
+                ffma2_acc(acc, hh ^ (sb | (sb << 32)), S64[e & 0x7fffu]);
               }
             }
           }

@@ -227,6 +227,10 @@ class Sector:
                 "edg_sector_autotune")
         return {"ms": ms[: nc.value].tolist(), "best": best.value}
 
+    def set_kernels(self, candidate: int, precision: int = L.EDG_PREC_F32) -> None:
+        """Pin the H x v kernel pair (an index of autotune()'s candidate list)."""
+        L.check(L.lib().edg_sector_set_kernels(self.handle, precision, candidate), "edg_sector_set_kernels")
+
     def release_work(self) -> None:
         """Hand the sector's work buffers (Lanczos vectors, FP32 basis, block vectors) back to
         the library's pool; tables and the state buffer stay."""

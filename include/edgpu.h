@@ -133,6 +133,9 @@ int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv);
  * every pair; FP32 packed up passes change the order of a row's terms. Untuned sectors use
  * candidate 0. No counterpart in the reference. */
 int edg_sector_autotune(edg_sector* s, int precision, int reps, double* ms, int* ncand, int* best);
+/* Pin the H x v kernel pair of this sector for one precision to candidate k of
+ * edg_sector_autotune's list (0..8 for FP32, 0..2 for FP64). No counterpart in the reference. */
+int edg_sector_set_kernels(edg_sector* s, int precision, int candidate);
 /* Device-resident forms (vectors in HBM, reference layout); stream-ordered, no sync. */
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv);
 int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv);

@@ -130,12 +130,20 @@ def test_chi_chain_block_momentum(prec):
     r = np.stack([xs.ravel(), ys.ravel()], 1)  # site i = x + lx*y
     qs = [(2 * np.pi * m / lx, 2 * np.pi * n / ly) for n in range(ly) for m in range(lx)]
     qcos = np.array([np.cos(q[0] * r[:, 0] + q[1] * r[:, 1]) for q in qs])
+    # the chains have the same coefficients; the poles and weights come from the device QL
+    # (block) and the host QL (single). The q = 0 charge operator is the conserved total N, so
+    # its start vector is an eigenvector: with FP32 vectors the chain continues on rounding
+    # noise, and the weights of those nearly decoupled poles agree only to FP32 level
+    wtol = 1e-12 if prec == E.EDG_PREC_F64 else 1e-8
     for kind in (0, 1):
         blk = E.chi_chain_block(s, 60, e0, kind=kind, qcos=qcos, precision=prec)
         for c in range(len(qs)):
             one = E.chi_chain(s, 1, 60, e0, kind=kind, qcos=qcos[c], precision=prec)
             assert blk[c].norm2 == one.norm2
-            np.testing.assert_allclose(blk[c].weight, one.weight, rtol=0, atol=1e-12 * max(1.0, one.norm2))
+            np.testing.assert_allclose(blk[c].weight, one.weight, rtol=0, atol=wtol * max(1.0, one.norm2))
+            mb = [(blk[c].weight * blk[c].poles ** n).sum() for n in range(5)]
+            mo = [(one.weight * one.poles ** n).sum() for n in range(5)]
+            assert np.allclose(mb, mo, rtol=1e-10, atol=1e-12), (kind, c)
             assert abs(blk[c].weight.sum() - blk[c].norm2) <= 1e-9 * max(1.0, blk[c].norm2)
     s.delete()
 
