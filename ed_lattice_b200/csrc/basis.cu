@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -515,6 +516,272 @@ static void build_schedule(int64_t dim, int rt, const std::vector<uint32_t>& off
   }
 }
 
+// Kronecker split of one spin's gather table at bit m (SpinBasis::kron_*), planned on the
+// host from the CSR rows and the basis map. Hops are classed by the two bits they move: both
+// below m (LL), both at or above m (HH), else cross. Fails (returns false) when the table
+// does not have the block structure the up pass relies on, or the schedule does not fit.
+struct KronPlan {
+  int m = 0;
+  int64_t within = 0;                 // LL + HH hops
+  std::vector<int4> thr;              // per thread: krow0, blocks, low row, lidx
+  std::vector<int32_t> bcol;          // per krow
+  std::vector<uint32_t> hoff;         // per krow + 1
+  std::vector<int32_t> hent;
+  std::vector<int32_t> lent;          // per thread: kKronLL slots
+  std::vector<uint32_t> xent, xoff, xwid;
+  int lmax = 0;
+};
+
+static bool plan_kron(int m, int rt, int64_t dim, const std::vector<uint32_t>& map, const std::vector<uint32_t>& off,
+                      const std::vector<uint32_t>& src, const std::vector<uint32_t>& sgn, KronPlan& P) {
+  const uint32_t mask = (1u << m) - 1u;
+  // blocks of equal high part, in column order, then grouped by popcount(high part)
+  std::vector<int64_t> bstart;        // per block (column order): first column
+  std::vector<int> bgrp;
+  for (int64_t c = 0; c < dim; ++c)
+    if (c == 0 || (map[c] >> m) != (map[c - 1] >> m)) {
+      bstart.push_back(c);
+      bgrp.push_back(__builtin_popcount(map[c] >> m));
+    }
+  const int nblk = int(bstart.size());
+  bstart.push_back(dim);
+  const int G = 33;
+  std::vector<int> gsize(G, -1), gcount(G, 0);
+  for (int b = 0; b < nblk; ++b) {
+    const int sz = int(bstart[b + 1] - bstart[b]);
+    if (gsize[bgrp[b]] < 0) gsize[bgrp[b]] = sz;
+    if (gsize[bgrp[b]] != sz) return false;  // blocks of one group must be alike
+    ++gcount[bgrp[b]];
+  }
+  std::vector<int> gblk(G + 1, 0), glow(G + 1, 0);  // group-major bases of krow and low row
+  for (int g = 0; g < G; ++g) {
+    gblk[g + 1] = gblk[g] + gcount[g];
+    glow[g + 1] = glow[g] + (gcount[g] ? gsize[g] : 0);
+  }
+  std::vector<int> krow_of(nblk), hidx_of(nblk), seen(G, 0);
+  for (int b = 0; b < nblk; ++b) {
+    hidx_of[b] = seen[bgrp[b]]++;
+    krow_of[b] = gblk[bgrp[b]] + hidx_of[b];
+  }
+  const int nkrow = gblk[G], nlow = glow[G];
+  P.m = m;
+  P.within = 0;
+  P.bcol.assign(nkrow, 0);
+  std::vector<std::vector<int32_t>> hh(nkrow), ll(nlow);
+  std::vector<char> hh_set(nkrow, 0), ll_set(nlow, 0);
+  std::vector<std::vector<uint32_t>> cross(dim);
+  for (int b = 0; b < nblk; ++b) {
+    const int g = bgrp[b], kr = krow_of[b];
+    P.bcol[kr] = int32_t(bstart[b]);
+    for (int64_t c = bstart[b]; c < bstart[b + 1]; ++c) {
+      const int lidx = int(c - bstart[b]), lr = glow[g] + lidx;
+      std::vector<int32_t> myll, myhh;
+      for (uint32_t k = off[c]; k < off[c + 1]; ++k) {
+        const uint32_t d = map[c] ^ map[src[k]];
+        const int64_t delta = int64_t(src[k]) - c;
+        if ((d & mask) == d) myll.push_back(int32_t((delta << 1) | sgn[k]));
+        else if ((d & mask) == 0) myhh.push_back(int32_t((delta << 1) | sgn[k]));
+        else cross[c].push_back(src[k] | (sgn[k] << 31));
+      }
+      P.within += int64_t(myll.size() + myhh.size());
+      if (!ll_set[lr]) { ll[lr] = myll; ll_set[lr] = 1; }
+      else if (ll[lr] != myll) return false;
+      if (!hh_set[kr]) { hh[kr] = myhh; hh_set[kr] = 1; }
+      else if (hh[kr] != myhh) return false;
+      if (int(myll.size()) > kKronLL) return false;
+      for (int32_t e : myll)
+        if ((e >> 1) < -32768 || (e >> 1) > 32767) return false;  // LL offsets are 16-bit in the up pass
+    }
+  }
+  // thread schedule: a thread owns (group, lidx) and a run of consecutive blocks of the
+  // group; runs of about equal length, the shortest length whose threads fit one CTA
+  int64_t lanes = 0;
+  for (int g = 0; g < G; ++g) lanes += gcount[g] ? gsize[g] : 0;
+  if (lanes > kKronThreads) return false;
+  int L = int((dim + kKronThreads - 1) / kKronThreads);
+  for (;; ++L) {
+    int64_t T = 0;
+    for (int g = 0; g < G; ++g)
+      if (gcount[g]) T += int64_t(gsize[g]) * ((gcount[g] + L - 1) / L);
+    if (T <= kKronThreads) break;
+  }
+  P.thr.clear();
+  P.lmax = 0;
+  for (int g = 0; g < G; ++g) {
+    if (!gcount[g]) continue;
+    const int nch = (gcount[g] + L - 1) / L;
+    for (int q = 0; q < nch; ++q) {
+      const int h0 = int(int64_t(q) * gcount[g] / nch), h1 = int(int64_t(q + 1) * gcount[g] / nch);
+      for (int lidx = 0; lidx < gsize[g]; ++lidx)
+        P.thr.push_back(make_int4(gblk[g] + h0, h1 - h0, glow[g] + lidx, lidx));
+      P.lmax = std::max(P.lmax, h1 - h0);
+    }
+  }
+  // HH table
+  P.hoff.assign(nkrow + 1, 0);
+  P.hent.clear();
+  for (int kr = 0; kr < nkrow; ++kr) {
+    P.hent.insert(P.hent.end(), hh[kr].begin(), hh[kr].end());
+    P.hoff[kr + 1] = uint32_t(P.hent.size());
+  }
+  P.hent.push_back(0);
+  // A shared-memory wavefront of the up pass serves G = 32/rt lanes reading rt*4-byte
+  // columns from M = G bank groups (column x sits in group x % M). Each thread's LL list and
+  // each warp step's cross lists are put in slot order by an edge colouring of lanes x bank
+  // groups (as the SELL schedule is), so that the lanes of a wavefront read distinct groups.
+  const int Gl = 32 / rt, M = Gl, nwarps = kKronThreads / 32;
+  const int nthr = int(P.thr.size());
+  // LL: per thread, kKronLL slots of (delta << 2) | valid << 1 | sign. The group of an LL
+  // source is (block start + lidx + delta) % M; lanes of one run share the block start, so
+  // the colouring uses (lidx + delta) % M.
+  P.lent.assign(size_t(kKronThreads) * kKronLL, 0);
+  for (int w = 0; w < nwarps; ++w)
+    for (int q = 0; q < 32 / Gl; ++q) {
+      std::vector<std::pair<int, int>> E;
+      std::vector<std::pair<int, int>> who;  // (thread, entry)
+      for (int l = 0; l < Gl; ++l) {
+        const int t = w * 32 + q * Gl + l;
+        if (t >= nthr || P.thr[t].y == 0) continue;
+        const auto& lst = ll[P.thr[t].z];
+        for (int j = 0; j < int(lst.size()); ++j) {
+          const int64_t col = int64_t(P.thr[t].w) + (lst[j] >> 1);
+          E.push_back({l, int(((col % M) + M) % M)});
+          who.push_back({t, j});
+        }
+      }
+      std::vector<int> colour;
+      const int D = E.empty() ? 0 : edge_colour(Gl, M, E, colour);
+      std::vector<int> next(Gl, 0);
+      for (size_t i = 0; i < who.size(); ++i) {
+        const int t = who[i].first, j = who[i].second, l = t - w * 32 - q * Gl;
+        const int slot = (D > 0 && D <= kKronLL) ? colour[i] : next[l]++;  // else natural order
+        const int32_t e = ll[P.thr[t].z][j];
+        P.lent[size_t(t) * kKronLL + slot] = ((e >> 1) << 2) | 2 | (e & 1);
+      }
+    }
+  // cross entries, warp by warp and step by step, lane-interleaved; a lane without an entry
+  // in a slot reads a zero slot dim + z whose bank group no lane of its wavefront uses there
+  P.xoff.assign(nwarps + 1, 0);
+  P.xwid.assign(size_t(nwarps) * P.lmax + 1, 0);
+  P.xent.clear();
+  for (int w = 0; w < nwarps; ++w) {
+    P.xoff[w] = uint32_t(P.xent.size() / 32);
+    for (int k = 0; k < P.lmax; ++k) {
+      std::vector<const std::vector<uint32_t>*> mine(32, nullptr);
+      for (int l = 0; l < 32; ++l) {
+        const int t = w * 32 + l;
+        if (t >= nthr || k >= P.thr[t].y) continue;
+        mine[l] = &cross[size_t(P.bcol[P.thr[t].x + k]) + size_t(P.thr[t].w)];
+      }
+      std::vector<std::vector<int>> slot_of(32);
+      int wd = 0;
+      for (int q = 0; q < 32 / Gl; ++q) {
+        std::vector<std::pair<int, int>> E;
+        std::vector<std::pair<int, int>> who;
+        for (int l = 0; l < Gl; ++l) {
+          const int lane = q * Gl + l;
+          if (!mine[lane]) continue;
+          slot_of[lane].assign(mine[lane]->size(), 0);
+          for (size_t j = 0; j < mine[lane]->size(); ++j) {
+            E.push_back({l, int(((*mine[lane])[j] & 0x7fffffffu) % uint32_t(M))});
+            who.push_back({lane, int(j)});
+          }
+        }
+        std::vector<int> colour;
+        const int D = E.empty() ? 0 : edge_colour(Gl, M, E, colour);
+        if (D < 0) return false;
+        for (size_t i = 0; i < who.size(); ++i) slot_of[who[i].first][who[i].second] = colour[i];
+        wd = std::max(wd, D);
+      }
+      P.xwid[size_t(w) * P.lmax + k] = uint32_t(wd);
+      const size_t base = P.xent.size();
+      P.xent.resize(base + size_t(wd) * 32, 0xffffffffu);
+      std::vector<char> used(size_t(wd) * 32 * M / Gl + 1, 0);  // [slot][group q][residue]
+      const int ngr = 32 / Gl;
+      for (int lane = 0; lane < 32; ++lane) {
+        if (!mine[lane]) continue;
+        for (size_t j = 0; j < mine[lane]->size(); ++j) {
+          const uint32_t e = (*mine[lane])[j];
+          const int sl = slot_of[lane][j];
+          P.xent[base + size_t(sl) * 32 + lane] = e;
+          used[(size_t(sl) * ngr + lane / Gl) * M + (e & 0x7fffffffu) % uint32_t(M)] = 1;
+        }
+      }
+      for (int sl = 0; sl < wd; ++sl)
+        for (int lane = 0; lane < 32; ++lane) {
+          uint32_t& e = P.xent[base + size_t(sl) * 32 + lane];
+          if (e != 0xffffffffu) continue;
+          int fr = 0;
+          const size_t u0 = (size_t(sl) * ngr + lane / Gl) * M;
+          while (fr < M && used[u0 + fr]) ++fr;
+          if (fr == M) fr = 0;
+          e = uint32_t(dim) + uint32_t(((fr - int(dim % M)) % M + M) % M);
+          used[u0 + fr] = 1;
+        }
+    }
+  }
+  P.xoff[nwarps] = uint32_t(P.xent.size() / 32);
+  P.xent.push_back(uint32_t(dim));
+  return true;
+}
+
+// Kronecker schedule of the FP32 up pass, for uniform real tables whose rows the up pass
+// stages in shared memory: the split with the most hops inside a part among those that fit.
+int build_kron(edg_sector_s* s, SpinBasis& B, const std::vector<uint32_t>& off, const std::vector<uint32_t>& src,
+               const std::vector<uint32_t>& sgn) {
+  cudaStream_t st = s->stream;
+  B.kron_m = 0;
+  const int ns = s->model.ns;
+  const int64_t dim = B.dim;
+  if (dim < 2 || B.nnz == 0 || up_rows_per_cta(dim, sizeof(float)) == 0 || ns < 2) return EDG_OK;
+  std::vector<uint32_t> map(dim);
+  EDG_CUDA(cudaMemcpyAsync(map.data(), B.map.p, dim * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  EDG_CUDA(cudaStreamSynchronize(st));
+  const int rt = up_rows_per_cta(dim, sizeof(float));
+  // Among the splits whose block tables fit in shared memory next to the staged rows: two
+  // CTAs per SM when the rows alone allow it, then the most hops inside a part, then the
+  // split nearer the middle. (A split near one end has blocks of one or two columns: nearly
+  // every hop counts as HH, but its HH table is a per-column table again.)
+  const bool two_rows_fit = size_t(dim + kUpZeroSlots) * rt * sizeof(float) <= kUpSmemTwoPerSM;
+  auto score = [&](const KronPlan& P) {
+    const size_t sm = kron_smem(dim, rt, int(P.bcol.size()), int(P.hent.size()));
+    return std::make_tuple(int(!two_rows_fit || sm <= kUpSmemTwoPerSM), P.within, -std::abs(2 * P.m - ns));
+  };
+  KronPlan best, cand;
+  for (int m = 1; m < ns; ++m) {
+    if (!plan_kron(m, rt, dim, map, off, src, sgn, cand)) continue;
+    if (kron_smem(dim, rt, int(cand.bcol.size()), int(cand.hent.size())) > kUpSmemOnePerSM) continue;
+    if (best.m == 0 || score(cand) > score(best)) std::swap(best, cand);
+  }
+  if (best.m == 0) return EDG_OK;
+  EDG_CHECK(B.kron_thr.alloc(kKronThreads, st, "Kronecker schedule"));
+  std::vector<int4> thr(kKronThreads, make_int4(0, 0, 0, 0));
+  std::copy(best.thr.begin(), best.thr.end(), thr.begin());
+  EDG_CHECK(B.kron_bcol.alloc(best.bcol.size(), st, "Kronecker schedule"));
+  EDG_CHECK(B.kron_hoff.alloc(best.hoff.size(), st, "Kronecker schedule"));
+  EDG_CHECK(B.kron_hent.alloc(best.hent.size(), st, "Kronecker schedule"));
+  EDG_CHECK(B.kron_lent.alloc(best.lent.size(), st, "Kronecker schedule"));
+  EDG_CHECK(B.kron_xent.alloc(best.xent.size(), st, "Kronecker schedule"));
+  EDG_CHECK(B.kron_xoff.alloc(best.xoff.size(), st, "Kronecker schedule"));
+  EDG_CHECK(B.kron_xwid.alloc(best.xwid.size(), st, "Kronecker schedule"));
+  auto up = [&](void* d, const void* h, size_t bytes) { return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st); };
+  EDG_CUDA(up(B.kron_thr.p, thr.data(), thr.size() * sizeof(int4)));
+  EDG_CUDA(up(B.kron_bcol.p, best.bcol.data(), best.bcol.size() * sizeof(int32_t)));
+  EDG_CUDA(up(B.kron_hoff.p, best.hoff.data(), best.hoff.size() * sizeof(uint32_t)));
+  EDG_CUDA(up(B.kron_hent.p, best.hent.data(), best.hent.size() * sizeof(int32_t)));
+  EDG_CUDA(up(B.kron_lent.p, best.lent.data(), best.lent.size() * sizeof(int32_t)));
+  EDG_CUDA(up(B.kron_xent.p, best.xent.data(), best.xent.size() * sizeof(uint32_t)));
+  EDG_CUDA(up(B.kron_xoff.p, best.xoff.data(), best.xoff.size() * sizeof(uint32_t)));
+  EDG_CUDA(up(B.kron_xwid.p, best.xwid.data(), best.xwid.size() * sizeof(uint32_t)));
+  EDG_CUDA(cudaStreamSynchronize(st));  // host plan goes out of scope
+  B.kron_nthr = int(best.thr.size());
+  B.kron_lmax = best.lmax;
+  B.kron_nkrow = int(best.bcol.size());
+  B.kron_nhent = int(best.hent.size());
+  B.kron_m = best.m;
+  return EDG_OK;
+}
+
 // SELL-32 copy of a gather table, built on the host from the device CSR (the tables are
 // O(DimUp) -- about 1 MB for a 4x4 lattice -- so this is a one-off of milliseconds).
 int build_sell(edg_sector_s* s, SpinBasis& B) {
@@ -698,6 +965,11 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
         B.p16_negoff = negoff;
       }
     }
+  }
+  if (uniform && B.nnz > 0) {
+    std::vector<uint32_t> sg(B.nnz);
+    for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
+    EDG_CHECK(build_kron(s, B, off, src, sg));
   }
   // column-split copy for rows that do not fit shared memory whole (FP64 rows above 227 KB)
   B.split_parts = 0;

@@ -328,7 +328,7 @@ int edg_sector_autotune(edg_sector* s, int precision, int reps, double* ms, int*
 int edg_sector_set_kernels(edg_sector* s, int precision, int candidate) {
   EDG_CHECK(check_sector(s));
   EDG_ARG(precision == EDG_PREC_F64 || precision == EDG_PREC_F32, "edg_sector_set_kernels: precision=%d", precision);
-  const int nup = precision == EDG_PREC_F32 ? 3 : 1;
+  const int nup = precision == EDG_PREC_F32 ? 4 : 1;
   EDG_ARG(candidate >= 0 && candidate < 3 * nup, "edg_sector_set_kernels: candidate=%d outside 0..%d", candidate,
           3 * nup - 1);
   const int f32 = precision == EDG_PREC_F32;

@@ -192,7 +192,42 @@ struct SpinBasis {
   DevBuf<uint32_t> group_rows;
   int groups = 0;
   int group_max = 0;            // most rows in one group
+  // Kronecker schedule of the FP32 up pass (uniform real tables). The sites split at bit
+  // kron_m into a low part (bits below kron_m) and a high part. Ascending order keeps the
+  // configurations of one high part h together: a block of consecutive columns, one per low
+  // part l. A hop inside the low part (LL) keeps h, so its source sits in the same block at
+  // a column offset that depends on l only; a hop inside the high part (HH) keeps l and moves
+  // to another block of the same size at an offset that depends on h only; the remaining
+  // (cross) hops change both and keep a per-column list. Blocks are grouped by popcount(h)
+  // ("group"), every block of a group has the same low parts, and block rows are numbered
+  // group-major (krow). A thread of the up pass owns one low part l of one group and a run of
+  // consecutive blocks of that group: its LL offsets stay in registers for the whole launch,
+  // its HH offsets are shared with the lanes on the same block, and only its cross hops read
+  // a per-column table.
+  int kron_m = 0;                 // 0: no Kronecker schedule
+  int kron_nthr = 0;              // threads with work (of kKronThreads)
+  int kron_lmax = 0;              // most blocks owned by one thread
+  int kron_nkrow = 0, kron_nhent = 0;  // block rows, HH entries
+  DevBuf<int4> kron_thr;          // per thread: first krow, blocks, low row (group base + lidx), lidx
+  DevBuf<int32_t> kron_bcol;      // per krow: first column of the block
+  DevBuf<uint32_t> kron_hoff;     // per krow: HH entry range [hoff[krow], hoff[krow+1])
+  DevBuf<int32_t> kron_hent;      // HH entries: (column delta << 1) | sign
+  DevBuf<int32_t> kron_lent;      // per thread: kKronLL LL slots (delta << 2) | valid << 1 | sign,
+                                  // in bank-conflict-free slot order
+  DevBuf<uint32_t> kron_xent;     // cross entries, warp by warp, step by step, lane-interleaved,
+                                  // bank-conflict-free slot order: source column | sign << 31
+                                  // (padding: a zero slot)
+  DevBuf<uint32_t> kron_xoff;     // per warp: first slot
+  DevBuf<uint32_t> kron_xwid;     // per warp and step (stride kron_lmax): slots
 };
+
+constexpr int kKronThreads = 512;  // threads per CTA of the Kronecker up pass
+constexpr int kKronLL = 12;        // LL entries per low part held in registers
+// Shared memory of the Kronecker up pass: rt staged rows plus the zero slots, then the block
+// tables (first column and HH range per block row, HH entries).
+inline size_t kron_smem(int64_t dimup, int rt, int nkrow, int nhent) {
+  return size_t(dimup + 32) * rt * sizeof(float) + (size_t(2) * nkrow + 1 + nhent) * sizeof(int32_t);
+}
 
 // Directed bond list for one spin: Hij(a,b) != 0, a != b, value = matrix element used when
 // an electron moves from b to a (direct form Hij(a,b), stored form conjg(Hij(a,b))).
@@ -248,7 +283,8 @@ struct edg_sector_s {
   // H x v kernel choice per vector precision ([0] FP64, [1] FP32), set by edg_sector_autotune:
   // down pass 0 = hop-balanced row groups, 1 = block-staged (one CTA per SM), 2 = block-staged
   // (two CTAs per SM); up pass (FP32) 0 = 32-bit SELL schedule, 1 = packed 16-bit schedule
-  // with negated copies, 2 = packed 16-bit schedule with sign bits. 0/0 until tuned.
+  // with negated copies, 2 = packed 16-bit schedule with sign bits, 3 = Kronecker schedule.
+  // 0/0 until tuned.
   int hxv_dw[2] = {0, 0};
   int hxv_up[2] = {0, 0};
 };

@@ -165,19 +165,32 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 // ONE: one CTA per SM (the staged rows take more than half of shared memory); the 64
 // registers per thread this allows carry the next batch of entries while the current one is
 // applied.
+// The Lanczos-fused form (LZ) runs 768 threads per CTA: with two CTAs per SM that leaves 40
+// registers per thread for the epilogue's FP64 state next to the batch of entries in flight
+// (at 1024 threads and 32 registers the batch no longer fit and the pass became latency-bound).
+template <bool LZ>
+constexpr int up_threads() { return LZ ? 768 : 1024; }
+
 template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE>
-__global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+__global__ void __launch_bounds__(up_threads<LZ>(), ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   if (!select_column(a)) return;
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
   V* S = reinterpret_cast<V*>(smem_up);
   const int64_t dimup = a.dimup;
-  double sc = 1.0, cc = 0.0, pa = 0.0;
+  // Lanczos scalars 1/bn[j] and bn[j]/bn[j-1]: the epilogue reads them from shared memory,
+  // so that they take no registers in the gather loop (the two-CTA FP32 form has 32)
+  __shared__ double s_lz[2];
+  double pa = 0.0, sc = 1.0;
   if (LZ) {
     sc = 1.0 / a.bn[a.jstep];
-    cc = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+    if (threadIdx.x == 0) {
+      s_lz[0] = sc;
+      s_lz[1] = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+    }
   }
   const T hs = LZ ? T(double(sl.h) * sc) : sl.h;
+  const double scn = UNIFORM ? 1.0 : sc;  // per-term scale of non-uniform values
   for (int zq = threadIdx.x; zq < kUpZeroSlots; zq += blockDim.x) {  // padding targets
     V z;
     T* zs = reinterpret_cast<T*>(&z);
@@ -250,7 +263,7 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, Sel
           }
 #pragma unroll
           for (int u = 0; u < kUpBatch; ++u) {
-            const T h = UNIFORM ? flip_sign(hs, e[u]) : (LZ ? T(double(hv_[u]) * sc) : hv_[u]);
+            const T h = UNIFORM ? flip_sign(hs, e[u]) : (LZ ? T(double(hv_[u]) * scn) : hv_[u]);
             const V x = S[e[u] & 0x7fffffffu];
             Fma<T, RT>::run(h, reinterpret_cast<const T*>(&x), acc);
           }
@@ -258,6 +271,8 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, Sel
       }
       if (LZ) {
         // w = Hv - c * uprev ;  partial <v, w> with v = sc * u (staged in S)
+        const volatile double* lz = s_lz;
+        const double sc = lz[0], cc = lz[1];
         const V xc = S[iup];
         const T* xs = reinterpret_cast<const T*>(&xc);
 #pragma unroll
@@ -285,6 +300,177 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, Sel
       double t = 0.0;
       for (int q = 0; q < int(blockDim.x >> 5); ++q) t += s_red[q];
       a.partial[blockIdx.x] = t;
+    }
+    finish_in_last_block(a.partial, gridDim.x, a.red_out, 0);
+  }
+}
+
+// FP32 up pass over the Kronecker schedule (SpinBasis::kron_*). The CTA stages RT rows
+// interleaved in shared memory as k_up_smem does; thread t owns one low part (lidx) of one
+// group and a run of consecutive blocks of that group, the same for every row block of the
+// launch. Its LL hops are (column offset, sign) pairs loaded once into registers; the HH hops
+// of a block are one short list shared by every lane on that block (the same cached words);
+// only the cross hops read a per-column table, lane-interleaved per warp and step. Lanes of a
+// warp hold consecutive lidx, so the reads and writes of Hv stay coalesced within a block.
+struct KronArgs {
+  const int4* __restrict__ thr;
+  const int32_t* __restrict__ bcol;
+  const uint32_t* __restrict__ hoff;
+  const int32_t* __restrict__ hent;
+  const int32_t* __restrict__ lent;
+  const uint32_t* __restrict__ xent;
+  const uint32_t* __restrict__ xoff;
+  const uint32_t* __restrict__ xwid;
+  int nthr, lmax;
+  int nkrow, nhent;  // block rows, HH entries (staged in shared memory)
+  float h;
+};
+
+constexpr int kKronX = 8;  // cross entries of a step loaded together into registers
+
+// h with its sign flipped when bit 0 of e is set
+__device__ __forceinline__ float flip_bit0(float h, uint32_t e) { return __uint_as_float(__float_as_uint(h) ^ (e << 31)); }
+
+template <int RT, bool LZ, bool ONE>
+__global__ void __launch_bounds__(kKronThreads, ONE ? 1 : 2) k_up_kron(HxvArgs<float> a, KronArgs q, int64_t nrowblk) {
+  if (!select_column(a)) return;
+  using V = typename VecT<float, RT>::type;
+  extern __shared__ __align__(16) unsigned char smem_kr[];
+  V* S = reinterpret_cast<V*>(smem_kr);
+  const int64_t dimup = a.dimup;
+  __shared__ double s_lz[2];  // 1/bn[j], bn[j]/bn[j-1]: read by the epilogue only
+  double pa = 0.0;
+  float hs = q.h;
+  if (LZ) {
+    const double sc = 1.0 / a.bn[a.jstep];
+    if (threadIdx.x == 0) {
+      s_lz[0] = sc;
+      s_lz[1] = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+    }
+    hs = float(double(q.h) * sc);
+  }
+  for (int zq = threadIdx.x; zq < kUpZeroSlots; zq += blockDim.x) {  // padding targets
+    V z;
+    float* zs = reinterpret_cast<float*>(&z);
+#pragma unroll
+    for (int r = 0; r < RT; ++r) zs[r] = 0.f;
+    S[dimup + zq] = z;
+  }
+  // the per-block tables (first column, HH range, HH entries) sit after the staged rows:
+  // every step reads them, and from L2 their loads were a dependent chain ahead of each gather
+  int32_t* s_bcol = reinterpret_cast<int32_t*>(S + dimup + kUpZeroSlots);
+  uint32_t* s_hoff = reinterpret_cast<uint32_t*>(s_bcol + q.nkrow);
+  int32_t* s_hent = reinterpret_cast<int32_t*>(s_hoff + q.nkrow + 1);
+  for (int i = threadIdx.x; i < q.nkrow; i += blockDim.x) s_bcol[i] = q.bcol[i];
+  for (int i = threadIdx.x; i <= q.nkrow; i += blockDim.x) s_hoff[i] = q.hoff[i];
+  for (int i = threadIdx.x; i < q.nhent; i += blockDim.x) s_hent[i] = q.hent[i];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int4 me = t < q.nthr ? q.thr[t] : make_int4(0, 0, 0, 0);
+  const int krow0 = me.x, len = me.y, lidx = me.w;
+  // this thread's LL slots, held in registers for the whole launch (the empty asm keeps
+  // the compiler from reloading them from the table inside the loops)
+  // (column offsets as 16-bit halves, two per register)
+  uint32_t lld[kKronLL / 2];
+  uint32_t lsg = 0, lval = 0;
+#pragma unroll
+  for (int j = 0; j < kKronLL; ++j) {
+    const int32_t e = q.lent[t * kKronLL + j];
+    const uint32_t d16 = uint32_t(e >> 2) & 0xffffu;
+    if (j & 1) lld[j >> 1] |= d16 << 16;
+    else lld[j >> 1] = d16;
+    lval |= uint32_t((e >> 1) & 1) << j;
+    lsg |= uint32_t(e & 1) << j;
+  }
+#pragma unroll
+  for (int j = 0; j < kKronLL / 2; ++j) asm volatile("" : "+r"(lld[j]));
+  asm volatile("" : "+r"(lval), "+r"(lsg));
+  int wlen = len;  // steps of the warp: the longest run among its lanes
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wlen = max(wlen, __shfl_xor_sync(0xffffffffu, wlen, o));
+  const uint32_t xbase = q.xoff[warp];
+  const uint32_t* __restrict__ xw = q.xwid + warp * q.lmax;
+  for (int64_t rb = blockIdx.x; rb < nrowblk; rb += gridDim.x) {
+    const int64_t r0 = rb * RT;
+    for (int64_t j = threadIdx.x; j < dimup; j += blockDim.x) {
+      V x;
+      float* xs = reinterpret_cast<float*>(&x);
+#pragma unroll
+      for (int r = 0; r < RT; ++r) xs[r] = (r0 + r < a.dimdw) ? a.v[(r0 + r) * dimup + j] : 0.f;
+      S[j] = x;
+    }
+    __syncthreads();
+    uint32_t xs = xbase;
+    for (int k = 0; k < wlen; ++k) {
+      const int wd = int(xw[k]);
+      if (k < len) {
+        // the step's loads from HBM/L2 first, all in flight together: its cross entries and
+        // the down pass's partial sums; the shared-memory terms then cover their latency
+        uint32_t xe[kKronX];
+#pragma unroll
+        for (int j = 0; j < kKronX; ++j) xe[j] = j < wd ? __ldg(q.xent + size_t(xs + j) * 32 + lane) : 0u;
+        const int kr = krow0 + k;
+        const int c = s_bcol[kr] + lidx;
+        float acc[RT];
+#pragma unroll
+        for (int r = 0; r < RT; ++r) acc[r] = (r0 + r < a.dimdw) ? a.hv[(r0 + r) * dimup + c] : 0.f;
+#pragma unroll
+        for (int j = 0; j < kKronLL; ++j) {
+          if ((lval >> j) & 1u) {
+            const int d = (j & 1) ? int(lld[j >> 1]) >> 16 : int(int16_t(lld[j >> 1] & 0xffffu));
+            const V x = S[c + d];
+            Fma<float, RT>::run(flip_bit0(hs, lsg >> j), reinterpret_cast<const float*>(&x), acc);
+          }
+        }
+        const uint32_t h1 = s_hoff[kr + 1];
+        for (uint32_t p = s_hoff[kr]; p < h1; ++p) {
+          const int32_t e = s_hent[p];
+          const V x = S[c + (e >> 1)];
+          Fma<float, RT>::run(flip_bit0(hs, uint32_t(e)), reinterpret_cast<const float*>(&x), acc);
+        }
+#pragma unroll
+        for (int j = 0; j < kKronX; ++j) {
+          if (j < wd) {
+            const V x = S[xe[j] & 0x7fffffffu];
+            Fma<float, RT>::run(flip_sign(hs, xe[j]), reinterpret_cast<const float*>(&x), acc);
+          }
+        }
+        for (int j = kKronX; j < wd; ++j) {
+          const uint32_t e = __ldg(q.xent + size_t(xs + j) * 32 + lane);
+          const V x = S[e & 0x7fffffffu];
+          Fma<float, RT>::run(flip_sign(hs, e), reinterpret_cast<const float*>(&x), acc);
+        }
+        if (LZ) {
+          const volatile double* lz = s_lz;
+          const double sc = lz[0], cc = lz[1];
+          const V xc = S[c];
+          const float* xv = reinterpret_cast<const float*>(&xc);
+#pragma unroll
+          for (int r = 0; r < RT; ++r)
+            if (r0 + r < a.dimdw) {
+              const int64_t e = (r0 + r) * dimup + c;
+              const float wt = float(double(acc[r]) - cc * double(a.uprev[e]));
+              pa = __fma_rn(double(xv[r]) * sc, double(wt), pa);
+              __stcs(a.hv + e, wt);
+            }
+        } else {
+#pragma unroll
+          for (int r = 0; r < RT; ++r)
+            if (r0 + r < a.dimdw) __stcs(a.hv + (r0 + r) * dimup + c, acc[r]);
+        }
+      }
+      xs += uint32_t(wd);
+    }
+    __syncthreads();
+  }
+  if (LZ) {  // block partial of <v, w>, fixed order
+    __shared__ double s_red[32];
+    for (int o = 16; o > 0; o >>= 1) pa += __shfl_down_sync(0xffffffffu, pa, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = pa;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tt = 0.0;
+      for (int w = 0; w < int(blockDim.x >> 5); ++w) tt += s_red[w];
+      a.partial[blockIdx.x] = tt;
     }
     finish_in_last_block(a.partial, gridDim.x, a.red_out, 0);
   }
@@ -1094,7 +1280,7 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
   if (LZ && g > kRedBlocks) g = kRedBlocks;  // one partial per block in the reduction scratch
-  kern<<<dim3(int(g), a.ncols), 1024, smem, st>>>(a, sl, nrb);
+  kern<<<dim3(int(g), a.ncols), up_threads<LZ>(), smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   if (grid) *grid = int(g);
   return EDG_OK;
@@ -1186,10 +1372,49 @@ bool launch_up_p16(const HxvArgs<float>& a, const SpinBasis& B, cudaStream_t st,
   return true;
 }
 
+// Kronecker-schedule FP32 up pass (k_up_kron); returns false when the sector has no schedule.
+template <int RT, bool LZ>
+int launch_up_kron_rt(const HxvArgs<float>& a, const KronArgs& q, cudaStream_t st, int sms) {
+  const size_t smem = kron_smem(a.dimup, RT, q.nkrow, q.nhent);
+  const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
+  auto kern = per_sm == 2 ? k_up_kron<RT, LZ, false> : k_up_kron<RT, LZ, true>;
+  if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int64_t nrb = (a.dimdw + RT - 1) / RT;
+  int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
+  if (LZ && g > kRedBlocks) g = kRedBlocks;
+  kern<<<dim3(int(g), a.ncols), kKronThreads, smem, st>>>(a, q, nrb);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+template <bool LZ>
+bool launch_up_kron(const HxvArgs<float>& a, const SpinBasis& B, cudaStream_t st, int sms, int* status) {
+  if (B.kron_m == 0 || a.upv != 3) return false;
+  KronArgs q;
+  q.thr = B.kron_thr.p;
+  q.bcol = B.kron_bcol.p;
+  q.hoff = B.kron_hoff.p;
+  q.hent = B.kron_hent.p;
+  q.lent = B.kron_lent.p;
+  q.xent = B.kron_xent.p;
+  q.xoff = B.kron_xoff.p;
+  q.xwid = B.kron_xwid.p;
+  q.nthr = B.kron_nthr;
+  q.lmax = B.kron_lmax;
+  q.nkrow = B.kron_nkrow;
+  q.nhent = B.kron_nhent;
+  q.h = float(B.sell_h);
+  const int rt = up_rows_per_cta(a.dimup, sizeof(float));
+  *status = rt == 4 ? launch_up_kron_rt<4, LZ>(a, q, st, sms)
+          : rt == 2 ? launch_up_kron_rt<2, LZ>(a, q, st, sms)
+                    : launch_up_kron_rt<1, LZ>(a, q, st, sms);
+  return true;
+}
+
 template <typename T, bool FIRST, bool LZ>
 int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms, int* grid) {
   if constexpr (std::is_same<T, float>::value && !FIRST) {
     int status = EDG_OK;
+    if (launch_up_kron<LZ>(a, B, st, sms, &status)) return status;
     if (launch_up_p16<LZ>(a, B, st, sms, &status)) return status;
   }
   const int rt = up_rows_per_cta(a.dimup, sizeof(T));
@@ -1393,19 +1618,19 @@ int hxv_block_lz(edg_sector_s* s, int ncols, const int* active, const T* u, cons
   EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nullptr)));
   return EDG_OK;
 }
-// Autotuner: every down-pass x up-pass pair (3 x 3 for FP32, 3 x 1 for FP64; a pair whose
+// Autotuner: every down-pass x up-pass pair (3 x 4 for FP32, 3 x 1 for FP64; a pair whose
 // kernel does not apply to the sector falls back to the default kernel and times like it) on
 // `reps` H x v of scratch vectors after one untimed application, timed with CUDA events on
 // the sector's stream; the fastest pair becomes the sector's choice for precision T. Its
-// arithmetic is unchanged in FP64 (every pair gives the same bits); in FP32 the packed up
-// passes sum the terms of a row in another order.
+// arithmetic is unchanged in FP64 (every pair gives the same bits); in FP32 the packed and
+// Kronecker up passes sum the terms of a row in another order.
 template <typename T>
 int hxv_autotune(edg_sector_s* s, int reps, double* ms, int* nc, int* best) {
   if (s->cplx || s->form != EDG_FORM_STORED) {
     set_error("edg_sector_autotune: only the real stored form has kernel variants");
     return EDG_ERR_UNSUPPORTED;
   }
-  const int nup = sizeof(T) == 4 ? 3 : 1;
+  const int nup = sizeof(T) == 4 ? 4 : 1;
   const int ncand = 3 * nup;
   cudaStream_t st = s->stream;
   DevBuf<T> x, y;

@@ -221,7 +221,7 @@ class Sector:
     def autotune(self, precision: int = L.EDG_PREC_F32, reps: int = 5) -> dict:
         """Time the H x v kernel variants on this sector and keep the fastest for `precision`
         (edg_sector_autotune): {"ms": per-candidate ms per H x v, "best": index kept}."""
-        ms = np.zeros(9)
+        ms = np.zeros(64)  # room for every candidate of either precision
         nc, best = C.c_int(), C.c_int()
         L.check(L.lib().edg_sector_autotune(self.handle, precision, reps, _pd(ms), C.byref(nc), C.byref(best)),
                 "edg_sector_autotune")

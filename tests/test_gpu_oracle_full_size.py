@@ -69,6 +69,33 @@ def test_stored_hxv_bit_exact_full_size(models, oracle_stored):
     assert np.array_equal(got, ref), f"max |diff| {np.abs(got - ref).max()}"
 
 
+def test_f32_hxv_every_up_pass_full_size(models, oracle_stored):
+    """FP32 H x v of the benchmarked sector on each FP32 up pass (SELL, packed 16-bit with
+    negated copies or sign bits, Kronecker) after the default down pass, against the oracle's
+    FP64 spMatVec: 2e-6 of max|Hv|. The Kronecker pass sums each element's terms in another
+    order than the SELL pass, so its result differs from it in rounding only."""
+    import torch
+    em, _ = models
+    s = _on_torch_stream(E.Sector(em, 8, 8, E.EDG_FORM_STORED))
+    v = O.random_vector(33, s.dim)
+    ref = oracle_stored.matvec_d(v)
+    scale = np.abs(ref).max()
+    x = torch.from_numpy(v).cuda().float()
+    got = {}
+    for up in range(4):
+        s.set_kernels(up, E.EDG_PREC_F32)  # candidate 4*down + up, down pass 0
+        y = torch.empty_like(x)
+        torch.cuda.synchronize()
+        L.check(L.lib().edg_hxv_dev_f32(s.handle, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())), "hxv")
+        torch.cuda.synchronize()
+        got[up] = y.double().cpu().numpy()
+        assert np.abs(got[up] - ref).max() <= 2e-6 * scale, (up, np.abs(got[up] - ref).max() / scale)
+    assert not np.array_equal(got[3], got[0])  # the Kronecker schedule is the one that ran
+    del x, y
+    s.delete()
+    torch.cuda.empty_cache()
+
+
 def test_direct_hxv_bit_exact_full_size(models):
     em, om = models
     s = _on_torch_stream(E.Sector(em, 8, 8, E.EDG_FORM_DIRECT))
@@ -159,8 +186,10 @@ def test_fp32_gf_weights_vs_oracle_chain():
         assert np.all(np.abs(moments(c.poles, c.weight) - m_o) <= tol * np.abs(m_o)), prec
         for pk, wk in zip(p_o[conv], w_o[conv]):
             near = np.abs(c.poles - pk) <= 1e-4
-            assert near.any(), (prec, pk)
-            # a recurrence that loses orthogonality may repeat a converged pole: the copies
-            # share its weight
+            # a recurrence that loses orthogonality may repeat a converged pole: the copies sit
+            # at its position and share its weight; an unconverged Ritz value that happens to
+            # lie within 1e-4 of it carries no weight of its own
+            copies = np.abs(c.poles - pk) <= tol * max(1.0, abs(pk))
+            assert copies.any(), (prec, pk, c.poles[near])
             assert abs(c.weight[near].sum() - wk) <= tol, (prec, pk, wk, c.weight[near].sum())
-            assert np.abs(c.poles[near] - pk).max() <= tol * max(1.0, abs(pk)), (prec, pk)
+            assert c.weight[near & ~copies].sum() <= tol, (prec, pk, c.poles[near], c.weight[near])
