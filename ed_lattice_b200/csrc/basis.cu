@@ -782,6 +782,117 @@ int build_kron(edg_sector_s* s, SpinBasis& B, const std::vector<uint32_t>& off, 
   return EDG_OK;
 }
 
+// Tables of the non-default H x v kernels (SpinBasis::rowblk, p16_*, kron_*), built from the
+// device CSR on first use: edg_sector_autotune and edg_sector_set_kernels ask for them, the
+// sector loops of a finite-temperature run (default kernels) never pay for them.
+int build_variants(edg_sector_s* s, SpinBasis& B) {
+  if (B.variants || s->cplx || B.dim == 0) return EDG_OK;
+  cudaStream_t st = s->stream;
+  const int64_t dim = B.dim;
+  std::vector<uint32_t> off(dim + 1), src(B.nnz + 1);
+  std::vector<double> val(B.nnz + 1);
+  EDG_CUDA(cudaMemcpyAsync(off.data(), B.off.p, (dim + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  if (B.nnz) {
+    EDG_CUDA(cudaMemcpyAsync(src.data(), B.src.p, B.nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaMemcpyAsync(val.data(), B.val64.p, B.nnz * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  EDG_CUDA(cudaStreamSynchronize(st));
+  const int64_t nsl = (dim + 31) / 32;
+  const bool uniform = B.sell_uniform;
+  const double hsgn = B.sell_h;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // contiguous blocks balanced by hops for the block-staged down pass, in two shapes: about
+  // one block per SM (1024-thread CTAs) and two per SM (512-thread CTAs); each a multiple
+  // of the SM count, enough blocks that one block's rows of a 256-column FP32 slab (1 KB per
+  // row) stay within 112 KB per SM
+  for (int shape = 0; shape < 2; ++shape) {
+    const int per_sm = shape + 1;
+    int64_t tot = 0;
+    for (int64_t r = 0; r < dim; ++r) tot += 1 + int64_t(off[r + 1] - off[r]);
+    int64_t CG = std::max<int64_t>(1, std::min<int64_t>(int64_t(sms) * per_sm, dim));
+    std::vector<uint32_t> coff;
+    int mx = 0;
+    for (int iter = 0; iter < 16; ++iter) {
+      coff.assign(1, 0u);
+      int64_t acc = 0, g = 1;
+      mx = 0;
+      uint32_t start = 0;
+      for (int64_t r = 0; r < dim; ++r) {
+        acc += 1 + int64_t(off[r + 1] - off[r]);
+        if (g < CG && acc * CG >= g * tot) {  // close block g-1 after row r
+          coff.push_back(uint32_t(r + 1));
+          mx = std::max<int>(mx, int(r + 1 - start));
+          start = uint32_t(r + 1);
+          ++g;
+        }
+      }
+      coff.push_back(uint32_t(dim));
+      mx = std::max<int>(mx, int(dim - start));
+      if (mx <= 112 / per_sm || CG >= dim) break;
+      CG = std::min<int64_t>(dim, CG + sms);
+    }
+    SpinBasis::RowBlocks& rb = B.rowblk[shape];
+    rb.max_rows = mx;
+    rb.count = int(coff.size() - 1);
+    EDG_CHECK(rb.off.alloc(coff.size(), st, "row blocks"));
+    EDG_CUDA(cudaMemcpyAsync(rb.off.p, coff.data(), coff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+  }
+  // Packed 16-bit schedule for the two-row FP32 up pass (slot counts rounded to 2)
+  B.p16_negoff = 0;
+  B.p16_ent.reset();
+  B.p16_off.reset();
+  B.p16f_ent.reset();
+  {
+    const uint32_t negoff = uint32_t((dim + kUpZeroSlots + 31) / 32 * 32);
+    if (uniform && B.nnz > 0 && 2 * int64_t(negoff) <= 32768) {
+      std::vector<uint32_t> sg(B.nnz);
+      for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
+      std::vector<uint32_t> qoff, qent;
+      bool ok = false;
+      build_schedule(dim, 2, off, src, sg, qoff, qent, &ok, 2);
+      if (ok) {
+        std::vector<uint32_t> woff(nsl + 1, 0), wn, wf;
+        for (int64_t sl = 0; sl < nsl; ++sl) {
+          const uint32_t width = (qoff[sl + 1] - qoff[sl]) / 32;  // even
+          woff[sl + 1] = woff[sl] + 32 * (width / 2);
+          for (uint32_t p = 0; p < width / 2; ++p)
+            for (int l = 0; l < 32; ++l) {
+              uint32_t en[2], ef[2];
+              for (int h = 0; h < 2; ++h) {
+                const uint32_t e = qent[qoff[sl] + (2 * p + h) * 32 + l];
+                const uint32_t sidx = e & 0x7fffffffu, neg = e >> 31;
+                en[h] = sidx + (neg ? negoff : 0u);
+                ef[h] = sidx | (neg << 15);
+              }
+              wn.push_back(en[0] | (en[1] << 16));
+              wf.push_back(ef[0] | (ef[1] << 16));
+            }
+        }
+        wn.resize(wn.size() + 128, 0u);  // the up pass loads whole batches of 4 words past a slice's end
+        wf.resize(wf.size() + 128, 0u);
+        EDG_CHECK(B.p16_off.alloc(woff.size(), st, "packed schedule"));
+        EDG_CHECK(B.p16_ent.alloc(wn.size(), st, "packed schedule"));
+        EDG_CHECK(B.p16f_ent.alloc(wf.size(), st, "packed schedule"));
+        EDG_CUDA(cudaMemcpyAsync(B.p16_off.p, woff.data(), woff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        EDG_CUDA(cudaMemcpyAsync(B.p16_ent.p, wn.data(), wn.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        EDG_CUDA(cudaMemcpyAsync(B.p16f_ent.p, wf.data(), wf.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        EDG_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
+        B.p16_negoff = negoff;
+      }
+    }
+  }
+  if (uniform && B.nnz > 0) {
+    std::vector<uint32_t> sg(B.nnz);
+    for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
+    EDG_CHECK(build_kron(s, B, off, src, sg));
+  }
+  B.variants = true;
+  return EDG_OK;
+}
+
 // SELL-32 copy of a gather table, built on the host from the device CSR (the tables are
 // O(DimUp) -- about 1 MB for a 4x4 lattice -- so this is a one-off of milliseconds).
 int build_sell(edg_sector_s* s, SpinBasis& B) {
@@ -830,43 +941,6 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
       B.group_max = std::max<int>(B.group_max, int(members[g].size()));
     }
     B.groups = int(G);
-    // contiguous blocks balanced by hops for the block-staged down pass, in two shapes: about
-    // one block per SM (1024-thread CTAs) and two per SM (512-thread CTAs); each a multiple
-    // of the SM count, enough blocks that one block's rows of a 256-column FP32 slab (1 KB per
-    // row) stay within 112 KB per SM
-    for (int shape = 0; shape < 2; ++shape) {
-      const int per_sm = shape + 1;
-      int64_t tot = 0;
-      for (int64_t r = 0; r < dim; ++r) tot += 1 + int64_t(off[r + 1] - off[r]);
-      int64_t CG = std::max<int64_t>(1, std::min<int64_t>(int64_t(sms) * per_sm, dim));
-      std::vector<uint32_t> coff;
-      int mx = 0;
-      for (int iter = 0; iter < 16; ++iter) {
-        coff.assign(1, 0u);
-        int64_t acc = 0, g = 1;
-        mx = 0;
-        uint32_t start = 0;
-        for (int64_t r = 0; r < dim; ++r) {
-          acc += 1 + int64_t(off[r + 1] - off[r]);
-          if (g < CG && acc * CG >= g * tot) {  // close block g-1 after row r
-            coff.push_back(uint32_t(r + 1));
-            mx = std::max<int>(mx, int(r + 1 - start));
-            start = uint32_t(r + 1);
-            ++g;
-          }
-        }
-        coff.push_back(uint32_t(dim));
-        mx = std::max<int>(mx, int(dim - start));
-        if (mx <= 112 / per_sm || CG >= dim) break;
-        CG = std::min<int64_t>(dim, CG + sms);
-      }
-      SpinBasis::RowBlocks& rb = B.rowblk[shape];
-      rb.max_rows = mx;
-      rb.count = int(coff.size() - 1);
-      EDG_CHECK(rb.off.alloc(coff.size(), st, "row blocks"));
-      EDG_CUDA(cudaMemcpyAsync(rb.off.p, coff.data(), coff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-      EDG_CUDA(cudaStreamSynchronize(st));
-    }
     EDG_CHECK(B.group_off.alloc(G + 1, st, "row groups"));
     EDG_CHECK(B.group_rows.alloc(grows.size() + 1, st, "row groups"));
     EDG_CUDA(cudaMemcpyAsync(B.group_off.p, goff.data(), goff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
@@ -921,55 +995,6 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
       EDG_CUDA(cudaMemcpyAsync(B.sched_ent.p, qent.data(), qent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
       B.sched_rt = rt32;
     }
-  }
-  // Packed 16-bit schedule for the two-row FP32 up pass (slot counts rounded to 2)
-  B.p16_negoff = 0;
-  B.p16_ent.reset();
-  B.p16_off.reset();
-  B.p16f_ent.reset();
-  {
-    const uint32_t negoff = uint32_t((dim + kUpZeroSlots + 31) / 32 * 32);
-    if (uniform && B.nnz > 0 && 2 * int64_t(negoff) <= 32768) {
-      std::vector<uint32_t> sg(B.nnz);
-      for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
-      std::vector<uint32_t> qoff, qent;
-      bool ok = false;
-      build_schedule(dim, 2, off, src, sg, qoff, qent, &ok, 2);
-      if (ok) {
-        std::vector<uint32_t> woff(nsl + 1, 0), wn, wf;
-        for (int64_t sl = 0; sl < nsl; ++sl) {
-          const uint32_t width = (qoff[sl + 1] - qoff[sl]) / 32;  // even
-          woff[sl + 1] = woff[sl] + 32 * (width / 2);
-          for (uint32_t p = 0; p < width / 2; ++p)
-            for (int l = 0; l < 32; ++l) {
-              uint32_t en[2], ef[2];
-              for (int h = 0; h < 2; ++h) {
-                const uint32_t e = qent[qoff[sl] + (2 * p + h) * 32 + l];
-                const uint32_t sidx = e & 0x7fffffffu, neg = e >> 31;
-                en[h] = sidx + (neg ? negoff : 0u);
-                ef[h] = sidx | (neg << 15);
-              }
-              wn.push_back(en[0] | (en[1] << 16));
-              wf.push_back(ef[0] | (ef[1] << 16));
-            }
-        }
-        wn.resize(wn.size() + 128, 0u);  // the up pass loads whole batches of 4 words past a slice's end
-        wf.resize(wf.size() + 128, 0u);
-        EDG_CHECK(B.p16_off.alloc(woff.size(), st, "packed schedule"));
-        EDG_CHECK(B.p16_ent.alloc(wn.size(), st, "packed schedule"));
-        EDG_CHECK(B.p16f_ent.alloc(wf.size(), st, "packed schedule"));
-        EDG_CUDA(cudaMemcpyAsync(B.p16_off.p, woff.data(), woff.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        EDG_CUDA(cudaMemcpyAsync(B.p16_ent.p, wn.data(), wn.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        EDG_CUDA(cudaMemcpyAsync(B.p16f_ent.p, wf.data(), wf.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        EDG_CUDA(cudaStreamSynchronize(st));  // host vectors go out of scope
-        B.p16_negoff = negoff;
-      }
-    }
-  }
-  if (uniform && B.nnz > 0) {
-    std::vector<uint32_t> sg(B.nnz);
-    for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
-    EDG_CHECK(build_kron(s, B, off, src, sg));
   }
   // column-split copy for rows that do not fit shared memory whole (FP64 rows above 227 KB)
   B.split_parts = 0;
@@ -1045,6 +1070,13 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
 }
 
 }  // namespace
+
+int sector_variant_tables(edg_sector_s* s) {
+  if (s->cplx || s->form != EDG_FORM_STORED) return EDG_OK;
+  EDG_CHECK(build_variants(s, s->up));
+  EDG_CHECK(build_variants(s, s->dw));
+  return EDG_OK;
+}
 
 int sector_build(edg_sector_s* s) {
   // exact binomial table C(n,k), n,k < kBinomN

@@ -332,6 +332,10 @@ int edg_sector_set_kernels(edg_sector* s, int precision, int candidate) {
   EDG_ARG(candidate >= 0 && candidate < 3 * nup, "edg_sector_set_kernels: candidate=%d outside 0..%d", candidate,
           3 * nup - 1);
   const int f32 = precision == EDG_PREC_F32;
+  if (candidate != 0) {
+    EDG_ON_DEVICE(s->device);
+    EDG_CHECK(sector_variant_tables(s));
+  }
   s->hxv_dw[f32] = candidate / nup;
   s->hxv_up[f32] = candidate % nup;
   return EDG_OK;

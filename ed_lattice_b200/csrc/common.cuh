@@ -204,6 +204,8 @@ struct SpinBasis {
   // consecutive blocks of that group: its LL offsets stay in registers for the whole launch,
   // its HH offsets are shared with the lanes on the same block, and only its cross hops read
   // a per-column table.
+  bool variants = false;          // the tables of the non-default kernels (rowblk, p16_*,
+                                  // kron_*) are built (sector_variant_tables)
   int kron_m = 0;                 // 0: no Kronecker schedule
   int kron_nthr = 0;              // threads with work (of kKronThreads)
   int kron_lmax = 0;              // most blocks owned by one thread
@@ -312,6 +314,8 @@ inline int up_rows_per_cta(int64_t dimup, size_t elem) {
 
 // ---- basis.cu
 int sector_build(edg_sector_s* s);
+// builds, once, the tables of the non-default H x v kernels of a real stored sector
+int sector_variant_tables(edg_sector_s* s);
 uint64_t binom_host(int n, int k);
 
 // ---- hxv.cu
@@ -434,5 +438,7 @@ int tridiag_lowest_host(int n, const double* d, const double* e, int k, double* 
 // k lowest eigenpairs (vectors z[k][n]) by bisection + twisted factorisation; EDG_ERR_NOCONV
 // when two of the k+1 lowest eigenvalues are closer than relgap * spectral radius
 int tridiag_lowest_vectors(int n, const double* d, const double* e, int k, double relgap, double* w, double* z);
+// dense symmetric n x n (column-major A): eigenvalues w ascending, eigenvectors Z column-major
+int sym_eigh_host(int n, const double* A, double* w, double* Z);
 
 }  // namespace edg

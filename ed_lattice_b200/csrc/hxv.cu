@@ -1633,6 +1633,7 @@ int hxv_autotune(edg_sector_s* s, int reps, double* ms, int* nc, int* best) {
   const int nup = sizeof(T) == 4 ? 4 : 1;
   const int ncand = 3 * nup;
   cudaStream_t st = s->stream;
+  EDG_CHECK(sector_variant_tables(s));
   DevBuf<T> x, y;
   EDG_CHECK(x.alloc(size_t(s->vlen), st, "autotune vectors"));
   EDG_CHECK(y.alloc(size_t(s->vlen), st, "autotune vectors"));

@@ -107,6 +107,15 @@ __global__ void k_gram_step(double* __restrict__ coef, int m, double* __restrict
   if (blockIdx.x == 0 && threadIdx.x == 0) *a_out = c[j];
 }
 
+// Gm[i][j] = (i == j) for i, j < r (leading dimension ld): the Gram matrix of a freshly
+// restarted basis (Ritz vectors and the residual direction, orthonormal to rounding)
+__global__ void k_gram_eye(double* __restrict__ Gm, int ld, int r) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < r * r; t += gridDim.x * blockDim.x) {
+    const int i = t / r, j = t - i * r;
+    Gm[int64_t(i) * ld + j] = i == j ? 1.0 : 0.0;
+  }
+}
+
 constexpr int kDotBlocks = 148 * 7;  // blocks per multi-dot launch, over all column groups
 
 // Launch shape of k_multidot for m columns of n elements: column group width, blocks per
@@ -489,6 +498,181 @@ struct LkRun {
     return EDG_OK;
   }
 
+  // Thick-restarted Lanczos (Wu & Simon, SIAM J. Matrix Anal. Appl. 22 (2000) 602; the
+  // exact-shift form of the implicit restart of ARPACK, which the reference's sp_eigh calls
+  // with Ncv basis vectors): real sectors. The basis holds at most ncv columns; every step
+  // is reorthogonalised against all of them as in run(), and the Gram-Schmidt coefficients
+  // y = Q^T H q_j are kept, column by column, as the projected matrix Hm = Q^T H Q. When the
+  // basis is full, its p lowest Ritz vectors Q z_i replace it, the residual direction w / b
+  // follows them, and Hm restarts as diag(theta_i) (the coupling of the residual direction
+  // to the Ritz vectors, b z_{m,i}, comes back as the Gram-Schmidt coefficients of the next
+  // step). The reorthogonalisation reads at most ncv columns per step instead of the whole
+  // Krylov basis. Converged when the k lowest Ritz pairs satisfy b |z_{m,i}| <= tol
+  // max(1, |theta_i|), as in run().
+  std::vector<double> thf, zf;  // final Ritz values and the coefficients of the k lowest
+  int steps = 0;
+  int run_tr(edg_sector_s* s, int k, const double* start, int maxit, int ncv, int p, double tol) {
+    const int64_t n = s->vlen;
+    const int64_t ne = s->dim;
+    cudaStream_t st = s->stream;
+    if (ncv > ne) ncv = int(ne);
+    if (p > ncv - 1) p = ncv - 1;
+    EDG_CHECK(Q.alloc(size_t(ncv) * n, st, "Lanczos basis (lowest-k, restarted)"));
+    EDG_CHECK(w.alloc(n, st, "Lanczos vector"));
+    size_t npart = 1;
+    for (int mm = 1; mm <= ncv; ++mm) npart = std::max(npart, size_t(2) * mm * dot_shape(mm, n).nsplit());
+    EDG_CHECK(part.alloc(npart, st, "multi-dot partials"));
+    EDG_CHECK(nred.alloc(kRedSlots, st, "norm reduction scratch"));
+    EDG_CHECK(red_scratch_reset(st, nred.p));
+    EDG_CHECK(coef.alloc(3 * size_t(ncv) + 8, st, "multi-dot coefficients"));
+    EDG_CHECK(Gm.alloc(size_t(ncv) * ncv, st, "Gram matrix"));
+    EDG_CHECK(dab.alloc(2 * size_t(ncv) + 4, st, "Lanczos scalars"));
+    DevBuf<double> Yc, Xr, Zd;
+    EDG_CHECK(Yc.alloc(size_t(ncv) * ncv, st, "projected matrix"));
+    double* dA = dab.p;           // a_j of the current cycle (scratch)
+    double* dB = dab.p + ncv + 1;  // b at column position t: dB[t]
+    EDG_CHECK(norm_vec<double>(st, start, n, nred.p, dB));
+    double nrm = 0.0;
+    EDG_CUDA(cudaMemcpyAsync(&nrm, dB, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EDG_CUDA(cudaStreamSynchronize(st));
+    if (!(nrm > 0.0)) {
+      set_error("edg_lowest_k: start vector has zero norm");
+      return EDG_ERR_ARG;
+    }
+    EDG_CHECK((convert_dev<T, double>(st, Q.p, start, n, 1.0 / nrm)));
+    std::vector<double> hY(size_t(ncv) * ncv), hb(size_t(ncv) + 2), Hm, th(ncv), Zm;
+    std::vector<double> lock;  // Ritz values of the kept block
+    int mcur = 1, next_check = k;
+    steps = 0;
+    for (;;) {
+      const int j = mcur - 1;
+      T* qj = Q.p + size_t(j) * n;
+      EDG_CHECK(hxv_apply<T>(s, qj, w.p));
+      int nsplit = 0;
+      EDG_CHECK(launch_multidot2<T>(Q.p, mcur, n, w.p, qj, part.p, st, &nsplit));
+      k_multifinish<<<(2 * mcur + 7) / 8, 256, 0, st>>>(part.p, nsplit, 2 * mcur, coef.p);
+      k_gram_step<<<(mcur + 7) / 8, 256, 0, st>>>(coef.p, mcur, Gm.p, ncv, dA + j);
+      k_multiaxpy<T><<<grid_n(n), kLkThreads, 0, st>>>(Q.p, coef.p + 2 * mcur, mcur, n, w.p);
+      EDG_CUDA(cudaGetLastError());
+      EDG_CUDA(cudaMemcpyAsync(Yc.p + size_t(j) * ncv, coef.p + 2 * mcur, size_t(mcur) * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st));
+      EDG_CHECK(norm_vec<T>(st, w.p, n, nred.p, dB + mcur));
+      ++steps;
+      const bool full = mcur == ncv;
+      const bool last = steps >= maxit || (mcur == ne && lock.empty());
+      if ((mcur >= k && steps >= next_check) || full || last) {
+        const int pl = int(lock.size());
+        EDG_CUDA(cudaMemcpyAsync(hY.data(), Yc.p, size_t(mcur) * ncv * sizeof(double), cudaMemcpyDeviceToHost, st));
+        EDG_CUDA(cudaMemcpyAsync(hb.data(), dB, size_t(mcur + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        EDG_CUDA(cudaStreamSynchronize(st));
+        // an invariant subspace reached at column position t (b_t ~ 0, or NaN) ends the run
+        int mm = mcur;
+        bool brk = false;
+        for (int t = pl + 1; t <= mcur; ++t)
+          if (!(hb[t] >= 1e-12)) {
+            mm = t;
+            brk = true;
+            break;
+          }
+        Hm.assign(size_t(mm) * mm, 0.0);
+        for (int i = 0; i < pl && i < mm; ++i) Hm[i + size_t(i) * mm] = lock[i];
+        for (int c = pl; c < mm; ++c)
+          for (int i = 0; i <= c; ++i) Hm[i + size_t(c) * mm] = Hm[c + size_t(i) * mm] = hY[size_t(c) * ncv + i];
+        const double b = brk ? 0.0 : hb[mcur];
+        const int kk = std::min(k, mm);
+        auto check = [&](const double* theta, const double* zend, double* worst) {
+          bool ok = mm >= k || brk;
+          *worst = 0.0;
+          for (int i = 0; i < kk; ++i) {
+            const double r = b * std::fabs(zend[i]);
+            const double lim = tol * std::max(1.0, std::fabs(theta[i]));
+            if (r > lim) ok = false;
+            *worst = std::max(*worst, r / lim);
+          }
+          return ok;
+        };
+        double worst = 0.0;
+        bool conv = false, dense = full || last || brk || pl > 0;
+        if (!dense) {
+          // before the first restart Hm is the Lanczos tridiagonal: the O(k m) test between
+          // steps, the dense eigenproblem only to confirm
+          std::vector<double> d(mm), e(mm, 0.0), zl(kk);
+          for (int c = 0; c < mm; ++c) d[c] = hY[size_t(c) * ncv + c];
+          for (int c = 1; c < mm; ++c) e[c] = hY[size_t(c) * ncv + c - 1];
+          if (tridiag_lowest_host(mm, d.data(), e.data(), kk, th.data(), zl.data()) == EDG_OK)
+            conv = check(th.data(), zl.data(), &worst);
+          else
+            conv = true;  // let the dense eigenproblem decide
+          dense = conv;
+        }
+        if (dense) {
+          Zm.assign(size_t(mm) * mm, 0.0);
+          EDG_CHECK(sym_eigh_host(mm, Hm.data(), th.data(), Zm.data()));
+          std::vector<double> zl(kk);
+          for (int i = 0; i < kk; ++i) zl[i] = Zm[size_t(mm) - 1 + size_t(i) * mm];
+          conv = check(th.data(), zl.data(), &worst);
+        }
+        if (conv || brk || last) {
+          m = mm;
+          blast = b;
+          thf.assign(th.begin(), th.begin() + kk);
+          zf.assign(Zm.begin(), Zm.begin() + size_t(mm) * kk);
+          zlast.resize(kk);
+          for (int i = 0; i < kk; ++i) zlast[i] = Zm[size_t(mm) - 1 + size_t(i) * mm];
+          return EDG_OK;
+        }
+        int gap = std::max(1, mcur / 32);
+        if (worst > 1e6) gap = std::max(gap, 8);
+        else if (worst > 1e3) gap = std::max(gap, 3);
+        next_check = steps + gap;
+        if (full) {
+          // restart: X = Q Z[:, 0:pp] in FP64, then the first pp columns := X, column pp :=
+          // w / b, Gm := I on the leading pp + 1 columns, Hm := diag(theta) on them
+          const int pp = std::min(p, mm - 1);
+          EDG_CHECK(Xr.alloc(size_t(pp) * n, st, "thick-restart Ritz vectors"));
+          EDG_CHECK(Zd.alloc(size_t(mm) * pp, st, "thick-restart coefficients"));
+          EDG_CUDA(cudaMemcpyAsync(Zd.p, Zm.data(), size_t(mm) * pp * sizeof(double), cudaMemcpyHostToDevice, st));
+          for (int r0 = 0; r0 < pp; r0 += kMaxK) {
+            const int nr = std::min(kMaxK, pp - r0);
+            k_ritz_k<T><<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p + size_t(r0) * mm, mm, nr, n,
+                                                          Xr.p + size_t(r0) * n);
+          }
+          EDG_CUDA(cudaGetLastError());
+          for (int r = 0; r < pp; ++r)
+            EDG_CHECK((convert_dev<T, double>(st, Q.p + size_t(r) * n, Xr.p + size_t(r) * n, n, 1.0)));
+          EDG_CHECK(scale_into<T>(st, Q.p + size_t(pp) * n, w.p, dB + mcur, n));
+          k_gram_eye<<<((pp + 1) * (pp + 1) + 255) / 256, 256, 0, st>>>(Gm.p, ncv, pp + 1);
+          EDG_CUDA(cudaGetLastError());
+          EDG_CUDA(cudaStreamSynchronize(st));  // Zm (host) is read by the copy above
+          lock.assign(th.begin(), th.begin() + pp);
+          mcur = pp + 1;
+          continue;
+        }
+      }
+      EDG_CHECK(scale_into<T>(st, Q.p + size_t(mcur) * n, w.p, dB + mcur, n));
+      ++mcur;
+    }
+  }
+  // Ritz pairs of a run_tr() run: the kk lowest values, residual estimates b |z_m,i| and
+  // (X != null) the vectors X[r] = sum_j Z[j][r] q_j in FP64 on the device
+  int ritz_tr(edg_sector_s* s, int kk, double* evals, double* resid, double* X) {
+    cudaStream_t st = s->stream;
+    const int64_t n = s->vlen;
+    for (int i = 0; i < kk; ++i) {
+      evals[i] = thf[i];
+      if (resid) resid[i] = blast * std::fabs(zlast[i]);
+    }
+    if (X) {
+      DevBuf<double> Zd;
+      EDG_CHECK(Zd.alloc(size_t(m) * kk, st, "Ritz coefficients"));
+      EDG_CUDA(cudaMemcpyAsync(Zd.p, zf.data(), size_t(m) * kk * sizeof(double), cudaMemcpyHostToDevice, st));
+      k_ritz_k<T><<<grid_n(n), kLkThreads, 0, st>>>(Q.p, Zd.p, m, kk, n, X);
+      EDG_CUDA(cudaGetLastError());
+      EDG_CUDA(cudaStreamSynchronize(st));
+    }
+    return EDG_OK;
+  }
+
   // the kk lowest Ritz values, their residual estimates, and (X != null) the Ritz vectors
   // X[r] = sum_j Z[j][r] q_j in FP64 on the device
   int ritz(edg_sector_s* s, int kk, double* evals, double* resid, double* X) {
@@ -554,31 +738,52 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
     EDG_CHECK(random_dev(st, x0.p, n, seed));
   }
   int steps32 = 0;
-  if (mode == EDG_LK_F32_REFINE && !s->cplx) {
-    // FP32-bulk phase to residuals kTol32, then its k Ritz vectors, summed, start the FP64 run:
-    // the FP64 Krylov space then holds the wanted eigenvectors to FP32 accuracy from its first
-    // k vectors and refines them in few steps
-    const int kk = k;
+  if (!s->cplx) {
+    // Real sectors: thick-restarted runs with the reference's basis size, Ncv = 10 k
+    // (lanc_ncv_factor * Neigen, src/DIAG/DIAG.f90:144-146), at least 2k + 16; a restart keeps
+    // the k + (ncv - k)/4 lowest Ritz vectors. Sectors of at most 4 Ncv states keep their
+    // whole Krylov basis (no restart). The H x v applications are bounded by maxit, and by
+    // no fewer than 8 Ncv (a restarted run may need more steps than the dimension).
+    int ncv = int(std::min<int64_t>(ne, std::max(10 * k, 2 * k + 16)));
+    if (ne <= 4 * int64_t(ncv)) ncv = int(ne);
+    const int steps_max = std::max({maxit, k, 8 * ncv});
+    if (mode == EDG_LK_F32_REFINE) {
+      // FP32-bulk phase to residuals kTol32; its k Ritz vectors, summed, start the FP64 run
+      DevBuf<double> X;
+      EDG_CHECK(X.alloc(size_t(k) * n, st, "FP32 Ritz vectors"));
+      {
+        int nc = ncv;
+        EDG_CHECK(basis_room(n, sizeof(float), k, &nc));
+        LkRun<float> r32;
+        EDG_CHECK(r32.run_tr(s, k, x0.p, steps_max, nc, k + (nc - k) / 4, std::max(tol, kTol32)));
+        steps32 = r32.steps;
+        const int k32 = int(r32.thf.size());
+        std::vector<double> ev(k32), rs(k32);
+        EDG_CHECK(r32.ritz_tr(s, k32, ev.data(), rs.data(), X.p));
+        EDG_CUDA(cudaMemsetAsync(x0.p, 0, n * sizeof(double), st));
+        for (int r = 0; r < k32; ++r) EDG_CHECK(axpy_accum_dev<double>(st, x0.p, X.p + size_t(r) * n, 1.0, n));
+      }  // the FP32 basis goes back to the pool before the FP64 one is taken
+    }
+    EDG_CHECK(basis_room(n, sizeof(double), k, &ncv));
+    LkRun<double> r64;
+    EDG_CHECK(r64.run_tr(s, k, x0.p, steps_max, ncv, k + (ncv - k) / 4, tol));
+    if (niter) *niter = steps32 + r64.steps;
+    const int kk = int(r64.thf.size());
     DevBuf<double> X;
-    EDG_CHECK(X.alloc(size_t(kk) * n, st, "FP32 Ritz vectors"));
-    {
-      int mmax = mmax0;
-      EDG_CHECK(basis_room(n, sizeof(float), k, &mmax));
-      LkRun<float> r32;
-      EDG_CHECK(r32.run(s, k, x0.p, mmax, std::max(tol, kTol32)));
-      steps32 = r32.m;
-      std::vector<double> ev(kk), rs(kk);
-      const int k32 = std::min(kk, r32.m);
-      EDG_CHECK(r32.ritz(s, k32, ev.data(), rs.data(), X.p));
-      EDG_CUDA(cudaMemsetAsync(x0.p, 0, n * sizeof(double), st));
-      for (int r = 0; r < k32; ++r) EDG_CHECK(axpy_accum_dev<double>(st, x0.p, X.p + size_t(r) * n, 1.0, n));
-    }  // the FP32 basis goes back to the pool before the FP64 one is taken
+    if (evecs_host) EDG_CHECK(X.alloc(size_t(kk) * n, st, "Ritz vectors"));
+    EDG_CHECK(r64.ritz_tr(s, kk, evals, resid, evecs_host ? X.p : nullptr));
+    if (evecs_host) {
+      EDG_CUDA(cudaMemcpyAsync(evecs_host, X.p, size_t(kk) * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+      EDG_CUDA(cudaStreamSynchronize(st));
+    }
+    return EDG_OK;
   }
+  // complex sectors: one unrestarted run with the whole Krylov basis (Gram-Schmidt applied twice)
   int mmax = mmax0;
   EDG_CHECK(basis_room(n, sizeof(double), k, &mmax));
   LkRun<double> r64;
   EDG_CHECK(r64.run(s, k, x0.p, mmax, tol));
-  if (niter) *niter = steps32 + r64.m;
+  if (niter) *niter = r64.m;
   const int kk = std::min(k, r64.m);
   DevBuf<double> X;
   if (evecs_host) EDG_CHECK(X.alloc(size_t(kk) * n, st, "Ritz vectors"));

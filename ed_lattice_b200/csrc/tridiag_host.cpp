@@ -268,4 +268,59 @@ int tridiag_lowest_vectors(int n, const double* d, const double* e, int k, doubl
   return EDG_OK;
 }
 
+// Dense symmetric eigenproblem of a small matrix (the projected matrix of a thick-restarted
+// Lanczos run, n up to a few dozen): Householder reduction to tridiagonal form T = P^T A P
+// (reflectors H = I - beta v v^T applied from both sides, P accumulated), the implicit QL
+// above on T, then the eigenvectors P Z_T. A: column-major n x n (only symmetric use); w[n]
+// ascending; Z column-major n x n.
+int sym_eigh_host(int n, const double* A, double* w, double* Z) {
+  if (n <= 0) return EDG_OK;
+  std::vector<double> a(A, A + size_t(n) * n), P(size_t(n) * n, 0.0), v(n), pv(n), qv(n);
+  for (int i = 0; i < n; ++i) P[i + size_t(i) * n] = 1.0;
+  auto at = [&](int i, int j) -> double& { return a[i + size_t(j) * n]; };
+  for (int kcol = 0; kcol + 2 < n; ++kcol) {
+    // reflector that zeroes a[kcol+2..n-1][kcol]
+    double sig = 0.0;
+    for (int i = kcol + 1; i < n; ++i) sig += at(i, kcol) * at(i, kcol);
+    const double x0 = at(kcol + 1, kcol);
+    const double alpha = -std::copysign(std::sqrt(sig), x0);
+    if (sig == 0.0 || sig - x0 * x0 == 0.0) continue;  // column already reduced
+    std::fill(v.begin(), v.end(), 0.0);
+    for (int i = kcol + 1; i < n; ++i) v[i] = at(i, kcol);
+    v[kcol + 1] -= alpha;
+    double vv = 0.0;
+    for (int i = kcol + 1; i < n; ++i) vv += v[i] * v[i];
+    const double beta = 2.0 / vv;
+    // A <- H A H with p = beta A v, q = p - (beta/2)(v^T p) v: A <- A - v q^T - q v^T
+    for (int i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int j = kcol + 1; j < n; ++j) t += at(i, j) * v[j];
+      pv[i] = beta * t;
+    }
+    double vp = 0.0;
+    for (int i = kcol + 1; i < n; ++i) vp += v[i] * pv[i];
+    for (int i = 0; i < n; ++i) qv[i] = pv[i] - 0.5 * beta * vp * v[i];
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) at(i, j) -= v[i] * qv[j] + qv[i] * v[j];
+    // P <- P H
+    for (int i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int j = kcol + 1; j < n; ++j) t += P[i + size_t(j) * n] * v[j];
+      t *= beta;
+      for (int j = kcol + 1; j < n; ++j) P[i + size_t(j) * n] -= t * v[j];
+    }
+  }
+  std::vector<double> d(n), e(n, 0.0), zt(size_t(n) * n);
+  for (int i = 0; i < n; ++i) d[i] = at(i, i);
+  for (int i = 1; i < n; ++i) e[i] = 0.5 * (at(i, i - 1) + at(i - 1, i));
+  EDG_CHECK(tridiag_eigh_host(n, d.data(), e.data(), w, nullptr, zt.data()));
+  for (int c = 0; c < n; ++c)
+    for (int i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int j = 0; j < n; ++j) t += P[i + size_t(j) * n] * zt[j + size_t(c) * n];
+      Z[i + size_t(c) * n] = t;
+    }
+  return EDG_OK;
+}
+
 }  // namespace edg

@@ -199,7 +199,7 @@ class DiagParams:
     lanc_nstates_total: int = 1      # set by setup()
     ed_twin: bool = False            # ED_TWIN: solve Nup >= Ndw only, twins by spin flip
     lanc_fp32_bulk: bool = False     # lowest-k sectors: FP32 bulk + FP64 refinement (no reference key)
-    sector_threads: int = 4          # sectors solved at once on one device (no reference key)
+    sector_threads: int = 8          # sectors solved at once on one device (no reference key)
 
     def setup(self, nsectors: int) -> "DiagParams":
         """State counts of the Lanczos method (src/SETUP.f90:89-104): at finite T an even

@@ -244,7 +244,8 @@ class Sector:
                  tol: float = 1e-10, want_vectors: bool = True, mode: int = L.EDG_LK_F64):
         """Lowest k eigenpairs (the sp_eigh branch of ed_diag_d, src/DIAG/DIAG.f90:191-202),
         FP64 (mode EDG_LK_F64) or FP32 bulk + FP64 refinement (EDG_LK_F32_REFINE).
-        Returns (evals[k'], evecs[k', dim] or None, resid[k'], basis size), k' = min(k, dim)."""
+        Real sectors run thick-restarted with the reference's Ncv = 10 k basis vectors.
+        Returns (evals[k'], evecs[k', dim] or None, resid[k'], H x v applications), k' = min(k, dim)."""
         kk = min(k, self.dim)
         ev = np.zeros(k)
         rs = np.zeros(k)

@@ -136,7 +136,9 @@ int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv);
  * Untuned sectors use candidate 0. No counterpart in the reference. */
 int edg_sector_autotune(edg_sector* s, int precision, int reps, double* ms, int* ncand, int* best);
 /* Pin the H x v kernel pair of this sector for one precision to candidate k of
- * edg_sector_autotune's list (0..11 for FP32, 0..2 for FP64). No counterpart in the reference. */
+ * edg_sector_autotune's list (0..11 for FP32, 0..2 for FP64). The tables of the non-default
+ * kernels are built on the first call that needs them (this one, or edg_sector_autotune);
+ * sectors that keep candidate 0 never build them. No counterpart in the reference. */
 int edg_sector_set_kernels(edg_sector* s, int precision, int candidate);
 /* Device-resident forms (vectors in HBM, reference layout); stream-ordered, no sync. */
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv);
@@ -189,23 +191,28 @@ int edg_ground_state_stats(const edg_sector* s, int* n_f32, int* n_f64);
 /* Lowest k (1..16) eigenpairs of a sector: the sp_eigh (ARPACK) branch of ed_diag_d,
  * Neigen = min(dim, lanc_nstates_sector) states per sector for the finite-temperature state
  * list (src/DIAG/DIAG.f90:144-146,191-202). FP64 Lanczos with full reorthogonalisation
- * (classical Gram-Schmidt with its second pass from the Gram matrix of the basis; applied
- * twice for complex vectors) against a basis of at most min(maxit, 1024) device
- * vectors (fewer if HBM is short); stops when every one of the k lowest Ritz pairs has
- * residual b_{m+1}|z_{m,i}| <= tol*max(1,|theta_i|), or the Krylov space becomes invariant,
- * or the basis is full. evals[k] ascending (NaN beyond dim); evecs (host, may be NULL):
- * k normalised vectors, vector r at evecs + r*dim; resid (may be NULL): the k residual
- * estimates at exit (the caller checks them against tol); *niter = basis size. v0 and
- * seed as in edg_ground_state. One vector per eigenspace: exactly degenerate levels
- * inside a sector appear once (use edg_sector_dense for small sectors with symmetries). */
+ * (classical Gram-Schmidt with its second pass from the Gram matrix of the basis). Real
+ * sectors: thick-restarted, the exact-shift form of ARPACK's implicit restart, with the
+ * reference's basis size Ncv = 10 k (at least 2k + 16; fewer if HBM is short): when the
+ * basis is full its k + (Ncv - k)/4 lowest Ritz vectors and the residual direction start the
+ * next cycle (sectors of at most 4 Ncv states keep their whole basis), and max(maxit, 8 Ncv)
+ * bounds the H x v applications. Complex sectors: one unrestarted run
+ * (Gram-Schmidt applied twice) with a basis of at most min(maxit, 1024) vectors. Stops when
+ * every one of the k lowest Ritz pairs has residual b |z_{m,i}| <= tol*max(1,|theta_i|), or
+ * the Krylov space becomes invariant, or maxit is reached. evals[k] ascending (NaN beyond
+ * dim); evecs (host, may be NULL): k normalised vectors, vector r at evecs + r*dim; resid
+ * (may be NULL): the k residual estimates at exit (the caller checks them against tol);
+ * *niter = H x v applications. v0 and seed as in edg_ground_state. One vector per
+ * eigenspace: exactly degenerate levels inside a sector appear once (use
+ * edg_sector_dense for small sectors with symmetries). */
 int edg_lowest_k(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol,
                  double* evals, double* evecs, double* resid, int* niter);
 /* Lowest-k modes: FP64 throughout (edg_lowest_k), or FP32 bulk + FP64 refinement: the same
  * solver with FP32 basis and H x v (FP64 scalars and sums) to Ritz residuals of 1e-6, whose k
  * Ritz vectors, summed, start the FP64 solve to tol. Real Hij only (complex sectors run FP64). */
 enum { EDG_LK_F64 = 0, EDG_LK_F32_REFINE = 1 };
-/* edg_lowest_k with a mode; *niter counts the basis vectors of both phases. The outputs are
- * those of the FP64 phase (evals, vectors and residuals to tol). */
+/* edg_lowest_k with a mode; *niter counts the H x v applications of both phases. The outputs
+ * are those of the FP64 phase (evals, vectors and residuals to tol). */
 int edg_lowest_k_mode(edg_sector* s, int k, const double* v0, uint64_t seed, int maxit, double tol,
                       int mode, double* evals, double* evecs, double* resid, int* niter);
 /* Dense sector Hamiltonian, column-major dim x dim (the matrix ed_buildh(Hmat) assembles for
