@@ -306,14 +306,15 @@ def lowest_k_3x4(E):
     return out
 
 
-def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150, widths=(1, 4, 8, 16)):
+def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150, widths=(1, 8, 16, 32)):
     """Green's function chains on the 4x4 lattice at U=4 (t=1, XMU=2): ground state of the
     half-filled sector (8,8) (FP32+refine, vector kept on the device), then c^+_{i,up} into
     (9,8) and c_{i,up} into (7,8) (D = 147,232,800 each) for the 16 sites: 32 chains of 150
     steps with FP32 vectors, G_ii(iw_n) on 4096 Matsubara frequencies at beta=50 and on the
     real axis (eta=0.05). The 16 chains of each sector run as blocks of width w (block H x V,
-    edg_gf_chain_block; w = 1 is one chain after another through edg_gf_chain); all 32 chains
-    are 2 sectors x 16. Also the first `nchains_f64` chains with FP64 vectors for the ratio."""
+    edg_gf_chain_block; w = 1 is one chain after another through edg_gf_chain); w = 32 runs the
+    16-chain blocks of both target sectors at the same time (two host threads, one stream per
+    sector). Also the first `nchains_f64` chains with FP64 vectors for the ratio."""
     import torch
     model = E.Model(E.square_lattice(4, 4), uloc=4.0, xmu=2.0, hfmode=False)
     gs = E.Sector(model, 8, 8)
@@ -335,10 +336,17 @@ def gf_4x4_chains(E, L, nchains_f64=4, nlanc=150, widths=(1, 4, 8, 16)):
         for to, op in ((part, +1), (hole, -1)):
             if w == 1:
                 chans += [E.gf_chain(gs, to, op, int(i), 1, nlanc, e0.value, precision=E.EDG_PREC_F32) for i in sites]
-            else:
+            elif w < 32:
                 for c0 in range(0, 16, w):
                     chans += E.gf_chain_block(gs, to, op, sites[c0:c0 + w], 1, nlanc, e0.value,
                                               precision=E.EDG_PREC_F32)
+        if w == 32:  # all 32 chains in flight: the 16-chain blocks of both target sectors at once,
+            # one host thread each, every sector on its own stream
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(max_workers=2) as ex:
+                futs = [ex.submit(E.gf_chain_block, gs, to, op, sites, 1, nlanc, e0.value, precision=E.EDG_PREC_F32)
+                        for to, op in ((part, +1), (hole, -1))]
+                chans = futs[0].result() + futs[1].result()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         steps = sum(len(ch.poles) for ch in chans)

@@ -37,11 +37,17 @@ def assert_spectra_close(sp, p_ref, w_ref, n2_ref, temp=0.02, nmats=64):
     g = (sp.weight[None, :] / (1j * wm[:, None] - sp.poles[None, :])).sum(1)
     gr = (w_ref[None, :] / (1j * wm[:, None] - p_ref[None, :])).sum(1)
     assert np.abs(g - gr).max() <= 1e-8 * np.abs(gr).max()
-    # the lowest three poles carrying weight have converged after the chain lengths used here
+    # the lowest three poles carrying weight have converged after the chain lengths used here;
+    # a chain that loses orthogonality may add a copy of a converged pole next to it (within
+    # 1e-6), and how the weight splits between the copies depends on rounding: compare the
+    # summed weight of each cluster
     weighted = [(pr, wr) for pr, wr in sorted(zip(p_ref, w_ref)) if wr > 1e-3 * n2_ref][:3]
     for pr, wr in weighted:
         j = np.argmin(np.abs(sp.poles - pr))
-        assert abs(sp.poles[j] - pr) < 1e-6 and abs(sp.weight[j] - wr) < 1e-6 * max(1.0, n2_ref)
+        assert abs(sp.poles[j] - pr) < 1e-6
+        w_dev = sp.weight[np.abs(sp.poles - pr) < 1e-6].sum()
+        w_ref_c = w_ref[np.abs(p_ref - pr) < 1e-6].sum()
+        assert abs(w_dev - w_ref_c) < 1e-6 * max(1.0, n2_ref), (pr, w_dev, w_ref_c)
 
 
 # ----------------------------------------------------------------------------- basis / tables
