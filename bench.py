@@ -443,8 +443,14 @@ def run_ours(args):
     D = sector.dim
     stream = torch.cuda.current_stream()
     L.check(lib.edg_sector_set_stream(sector.handle, C.c_void_p(stream.cuda_stream)), "set_stream")
-    # the autotuner picks the H x v kernel pair of this sector for each precision (untimed)
-    tune = {"f32": sector.autotune(E.EDG_PREC_F32, reps=5), "f64": sector.autotune(E.EDG_PREC_F64, reps=3)}
+    # the autotuner picks the H x v kernel pair of this sector for each precision (untimed);
+    # --pin-kernels K pins FP32 candidate K and FP64 candidate 0 instead (a profiler distorts
+    # the autotuner's timings, so profiled runs pin the pair the plain run chose)
+    if args.pin_kernels is None:
+        tune = {"f32": sector.autotune(E.EDG_PREC_F32, reps=5), "f64": sector.autotune(E.EDG_PREC_F64, reps=3)}
+    else:
+        sector.set_kernels(args.pin_kernels, E.EDG_PREC_F32)
+        tune = {"pinned_f32_candidate": args.pin_kernels}
     g = torch.Generator(device="cuda")
     g.manual_seed(1234 + rank)
     v = torch.rand(D, device="cuda", dtype=torch.float32, generator=g) * 2 - 1
@@ -611,6 +617,8 @@ def main():
     ap.add_argument("--no-thermal", action="store_true")
     ap.add_argument("--no-gf", action="store_true")
     ap.add_argument("--no-lowk", action="store_true")
+    ap.add_argument("--pin-kernels", type=int, default=None,
+                    help="pin FP32 H x v candidate K (see edg_sector_autotune) instead of autotuning")
     ap.add_argument("--config5", action="store_true",
                     help="also run the 6x3 susceptibility sweep (36 chains of 200 steps on 2.36e9 states, minutes)")
     args = ap.parse_args()

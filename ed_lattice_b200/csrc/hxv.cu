@@ -165,14 +165,15 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 // ONE: one CTA per SM (the staged rows take more than half of shared memory); the 64
 // registers per thread this allows carry the next batch of entries while the current one is
 // applied.
-// The Lanczos-fused form (LZ) runs 768 threads per CTA: with two CTAs per SM that leaves 40
+// The Lanczos-fused form (LZ) with two CTAs per SM runs 768 threads per CTA: that leaves 40
 // registers per thread for the epilogue's FP64 state next to the batch of entries in flight
-// (at 1024 threads and 32 registers the batch no longer fit and the pass became latency-bound).
-template <bool LZ>
-constexpr int up_threads() { return LZ ? 768 : 1024; }
+// (at 1024 threads and 32 registers the batch no longer fit and the pass became latency-bound:
+// 2.56 against 1.34 ms on the 4x4 half-filled sector). One CTA per SM keeps 1024 threads.
+template <bool LZ, bool ONE>
+constexpr int up_threads() { return LZ && !ONE ? 768 : 1024; }
 
 template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE>
-__global__ void __launch_bounds__(up_threads<LZ>(), ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+__global__ void __launch_bounds__(up_threads<LZ, ONE>(), ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   if (!select_column(a)) return;
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
@@ -746,7 +747,12 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
                                                 const uint32_t* __restrict__ grows, int64_t nslab) {
   if (!select_column(a)) return;
   extern __shared__ __align__(16) unsigned char smem_dw[];
+  // the Lanczos scale 1/bn[j] (SCALED): folded into the hop values staged below, and read
+  // from shared memory where the diagonal is formed, so that it holds no registers in the
+  // slab loop (the FP64 form spilled with it)
+  __shared__ double s_sc;
   const double sc = SCALED ? 1.0 / a.bn[a.jstep] : 1.0;
+  if (SCALED && threadIdx.x == 0) s_sc = sc;
   __shared__ int s_ctr;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t gr0 = goff[blockIdx.x];
@@ -802,10 +808,11 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
           const uint32_t mdw = s_mdw[rr];
           T x[VEC];
           VecLd<T, VEC>::load(a.v + e0 + g * SEGW, x);
+          const double scl = SCALED ? *static_cast<volatile double*>(&s_sc) : 1.0;
 #pragma unroll
           for (int r = 0; r < VEC; ++r) {
             const T d = a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw));
-            acc[g][r] = (SCALED ? T(double(d) * sc) : d) * x[r];
+            acc[g][r] = (SCALED ? T(double(d) * scl) : d) * x[r];
           }
         } else {
 #pragma unroll
@@ -1280,7 +1287,7 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
   if (LZ && g > kRedBlocks) g = kRedBlocks;  // one partial per block in the reduction scratch
-  kern<<<dim3(int(g), a.ncols), up_threads<LZ>(), smem, st>>>(a, sl, nrb);
+  kern<<<dim3(int(g), a.ncols), per_sm == 2 ? up_threads<LZ, false>() : up_threads<LZ, true>(), smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   if (grid) *grid = int(g);
   return EDG_OK;
@@ -1312,9 +1319,11 @@ int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms)
     }
   }
   if (Bdw.max_row <= kDwHops && Bdw.groups > 0) {
-    // FP32: 4 float2 segments per lane (256 columns per slab); FP64: 2 double2 segments
+    // FP32: 4 float2 segments per lane (256 columns per slab); FP64: 2 double2 segments,
+    // 4 hops in flight (3 in the Lanczos-scaled form, which spilled at 4 within the 64
+    // registers of 4 CTAs per SM)
     constexpr int NSEG = sizeof(T) == 4 ? 4 : 2;
-    constexpr int KU = sizeof(T) == 4 ? 3 : 4;
+    constexpr int KU = sizeof(T) == 4 ? 3 : (SCALED ? 3 : 4);
     auto kern = v2 ? k_dw_grp<T, 2, NSEG, KU, FIRST, SCALED> : k_dw_grp<T, 1, NSEG, KU, FIRST, SCALED>;
     const size_t smem = size_t(Bdw.group_max) * (kDwHops * (sizeof(T) + 4) + sizeof(T) + 12) + 16;
     if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
