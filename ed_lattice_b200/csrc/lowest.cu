@@ -543,6 +543,8 @@ struct LkRun {
     std::vector<double> hY(size_t(ncv) * ncv), hb(size_t(ncv) + 2), Hm, th(ncv), Zm;
     std::vector<double> lock;  // Ritz values of the kept block
     int mcur = 1, next_check = k;
+    double prev_worst = 0.0;   // the last test's worst residual ratio, its step and restart
+    int prev_steps = 0, prev_lock = -1;
     steps = 0;
     for (;;) {
       const int j = mcur - 1;
@@ -621,9 +623,20 @@ struct LkRun {
           for (int i = 0; i < kk; ++i) zlast[i] = Zm[size_t(mm) - 1 + size_t(i) * mm];
           return EDG_OK;
         }
+        // next test: the residuals of Lanczos fall about geometrically, so two tests give the
+        // rate and the steps still needed; the next test comes at 3/4 of them (a test costs a
+        // host round trip, several steps' worth on a small sector)
         int gap = std::max(1, mcur / 32);
         if (worst > 1e6) gap = std::max(gap, 8);
         else if (worst > 1e3) gap = std::max(gap, 3);
+        if (prev_worst > 0.0 && worst < prev_worst && worst > 1.0 && steps > prev_steps && pl == prev_lock) {
+          const double rate = std::log(prev_worst / worst) / double(steps - prev_steps);  // per step
+          const double need = std::log(worst) / rate;
+          gap = std::max(gap, std::min(32, int(0.75 * need)));
+        }
+        prev_worst = worst;
+        prev_steps = steps;
+        prev_lock = pl;
         next_check = steps + gap;
         if (full) {
           // restart: X = Q Z[:, 0:pp] in FP64, then the first pp columns := X, column pp :=
