@@ -223,6 +223,7 @@ struct SpinBasis {
   DevBuf<uint32_t> kron_xwid;     // per warp and step (stride kron_lmax): slots
 };
 
+constexpr int64_t kFusedMaxDim = 500000;  // largest sector that defaults to the single-pass H x v
 constexpr int kKronThreads = 512;  // threads per CTA of the Kronecker up pass
 constexpr int kKronLL = 12;        // LL entries per low part held in registers
 // Shared memory of the Kronecker up pass: rt staged rows plus the zero slots, then the block
@@ -284,9 +285,10 @@ struct edg_sector_s {
   int last_n32 = 0, last_n64 = 0;  // H x v applications of the last ground-state run per precision
   // H x v kernel choice per vector precision ([0] FP64, [1] FP32), set by edg_sector_autotune:
   // down pass 0 = hop-balanced row groups, 1 = block-staged (one CTA per SM), 2 = block-staged
-  // (two CTAs per SM); up pass (FP32) 0 = 32-bit SELL schedule, 1 = packed 16-bit schedule
-  // with negated copies, 2 = packed 16-bit schedule with sign bits, 3 = Kronecker schedule.
-  // 0/0 until tuned.
+  // (two CTAs per SM), 3 = single pass (k_hxv_fused: the whole H x v, no up pass); up pass
+  // (FP32) 0 = 32-bit SELL schedule, 1 = packed 16-bit schedule with negated copies, 2 = packed
+  // 16-bit schedule with sign bits, 3 = Kronecker schedule. Until tuned: 3/0 for real stored
+  // sectors of at most kFusedMaxDim states, else 0/0.
   int hxv_dw[2] = {0, 0};
   int hxv_up[2] = {0, 0};
 };

@@ -733,6 +733,70 @@ __global__ void __launch_bounds__(256) k_dw_seg(HxvArgs<T> a, int64_t ntiles) {
   }
 }
 
+// Single-pass stored-form H x v for sectors whose vectors sit in L2 (D up to a few million):
+// one warp per 32 consecutive columns of one row idw. The down hops of the row are the same
+// for the 32 lanes (one broadcast entry each, a coalesced read of the source row's segment),
+// the up hops are each lane's own CSR list (gathers inside the row, from L1/L2). Terms in the
+// stored form's order, diag, DW, UP, sources ascending, so FP64 results equal the two-pass
+// kernels' and the reference's bit for bit on integer-valued models. LZ: the Lanczos-fused
+// step of k_up_smem (v = u / bn[j] through scaled matrix elements, w = Hv - c u_prev and the
+// block partials of <v, w>), in the same single pass.
+template <typename T, bool LZ>
+__global__ void __launch_bounds__(256) k_hxv_fused(HxvArgs<T> a, int64_t ntiles) {
+  if (!select_column(a)) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t wpb = blockDim.x >> 5;
+  const int64_t dimup = a.dimup;
+  const int64_t nct = (dimup + 31) >> 5;  // column tiles per row
+  double sc = 1.0, cc = 0.0, pa = 0.0;
+  if (LZ) {
+    sc = 1.0 / a.bn[a.jstep];
+    cc = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+  }
+  for (int64_t tile = blockIdx.x * wpb + (threadIdx.x >> 5); tile < a.dimdw * nct;
+       tile += int64_t(gridDim.x) * wpb) {
+    const int64_t idw = tile / nct;
+    const int64_t iup = (tile - idw * nct) * 32 + lane;
+    const bool act = iup < dimup;
+    const int64_t cup = act ? iup : dimup - 1;  // inactive lanes read a valid column, store nothing
+    const T* __restrict__ vrow = a.v + idw * dimup;
+    const T d = a.e_up[cup] + a.e_dw[idw] + a.U * T(__popc(a.map_up[cup] & a.map_dw[idw]));
+    T acc = (LZ ? T(double(d) * sc) : d) * vrow[cup];
+    const uint32_t k1 = a.off_dw[idw + 1];
+    for (uint32_t k = a.off_dw[idw]; k < k1; ++k) {
+      const T h = LZ ? T(double(a.val_dw[k]) * sc) : a.val_dw[k];
+      acc = fmaT<T>(h, a.v[int64_t(a.src_dw[k]) * dimup + cup], acc);
+    }
+    const uint32_t u1 = a.off_up[cup + 1];
+    for (uint32_t k = a.off_up[cup]; k < u1; ++k) {
+      const T h = LZ ? T(double(a.val_up[k]) * sc) : a.val_up[k];
+      acc = fmaT<T>(h, __ldg(vrow + a.src_up[k]), acc);
+    }
+    if (act) {
+      const int64_t e = idw * dimup + iup;
+      if (LZ) {
+        const T wt = T(double(acc) - cc * double(a.uprev[e]));
+        pa = __fma_rn(double(vrow[iup]) * sc, double(wt), pa);
+        __stcs(a.hv + e, wt);
+      } else {
+        __stcs(a.hv + e, acc);
+      }
+    }
+  }
+  if (LZ) {  // block partial of <v, w>, fixed order
+    __shared__ double s_red[8];
+    for (int o = 16; o > 0; o >>= 1) pa += __shfl_down_sync(0xffffffffu, pa, o);
+    if (lane == 0) s_red[threadIdx.x >> 5] = pa;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < int(wpb); ++w) t += s_red[w];
+      a.partial[blockIdx.x] = t;
+    }
+    finish_in_last_block(a.partial, gridDim.x, a.red_out, 0);
+  }
+}
+
 // Down-spin pass, balanced persistent form. CTA g owns the rows of group g (rows grouped on
 // the host so every group carries the same total number of hops); their hop lists sit in
 // shared memory. All CTAs sweep the column slabs (32*VEC columns) in the same order; inside
@@ -1499,6 +1563,19 @@ HxvArgs<T> make_args(edg_sector_s* s, const T* v, T* hv) {
   return a;
 }
 
+// Single-pass H x v (down-pass choice 3): one launch does the whole H x v; no up pass.
+template <typename T, bool LZ>
+int fused_pass(const HxvArgs<T>& a, cudaStream_t st, int sms) {
+  const int64_t ntiles = a.dimdw * ((a.dimup + 31) / 32);
+  const int64_t want = (ntiles + 7) / 8;
+  int64_t g = want < int64_t(sms) * 8 ? want : int64_t(sms) * 8;
+  if (LZ && g > kRedBlocks) g = kRedBlocks;  // one partial per block in the reduction scratch
+  if (g < 1) g = 1;
+  k_hxv_fused<T, LZ><<<dim3(int(g), a.ncols), 256, 0, st>>>(a, ntiles);
+  EDG_CUDA(cudaGetLastError());
+  return EDG_OK;
+}
+
 }  // namespace
 
 template <typename T>
@@ -1529,6 +1606,7 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
     return EDG_OK;
   }
   if (s->form == EDG_FORM_STORED) {
+    if (a.dwv == 3) return fused_pass<T, false>(a, st, sms);
     EDG_CHECK((dw_pass<T, true, false>(a, s->dw, st, sms)));
     EDG_CHECK((up_pass<T, false, false>(a, s->up, st, sms, nullptr)));
   } else {
@@ -1581,6 +1659,7 @@ int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double
   a.partial = partial;
   a.red_out = aout;
   const int sms = sm_count();
+  if (a.dwv == 3) return fused_pass<T, true>(a, s->stream, sms);
   EDG_CHECK((dw_pass<T, true, true>(a, s->dw, s->stream, sms)));
   EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nullptr)));
   return EDG_OK;
@@ -1600,6 +1679,7 @@ int hxv_block(edg_sector_s* s, int ncols, const int* active, const T* v, T* hv) 
   a.active = active;
   a.ncols = ncols;
   const int sms = sm_count();
+  if (a.dwv == 3) return fused_pass<T, false>(a, s->stream, sms);
   EDG_CHECK((dw_pass<T, true, false>(a, s->dw, s->stream, sms)));
   EDG_CHECK((up_pass<T, false, false>(a, s->up, s->stream, sms, nullptr)));
   return EDG_OK;
@@ -1623,11 +1703,12 @@ int hxv_block_lz(edg_sector_s* s, int ncols, const int* active, const T* u, cons
   a.active = active;
   a.ncols = ncols;
   const int sms = sm_count();
+  if (a.dwv == 3) return fused_pass<T, true>(a, s->stream, sms);
   EDG_CHECK((dw_pass<T, true, true>(a, s->dw, s->stream, sms)));
   EDG_CHECK((up_pass<T, false, true>(a, s->up, s->stream, sms, nullptr)));
   return EDG_OK;
 }
-// Autotuner: every down-pass x up-pass pair (3 x 4 for FP32, 3 x 1 for FP64; a pair whose
+// Autotuner: every down-pass x up-pass pair (4 x 4 for FP32, 4 x 1 for FP64; a pair whose
 // kernel does not apply to the sector falls back to the default kernel and times like it) on
 // `reps` H x v of scratch vectors after one untimed application, timed with CUDA events on
 // the sector's stream; the fastest pair becomes the sector's choice for precision T. Its
@@ -1640,7 +1721,7 @@ int hxv_autotune(edg_sector_s* s, int reps, double* ms, int* nc, int* best) {
     return EDG_ERR_UNSUPPORTED;
   }
   const int nup = sizeof(T) == 4 ? 4 : 1;
-  const int ncand = 3 * nup;
+  const int ncand = 4 * nup;
   cudaStream_t st = s->stream;
   EDG_CHECK(sector_variant_tables(s));
   DevBuf<T> x, y;

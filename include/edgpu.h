@@ -122,21 +122,24 @@ int edg_hxv_z(edg_sector* s, int64_t nloc, const double* v, double* hv);
 /* Same on real host vectors (real Hij only). */
 int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv);
 /* Autotuner of the stored-form H x v (real Hij): times each candidate pair of down-spin and
- * up-spin pass kernels (3 x 4 for FP32 vectors, 3 x 1 for FP64) on `reps` applications to
+ * up-spin pass kernels (4 x 4 for FP32 vectors, 4 x 1 for FP64) on `reps` applications to
  * scratch vectors of this sector (after one untimed application each), with CUDA events on
  * the sector's stream, and keeps the fastest pair for that precision: the H x v, the fused
  * Lanczos steps and the block chains of this sector then use it. Candidate k = nup*down + up
  * (nup = 4 for FP32, 1 for FP64): down 0 hop-balanced row groups, 1 block-staged rows (one
- * CTA per SM), 2 block-staged rows (two CTAs per SM); up (FP32) 0 32-bit SELL schedule,
+ * CTA per SM), 2 block-staged rows (two CTAs per SM), 3 the single-pass H x v (the whole
+ * product in one launch, for vectors that sit in L2; the up choice is then unused); up (FP32)
+ * 0 32-bit SELL schedule,
  * 1 packed 16-bit schedule with negated copies, 2 packed 16-bit schedule with sign bits,
  * 3 Kronecker schedule (hops inside the low or the high half of the sites from per-half
  * tables, the rest from a per-column table). ms (may be NULL) receives each candidate's ms
  * per H x v, *ncand their number, *best the index kept. FP64 results are the same bits for
  * every pair; the FP32 packed and Kronecker up passes change the order of a row's terms.
- * Untuned sectors use candidate 0. No counterpart in the reference. */
+ * Untuned real stored sectors of at most 500,000 states use the single pass (candidate 12
+ * for FP32, 3 for FP64), other sectors candidate 0. No counterpart in the reference. */
 int edg_sector_autotune(edg_sector* s, int precision, int reps, double* ms, int* ncand, int* best);
 /* Pin the H x v kernel pair of this sector for one precision to candidate k of
- * edg_sector_autotune's list (0..11 for FP32, 0..2 for FP64). The tables of the non-default
+ * edg_sector_autotune's list (0..15 for FP32, 0..3 for FP64). The tables of the non-default
  * kernels are built on the first call that needs them (this one, or edg_sector_autotune);
  * sectors that keep candidate 0 never build them. No counterpart in the reference. */
 int edg_sector_set_kernels(edg_sector* s, int precision, int candidate);

@@ -3,8 +3,9 @@ H x v is bit-exact for every pair (the passes keep the reference's summation ord
 FP32 one agrees with FP64 to 2e-6 relative, and the fused Lanczos step and block chains run
 on the pinned pair. Sectors: the 3x4 disordered lattice's (6,6) (D = 853,776) and the
 4x4 U=8 (5,5) sector (D = 19,079,424, DimUp 4368 < 2^15: the packed schedules apply).
-FP32 candidates are 4*down + up with up 3 the Kronecker schedule; the last pair (down 2,
-up 3) also runs the fused FP32 Lanczos steps."""
+FP32 candidates are 4*down + up with up 3 the Kronecker schedule and down 3 the single-pass
+H x v (no up pass); the last FP32 candidate (the single pass) also runs the fused FP32
+Lanczos steps."""
 import ctypes as C
 
 import numpy as np
@@ -47,11 +48,11 @@ def test_all_kernel_pairs(case):
     x64 = torch.from_numpy(v).cuda()
     x32 = x64.float()
     scale = np.abs(ref).max()
-    for cand in range(3):
+    for cand in range(4):
         s.set_kernels(cand, E.EDG_PREC_F64)
         y = _hxv(s, x64, L.lib().edg_hxv_dev_f64).cpu().numpy()
         assert np.array_equal(y, ref), (case, "f64", cand, np.abs(y - ref).max())
-    for cand in range(12):
+    for cand in range(16):
         s.set_kernels(cand, E.EDG_PREC_F32)
         y = _hxv(s, x32, L.lib().edg_hxv_dev_f32).double().cpu().numpy()
         assert np.abs(y - ref).max() <= 2e-6 * scale, (case, "f32", cand, np.abs(y - ref).max() / scale)
@@ -61,9 +62,9 @@ def test_all_kernel_pairs(case):
     assert abs(e32 - e64) <= 1e-10 * abs(e64)
     # autotune leaves a valid choice that reproduces the FP64 result bit for bit
     t = s.autotune(E.EDG_PREC_F64, reps=1)
-    assert len(t["ms"]) == 3 and 0 <= t["best"] < 3
+    assert len(t["ms"]) == 4 and 0 <= t["best"] < 4
     y = _hxv(s, x64, L.lib().edg_hxv_dev_f64).cpu().numpy()
     assert np.array_equal(y, ref)
     with pytest.raises(E.EdgError):
-        s.set_kernels(12, E.EDG_PREC_F32)
+        s.set_kernels(16, E.EDG_PREC_F32)
     s.delete()
