@@ -762,15 +762,33 @@ __global__ void __launch_bounds__(256) k_hxv_fused(HxvArgs<T> a, int64_t ntiles)
     const T* __restrict__ vrow = a.v + idw * dimup;
     const T d = a.e_up[cup] + a.e_dw[idw] + a.U * T(__popc(a.map_up[cup] & a.map_dw[idw]));
     T acc = (LZ ? T(double(d) * sc) : d) * vrow[cup];
-    const uint32_t k1 = a.off_dw[idw + 1];
-    for (uint32_t k = a.off_dw[idw]; k < k1; ++k) {
-      const T h = LZ ? T(double(a.val_dw[k]) * sc) : a.val_dw[k];
-      acc = fmaT<T>(h, a.v[int64_t(a.src_dw[k]) * dimup + cup], acc);
+    // sources in batches of 4 loads issued together, terms added in list order
+    constexpr int kB = 4;
+    const uint32_t k0 = a.off_dw[idw], k1 = a.off_dw[idw + 1];
+    for (uint32_t k = k0; k < k1; k += kB) {
+      T x[kB], h[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const uint32_t kk = k + u < k1 ? k + u : k;
+        h[u] = LZ ? T(double(a.val_dw[kk]) * sc) : a.val_dw[kk];
+        x[u] = a.v[int64_t(a.src_dw[kk]) * dimup + cup];
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u)
+        if (k + u < k1) acc = fmaT<T>(h[u], x[u], acc);
     }
-    const uint32_t u1 = a.off_up[cup + 1];
-    for (uint32_t k = a.off_up[cup]; k < u1; ++k) {
-      const T h = LZ ? T(double(a.val_up[k]) * sc) : a.val_up[k];
-      acc = fmaT<T>(h, __ldg(vrow + a.src_up[k]), acc);
+    const uint32_t u0 = a.off_up[cup], u1 = a.off_up[cup + 1];
+    for (uint32_t k = u0; k < u1; k += kB) {
+      T x[kB], h[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        const uint32_t kk = k + u < u1 ? k + u : k;
+        h[u] = LZ ? T(double(a.val_up[kk]) * sc) : a.val_up[kk];
+        x[u] = __ldg(vrow + a.src_up[kk]);
+      }
+#pragma unroll
+      for (int u = 0; u < kB; ++u)
+        if (k + u < u1) acc = fmaT<T>(h[u], x[u], acc);
     }
     if (act) {
       const int64_t e = idw * dimup + iup;
