@@ -712,11 +712,13 @@ struct LkRun {
 };
 
 // Basis columns of precision `elem` that fit in HBM beyond a 2 GB reserve, at most mmax.
-int basis_room(int64_t n, size_t elem, int k, int* mmax) {
+// `kept`: FP64 vectors held next to the basis at a thick restart (0 without restarts).
+int basis_room(int64_t n, size_t elem, int k, int* mmax, int kept = 0) {
   size_t fr = 0, tot = 0;
   EDG_CUDA(cudaMemGetInfo(&fr, &tot));
   const size_t reserve = size_t(2) << 30, per = size_t(n) * elem;
-  const size_t extra = size_t(n) * sizeof(double) * (size_t(k) + 4);  // Ritz and start vectors
+  // Ritz, start and restart vectors
+  const size_t extra = size_t(n) * sizeof(double) * (size_t(k) + 4 + size_t(kept));
   const int64_t fit = fr > reserve + extra ? int64_t((fr - reserve - extra) / per) - 2 : 0;
   if (fit < *mmax) *mmax = int(fit);
   if (*mmax < k || *mmax < 1) {
@@ -766,7 +768,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
       EDG_CHECK(X.alloc(size_t(k) * n, st, "FP32 Ritz vectors"));
       {
         int nc = ncv;
-        EDG_CHECK(basis_room(n, sizeof(float), k, &nc));
+        EDG_CHECK(basis_room(n, sizeof(float), k, &nc, k + (nc - k) / 4));
         LkRun<float> r32;
         EDG_CHECK(r32.run_tr(s, k, x0.p, steps_max, nc, k + (nc - k) / 4, std::max(tol, kTol32)));
         steps32 = r32.steps;
@@ -777,7 +779,7 @@ int lowest_k(edg_sector_s* s, int k, const double* v0_host, uint64_t seed, int m
         for (int r = 0; r < k32; ++r) EDG_CHECK(axpy_accum_dev<double>(st, x0.p, X.p + size_t(r) * n, 1.0, n));
       }  // the FP32 basis goes back to the pool before the FP64 one is taken
     }
-    EDG_CHECK(basis_room(n, sizeof(double), k, &ncv));
+    EDG_CHECK(basis_room(n, sizeof(double), k, &ncv, ncv < ne ? k + (ncv - k) / 4 : 0));
     LkRun<double> r64;
     EDG_CHECK(r64.run_tr(s, k, x0.p, steps_max, ncv, k + (ncv - k) / 4, tol));
     if (niter) *niter = steps32 + r64.steps;

@@ -257,16 +257,23 @@ def device_solver(model: Model, nup: int, ndw: int, neigen: int, lanc_solve: boo
 
 def sector_device_bytes(dim: int, neigen: int, lanc_solve: bool, params: DiagParams, cplx: bool = False) -> int:
     """Device memory one sector solve holds at its peak, in bytes: the Lanczos basis of
-    edg_lowest_k (min(lanc_niter, dim) vectors) plus its Ritz vectors and work vectors, the
+    edg_lowest_k plus its Ritz, start, work and (real sectors) restart vectors, the
     ground-state vectors of edg_ground_state, or the dense matrix with the eigensolver's
-    copy and workspace; twice that for the complex vectors of a complex-Hij model. The hop
-    tables of a sector are small beside these."""
+    copy and workspace; twice that for the complex vectors of a complex-Hij model. A real
+    sector's basis holds Ncv = max(10 k, 2k + 16) vectors (all of a sector of at most 4 Ncv
+    states), a complex sector's min(lanc_niter, dim). The hop tables are small beside these."""
     w = 16 if cplx else 8
     if not lanc_solve:
         return 3 * dim * dim * w + (1 << 20)
     if params.lanc_method == "lanczos":
         return 8 * dim * w + (1 << 20)
-    return (min(params.lanc_niter, dim) + neigen + 4) * dim * w + (1 << 20)
+    if cplx:
+        return (min(params.lanc_niter, dim) + neigen + 4) * dim * w + (1 << 20)
+    ncv = min(dim, max(10 * neigen, 2 * neigen + 16))
+    if dim <= 4 * ncv:
+        ncv = dim
+    kept = neigen + (ncv - neigen) // 4 if ncv < dim else 0
+    return (ncv + kept + neigen + 4) * dim * w + (1 << 20)
 
 
 class SectorScheduler:
