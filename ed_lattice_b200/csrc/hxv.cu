@@ -38,7 +38,8 @@ struct HxvArgs {
   const uint32_t* __restrict__ map_dw;
   T U;
   // Lanczos-fused mode (v = u / bn[jstep] is applied with the scale folded into the matrix
-  // elements; the up pass then forms w = Hv - (bn[j]/bn[j-1]) uprev and partial <v, w>)
+  // elements; the step forms w = Hv - (bn[j]/bn[j-1]) uprev and the up pass the partial
+  // <v, w>; lz_sub_in_dw says which pass subtracts uprev)
   const double* __restrict__ bn = nullptr;
   int jstep = 0;
   const T* __restrict__ uprev = nullptr;
@@ -53,6 +54,13 @@ struct HxvArgs {
   int ncols = 1;
   int dwv = 0, upv = 0;  // kernel choice (edg_sector_s::hxv_dw / hxv_up)
 };
+
+// Which pass of the Lanczos-fused step subtracts c * uprev. FP32: the down pass, as the start
+// of its diagonal term (it runs at a fraction of HBM bandwidth, and the up pass, short of
+// registers, then reads no third vector). FP64: the up pass, after all hops, which is the
+// reference's order (w = Hv - b u_prev), so FP64 coefficients stay bit-exact.
+template <typename T>
+constexpr bool lz_sub_in_dw() { return sizeof(T) == 4; }
 
 // Points a block-mode launch's arguments at this CTA's column; false when the column has
 // stopped. A single-vector launch (gridDim.y == 1, active == nullptr) is left as it is.
@@ -165,15 +173,17 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 // ONE: one CTA per SM (the staged rows take more than half of shared memory); the 64
 // registers per thread this allows carry the next batch of entries while the current one is
 // applied.
-// The Lanczos-fused form (LZ) with two CTAs per SM runs 768 threads per CTA: that leaves 40
-// registers per thread for the epilogue's FP64 state next to the batch of entries in flight
-// (at 1024 threads and 32 registers the batch no longer fit and the pass became latency-bound:
-// 2.56 against 1.34 ms on the 4x4 half-filled sector). One CTA per SM keeps 1024 threads.
-template <bool LZ, bool ONE>
-constexpr int up_threads() { return LZ && !ONE ? 768 : 1024; }
+// The FP64 Lanczos-fused form (LZ) with two CTAs per SM runs 768 threads per CTA: that
+// leaves 40 registers per thread for reading uprev and the epilogue's FP64 state next to the
+// batch of entries in flight. The FP32 form reads no uprev (its down pass subtracts it) and
+// runs 1024 threads: 1.34 ms with uprev at 768 threads, against 2.56 ms with uprev at 1024,
+// on the 4x4 half-filled sector; without uprev 1024 threads are the faster choice
+// (FP32+refine E0 0.2427 -> 0.2365 s). One CTA per SM keeps 1024 threads.
+template <typename T, bool LZ, bool ONE>
+constexpr int up_threads() { return LZ && !ONE && !lz_sub_in_dw<T>() ? 768 : 1024; }
 
 template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE>
-__global__ void __launch_bounds__(up_threads<LZ, ONE>(), ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
+__global__ void __launch_bounds__(up_threads<T, LZ, ONE>(), ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   if (!select_column(a)) return;
   using V = typename VecT<T, RT>::type;
   extern __shared__ __align__(16) unsigned char smem_up[];
@@ -271,16 +281,17 @@ __global__ void __launch_bounds__(up_threads<LZ, ONE>(), ONE ? 1 : 2) k_up_smem(
         }
       }
       if (LZ) {
-        // w = Hv - c * uprev ;  partial <v, w> with v = sc * u (staged in S)
+        // w = Hv - c * uprev (FP64 here; FP32: the down pass began from -c * uprev);
+        // partial <v, w> with v = sc * u (staged in S)
         const volatile double* lz = s_lz;
-        const double sc = lz[0], cc = lz[1];
+        const double sc = lz[0], cc = lz_sub_in_dw<T>() ? 0.0 : lz[1];
         const V xc = S[iup];
         const T* xs = reinterpret_cast<const T*>(&xc);
 #pragma unroll
         for (int r = 0; r < RT; ++r)
           if (r0 + r < a.dimdw) {
             const int64_t e = (r0 + r) * dimup + iup;
-            const T wt = T(double(acc[r]) - cc * double(a.uprev[e]));
+            const T wt = lz_sub_in_dw<T>() ? acc[r] : T(double(acc[r]) - cc * double(a.uprev[e]));
             pa = __fma_rn(double(xs[r]) * sc, double(wt), pa);
             __stcs(a.hv + e, wt);
           }
@@ -442,14 +453,14 @@ __global__ void __launch_bounds__(kKronThreads, ONE ? 1 : 2) k_up_kron(HxvArgs<f
         }
         if (LZ) {
           const volatile double* lz = s_lz;
-          const double sc = lz[0], cc = lz[1];
+          const double sc = lz[0];
           const V xc = S[c];
           const float* xv = reinterpret_cast<const float*>(&xc);
 #pragma unroll
           for (int r = 0; r < RT; ++r)
             if (r0 + r < a.dimdw) {
               const int64_t e = (r0 + r) * dimup + c;
-              const float wt = float(double(acc[r]) - cc * double(a.uprev[e]));
+              const float wt = acc[r];  // c * uprev: subtracted by the down pass
               pa = __fma_rn(double(xv[r]) * sc, double(wt), pa);
               __stcs(a.hv + e, wt);
             }
@@ -504,11 +515,8 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_p16(HxvArgs<float> a, 
   float2* S = reinterpret_cast<float2*>(smem_p16);
   const uint64_t* S64 = reinterpret_cast<const uint64_t*>(smem_p16);
   const int64_t dimup = a.dimup;
-  double sc = 1.0, cc = 0.0, pa = 0.0;
-  if (LZ) {
-    sc = 1.0 / a.bn[a.jstep];
-    cc = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
-  }
+  double sc = 1.0, pa = 0.0;
+  if (LZ) sc = 1.0 / a.bn[a.jstep];
   const float hs = LZ ? float(double(q.h) * sc) : q.h;
   const uint64_t hh = (uint64_t(__float_as_uint(hs)) << 32) | __float_as_uint(hs);
   for (int zq = threadIdx.x; zq < kUpZeroSlots; zq += blockDim.x) {  // padding targets
@@ -555,12 +563,11 @@ __global__ void __launch_bounds__(1024, ONE ? 1 : 2) k_up_p16(HxvArgs<float> a, 
       const float acc0 = __uint_as_float(uint32_t(acc)), acc1 = __uint_as_float(uint32_t(acc >> 32));
       if (LZ) {
         const float2 xc = S[iup];
-        const int64_t e0 = r0 * dimup + iup;
-        const float w0 = float(double(acc0) - cc * double(a.uprev[e0]));
+        const float w0 = acc0;  // c * uprev: subtracted by the down pass
         pa = __fma_rn(double(xc.x) * sc, double(w0), pa);
         __stcs(h0 + iup, w0);
         if (two) {
-          const float w1 = float(double(acc1) - cc * double(a.uprev[e0 + dimup]));
+          const float w1 = acc1;
           pa = __fma_rn(double(xc.y) * sc, double(w1), pa);
           __stcs(h1 + iup, w1);
         }
@@ -832,9 +839,13 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
   // the Lanczos scale 1/bn[j] (SCALED): folded into the hop values staged below, and read
   // from shared memory where the diagonal is formed, so that it holds no registers in the
   // slab loop (the FP64 form spilled with it)
-  __shared__ double s_sc;
+  __shared__ double s_sc, s_cc;
   const double sc = SCALED ? 1.0 / a.bn[a.jstep] : 1.0;
-  if (SCALED && threadIdx.x == 0) s_sc = sc;
+  if (SCALED && threadIdx.x == 0) {
+    s_sc = sc;
+    s_cc = a.jstep > 0 ? a.bn[a.jstep] / a.bn[a.jstep - 1] : 0.0;
+  }
+  constexpr bool SUB = SCALED && lz_sub_in_dw<T>();  // this pass starts from -c * uprev
   __shared__ int s_ctr;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t gr0 = goff[blockIdx.x];
@@ -888,13 +899,19 @@ __global__ void __launch_bounds__(256, 4) k_dw_grp(HxvArgs<T> a, const uint32_t*
         if (FIRST) {
           const T edw = s_edw[rr];
           const uint32_t mdw = s_mdw[rr];
-          T x[VEC];
+          T x[VEC], up[VEC];
           VecLd<T, VEC>::load(a.v + e0 + g * SEGW, x);
+          if (SUB) VecLd<T, VEC>::load(a.uprev + e0 + g * SEGW, up);
           const double scl = SCALED ? *static_cast<volatile double*>(&s_sc) : 1.0;
 #pragma unroll
           for (int r = 0; r < VEC; ++r) {
             const T d = a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw));
             acc[g][r] = (SCALED ? T(double(d) * scl) : d) * x[r];
+          }
+          if (SUB) {
+            const T ccn = T(-*static_cast<volatile double*>(&s_cc));
+#pragma unroll
+            for (int r = 0; r < VEC; ++r) acc[g][r] = fmaT<T>(ccn, up[r], acc[g][r]);
           }
         } else {
 #pragma unroll
@@ -970,6 +987,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_dw_blk(HxvArgs<T> a, const ui
   extern __shared__ __align__(16) unsigned char smem_dwb[];
   constexpr int SEGW = 32 * VEC, SLAB = SEGW * NSEG;
   const double sc = SCALED ? 1.0 / a.bn[a.jstep] : 1.0;
+  constexpr bool SUB = SCALED && lz_sub_in_dw<T>();  // this pass starts from -c * uprev
+  const T ccn = SUB && a.jstep > 0 ? T(-(a.bn[a.jstep] / a.bn[a.jstep - 1])) : T(0);
   __shared__ int s_ctr;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const uint32_t r0 = boff[blockIdx.x];
@@ -1029,12 +1048,14 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_dw_blk(HxvArgs<T> a, const ui
         if (FIRST) {
           const T edw = s_edw[rr];
           const uint32_t mdw = s_mdw[rr];
-          T x[VEC];
+          T x[VEC], up[VEC];
           VecLds<T, VEC>::load(tcol + size_t(rr) * SLAB + g * SEGW, x);
+          if (SUB) VecLd<T, VEC>::load(a.uprev + e0 + g * SEGW, up);
 #pragma unroll
           for (int r = 0; r < VEC; ++r) {
             const T d = a.e_up[c + r] + edw + a.U * T(__popc(a.map_up[c + r] & mdw));
             acc[g][r] = (SCALED ? T(double(d) * sc) : d) * x[r];
+            if (SUB) acc[g][r] = fmaT<T>(ccn, up[r], acc[g][r]);
           }
         } else {
 #pragma unroll
@@ -1369,7 +1390,7 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
   if (LZ && g > kRedBlocks) g = kRedBlocks;  // one partial per block in the reduction scratch
-  kern<<<dim3(int(g), a.ncols), per_sm == 2 ? up_threads<LZ, false>() : up_threads<LZ, true>(), smem, st>>>(a, sl, nrb);
+  kern<<<dim3(int(g), a.ncols), per_sm == 2 ? up_threads<T, LZ, false>() : up_threads<T, LZ, true>(), smem, st>>>(a, sl, nrb);
   EDG_CUDA(cudaGetLastError());
   if (grid) *grid = int(g);
   return EDG_OK;
@@ -1381,7 +1402,8 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
 template <typename T, bool FIRST, bool SCALED>
 int dw_pass(const HxvArgs<T>& a, const SpinBasis& Bdw, cudaStream_t st, int sms) {
   const bool v2 = (a.dimup % 2 == 0) && (reinterpret_cast<uintptr_t>(a.v) % (2 * sizeof(T)) == 0) &&
-                  (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0);
+                  (reinterpret_cast<uintptr_t>(a.hv) % (2 * sizeof(T)) == 0) &&
+                  (!(SCALED && lz_sub_in_dw<T>()) || reinterpret_cast<uintptr_t>(a.uprev) % (2 * sizeof(T)) == 0);
   const int vec = v2 ? 2 : 1;
   const SpinBasis::RowBlocks* rb = (a.dwv == 1 || a.dwv == 2) ? &Bdw.rowblk[a.dwv - 1] : nullptr;
   if (rb && Bdw.max_row <= kDwHops && rb->count > 0) {
