@@ -67,6 +67,10 @@ SIGNATURES = {
     "edg_sector_set_kernels": (_i, [_p, _i, _i]),
     "edg_hxv_dev_f64": (_i, [_p, _p, _p]),
     "edg_hxv_dev_f32": (_i, [_p, _p, _p]),
+    "edg_hxv_cols_dev_f64": (_i, [_p, _i64, _i64, _p, _p]),
+    "edg_hxv_cols_dev_f32": (_i, [_p, _i64, _i64, _p, _p]),
+    "edg_hxv_rows_dev_f64": (_i, [_p, _i64, _i64, _p, _p]),
+    "edg_hxv_rows_dev_f32": (_i, [_p, _i64, _i64, _p, _p]),
     "edg_tridiag_d": (_i, [_p, _pd, _i, _d, _i, _pd, _pd, _pd, _pi]),
     "edg_tridiag_dev_f64": (_i, [_p, _p, _i, _d, _i, _pd, _pd, _pd, _pi]),
     "edg_tridiag_dev_f64_noalloc": (_i, [_p, _p, _i, _d, _pd, _pd, _pd, _pi]),

@@ -100,6 +100,19 @@ int check_vec_align(const edg_sector_s* s, const void* p, const char* what) {
   return EDG_OK;
 }
 
+// The slab H x v entries (edg_hxv_cols_dev_*, edg_hxv_rows_dev_*): argument checks, then
+// hxv_cols / hxv_rows on the sector's stream.
+template <typename T>
+int slab_hxv(edg_sector* s, int cols, int64_t first, int64_t count, const T* dv, T* dhv, const char* what) {
+  EDG_CHECK(check_sector(s));
+  EDG_ARG(dv && dhv && dv != dhv, "%s: bad vectors", what);
+  const int64_t extent = cols ? s->up.dim : s->dw.dim;
+  EDG_ARG(first >= 0 && count >= 0 && first + count <= extent, "%s: slab [%lld, %lld) outside [0, %lld)", what,
+          (long long)first, (long long)(first + count), (long long)extent);
+  if (count == 0) return EDG_OK;
+  EDG_ON_DEVICE(s->device);
+  return cols ? hxv_cols<T>(s, first, count, dv, dhv) : hxv_rows<T>(s, first, count, dv, dhv);
+}
 }  // namespace
 
 extern "C" {
@@ -362,6 +375,19 @@ int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv) {
   EDG_CHECK(check_vec_align<float>(s, dhv, "edg_hxv_dev_f32"));
   EDG_ON_DEVICE(s->device);
   return hxv_apply<float>(s, dv, dhv);
+}
+
+int edg_hxv_cols_dev_f64(edg_sector* s, int64_t col0, int64_t ncols, const double* dv, double* dhv) {
+  return slab_hxv<double>(s, 1, col0, ncols, dv, dhv, "edg_hxv_cols_dev_f64");
+}
+int edg_hxv_cols_dev_f32(edg_sector* s, int64_t col0, int64_t ncols, const float* dv, float* dhv) {
+  return slab_hxv<float>(s, 1, col0, ncols, dv, dhv, "edg_hxv_cols_dev_f32");
+}
+int edg_hxv_rows_dev_f64(edg_sector* s, int64_t row0, int64_t nrows, const double* dv, double* dhv) {
+  return slab_hxv<double>(s, 0, row0, nrows, dv, dhv, "edg_hxv_rows_dev_f64");
+}
+int edg_hxv_rows_dev_f32(edg_sector* s, int64_t row0, int64_t nrows, const float* dv, float* dhv) {
+  return slab_hxv<float>(s, 0, row0, nrows, dv, dhv, "edg_hxv_rows_dev_f32");
 }
 
 int edg_hxv_d(edg_sector* s, int64_t nloc, const double* v, double* hv) {

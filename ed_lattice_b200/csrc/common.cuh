@@ -324,6 +324,10 @@ uint64_t binom_host(int n, int k);
 template <typename T>
 int hxv_apply(edg_sector_s* s, const T* v, T* hv);
 template <typename T>
+int hxv_cols(edg_sector_s* s, int64_t col0, int64_t ncols, const T* v, T* hv);
+template <typename T>
+int hxv_rows(edg_sector_s* s, int64_t row0, int64_t nrows, const T* v, T* hv);
+template <typename T>
 int hxv_apply_lz(edg_sector_s* s, const T* u, const T* uprev, T* w, const double* bn, int j, double* partial,
                  double* aout);
 bool hxv_lz_available(const edg_sector_s* s, size_t elem);

@@ -1681,6 +1681,42 @@ int hxv_apply(edg_sector_s* s, const T* v, T* hv) {
 template int hxv_apply<float>(edg_sector_s*, const float*, float*);
 template int hxv_apply<double>(edg_sector_s*, const double*, double*);
 
+// Slab forms of the stored H x v for vectors split over ranks by rows (the down-spin index).
+// Column slab: all DimDw rows of columns [col0, col0 + ncols), row-major with row length
+// ncols; hv = (diag + H_dw x I) v there, by the down pass of hxv_apply. Row slab: rows
+// [row0, row0 + nrows) of length DimUp; hv += (I x H_up) v, by its up pass. The column form
+// and then (after the transposes) the row form compute every element in hxv_apply's order,
+// so the split H x v equals it bit for bit.
+template <typename T>
+int hxv_cols(edg_sector_s* s, int64_t col0, int64_t ncols, const T* v, T* hv) {
+  if (s->cplx || s->form != EDG_FORM_STORED) {
+    set_error("slab H x v: real stored-form sectors only");
+    return EDG_ERR_UNSUPPORTED;
+  }
+  HxvArgs<T> a = make_args<T>(s, v, hv);
+  a.dimup = ncols;
+  a.e_up += col0;
+  a.map_up += col0;
+  if (a.dwv == 3) a.dwv = 0;  // the single pass needs whole rows
+  return dw_pass<T, true, false>(a, s->dw, s->stream, sm_count());
+}
+template <typename T>
+int hxv_rows(edg_sector_s* s, int64_t row0, int64_t nrows, const T* v, T* hv) {
+  if (s->cplx || s->form != EDG_FORM_STORED) {
+    set_error("slab H x v: real stored-form sectors only");
+    return EDG_ERR_UNSUPPORTED;
+  }
+  HxvArgs<T> a = make_args<T>(s, v, hv);
+  a.dimdw = nrows;
+  a.e_dw += row0;
+  a.map_dw += row0;
+  return up_pass<T, false, false>(a, s->up, s->stream, sm_count(), nullptr);
+}
+template int hxv_cols<float>(edg_sector_s*, int64_t, int64_t, const float*, float*);
+template int hxv_cols<double>(edg_sector_s*, int64_t, int64_t, const double*, double*);
+template int hxv_rows<float>(edg_sector_s*, int64_t, int64_t, const float*, float*);
+template int hxv_rows<double>(edg_sector_s*, int64_t, int64_t, const double*, double*);
+
 // Lanczos-fused H x v (stored form): with v = u / bn[j], writes w = H v - (bn[j]/bn[j-1]) uprev
 // into `w` and <v, w> into *aout (`partial`: a reduction scratch of kRedSlots doubles). Returns
 // EDG_ERR_UNSUPPORTED when the sector needs one of the general kernels instead.

@@ -146,6 +146,20 @@ int edg_sector_set_kernels(edg_sector* s, int precision, int candidate);
 /* Device-resident forms (vectors in HBM, reference layout); stream-ordered, no sync. */
 int edg_hxv_dev_f64(edg_sector* s, const double* dv, double* dhv);
 int edg_hxv_dev_f32(edg_sector* s, const float* dv, float* dhv);
+/* Slab forms of the stored H x v for a sector whose vectors are split over the ranks of a
+ * process group by rows (the down-spin index idw of element iup + idw*DimUp); the sector
+ * object itself holds only the O(DimUp + DimDw) tables. Replaces, for sectors beyond one
+ * GPU's memory, the reference's MPI split of spMatVec (src/DIAG/HAMILTONIAN_STORED_HxV.f90,
+ * MPI branch), which this build does not otherwise reproduce.
+ *  - cols: dv/dhv hold ALL DimDw rows of columns [col0, col0+ncols), row-major with row
+ *    length ncols (the transpose of the row slabs); dhv = (diag + H_dw x I) dv there.
+ *  - rows: dv/dhv hold rows [row0, row0+nrows), row length DimUp; dhv += (I x H_up) dv.
+ * The column form, then the row form on its transposed result, is edg_hxv_dev_* bit for bit.
+ * Real stored-form sectors; stream-ordered, no sync. No counterpart in the reference. */
+int edg_hxv_cols_dev_f64(edg_sector* s, int64_t col0, int64_t ncols, const double* dv, double* dhv);
+int edg_hxv_cols_dev_f32(edg_sector* s, int64_t col0, int64_t ncols, const float* dv, float* dhv);
+int edg_hxv_rows_dev_f64(edg_sector* s, int64_t row0, int64_t nrows, const double* dv, double* dhv);
+int edg_hxv_rows_dev_f32(edg_sector* s, int64_t row0, int64_t nrows, const float* dv, float* dhv);
 
 /* ------------------------------------------------------------------ Lanczos
  * tridiag_Hv_sector(isector,vvinit,alanc,blanc,norm2) (src/DIAG/HAMILTONIAN.f90:242-275)
