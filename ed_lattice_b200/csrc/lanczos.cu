@@ -130,16 +130,12 @@ struct Recurrence {
   const double* b_dev() const { return fused ? sc.bn : sc.b; }
   // step j: W <- the unnormalised u_{j+1}; returns a_j and b_{j+1} on the host
   int step(int j, double* a, double* b) {
-    const int64_t n = s->vlen;
+    EDG_CHECK(step_dev(j));
+    return read(j, a, b);
+  }
+  // a_j and b_{j+1} of a queued step j, on the host (waits for step j)
+  int read(int j, double* a, double* b) {
     cudaStream_t st = s->stream;
-    if (fused) {
-      EDG_CHECK(hxv_apply_lz<T>(s, U, P, W, sc.bn, j, sc.partial, sc.a + j));
-      EDG_CHECK(lanczos_step_b2<T>(st, W, U, sc.a + j, sc.bn + j, n, sc.partial, sc.bn + j + 1));
-    } else {
-      EDG_CHECK(hxv_apply<T>(s, U, W));
-      EDG_CHECK(lanczos_step_a<T>(st, W, P, U, sc.b + j, n, sc.partial, sc.a + j));
-      EDG_CHECK(lanczos_step_b<T>(st, W, U, sc.a + j, n, sc.partial, sc.b + j + 1));
-    }
     double h[2];
     EDG_CUDA(cudaMemcpyAsync(&h[0], sc.a + j, sizeof(double), cudaMemcpyDeviceToHost, st));
     EDG_CUDA(cudaMemcpyAsync(&h[1], (fused ? sc.bn : sc.b) + j + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -353,8 +349,8 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
   A->clear();
   B->assign(1, 0.0);
   colscale->clear();
-  double eold = 0.0;
-  for (int j = 0; j < maxit; ++j) {
+  // the basis column of step j (before the step is queued)
+  auto column = [&](int j) -> int {
     if (basis && j < basis_cols) {
       if (R.ext) {
         colscale->push_back(R.vscale(j));  // column j holds u_j = v_j / vscale(j)
@@ -363,26 +359,47 @@ int gs_run(edg_sector_s* s, const double* dv0, int maxit, double tol, std::vecto
         colscale->push_back(1.0);
       }
     }
+    return EDG_OK;
+  };
+  double eold = 0.0, err_prev = HUGE_VAL;
+  bool queued = false;  // step j was queued by the previous iteration
+  for (int j = 0; j < maxit; ++j) {
+    if (!queued) {
+      EDG_CHECK(column(j));
+      EDG_CHECK(R.step_dev(j));
+    }
     double a, b;
-    EDG_CHECK(R.step(j, &a, &b));
+    EDG_CHECK(R.read(j, &a, &b));
     if (!std::isfinite(a) || !std::isfinite(b)) {
       set_error("Lanczos produced a non-finite coefficient at step %d", j);
       return EDG_ERR_NOCONV;
     }
     A->push_back(a);
+    // While the last test was far from convergence (its error estimate more than 100x the
+    // target 0.1 tol |E0|), step j+1 is queued before step j is tested, so the host's test
+    // runs while the GPU works; near convergence the test comes first, so no step is wasted.
+    queued = j + 1 < maxit && b >= 1e-14 && err_prev > 10.0 * tol * std::fabs(eold);
+    if (queued) {
+      EDG_CHECK(R.advance(j, b));
+      EDG_CHECK(column(j + 1));
+      EDG_CHECK(R.step_dev(j + 1));
+    }
     // FP32 vectors lose orthogonality within tens of steps: skip the copies of E0 that follow
     const Ritz rz = lowest_ritz(*A, *B, b, sizeof(T) == 4 ? 10.0 * tol : 0.0);
     const double e = rz.e0;
     // converged when the error estimate is 10x below tol*|E0| (or, as a fallback for a
-    // degenerate lowest level, when E0 stops moving), or the Krylov space is exhausted
+    // degenerate lowest level, when E0 stops moving), or the Krylov space is exhausted; a
+    // step queued ahead is then discarded (its column lies past the Ritz vector's)
     const bool conv = (j > 0 && rz.err <= 0.1 * tol * std::fabs(e)) ||
                       (j > 0 && std::fabs(e - eold) <= 0.01 * tol * std::fabs(e)) || b < 1e-14;
     eold = e;
+    err_prev = rz.err;
     B->push_back(b);
     *e0 = e;
     if (conv || j + 1 == maxit) break;
-    EDG_CHECK(R.advance(j, b));
+    if (!queued) EDG_CHECK(R.advance(j, b));
   }
+  EDG_CUDA(cudaStreamSynchronize(st));  // a discarded step still runs on the work vectors
   return EDG_OK;
 }
 
