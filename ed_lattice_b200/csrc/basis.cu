@@ -461,9 +461,14 @@ static int edge_colour(int G, int M, const std::vector<std::pair<int, int>>& edg
 // columns from M = G bank groups (column src sits in group src % M). Per slice and lane
 // group, lanes x groups are edge-coloured; colour = slot. Lanes without an entry in a slot
 // read one of the zero columns DimUp..DimUp+31 whose bank group is free in that slot.
+// Slot c of lane l sits at c*32 + l of its slice, or, with v4, at (c/4)*128 + l*4 + c%4: a
+// lane's slots 4i..4i+3 side by side, one 16-byte load (widths are multiples of 8).
 static void build_schedule(int64_t dim, int rt, const std::vector<uint32_t>& off, const std::vector<uint32_t>& src,
                            const std::vector<uint32_t>& sgn, std::vector<uint32_t>& soff, std::vector<uint32_t>& ent,
-                           bool* ok, int round_to = kSellBatch) {
+                           bool* ok, int round_to = kSellBatch, bool v4 = false) {
+  auto at = [v4](int c, int lane) -> size_t {
+    return v4 ? size_t(c / 4) * 128 + size_t(lane) * 4 + size_t(c % 4) : size_t(c) * 32 + size_t(lane);
+  };
   const int G = 32 / rt, M = G;
   const int64_t nsl = (dim + 31) / 32;
   soff.assign(nsl + 1, 0);
@@ -500,7 +505,7 @@ static void build_schedule(int64_t dim, int rt, const std::vector<uint32_t>& off
       for (size_t q = 0; q < grp_edges[g].size(); ++q) {
         const int l = grp_edges[g][q].first, c = grp_colour[g][q], k = grp_eidx[g][q];
         const int lane = g * G + l;
-        ent[base + size_t(c) * 32 + lane] = src[k] | (sgn[k] << 31);
+        ent[base + at(c, lane)] = src[k] | (sgn[k] << 31);
         filled[size_t(c) * 32 + lane] = 1;
         used[size_t(c) * M + grp_edges[g][q].second] = 1;
       }
@@ -510,7 +515,7 @@ static void build_schedule(int64_t dim, int rt, const std::vector<uint32_t>& off
         if (free_bank == M) free_bank = 0;  // every lane of the group has an entry: no padding here
         const uint32_t zcol = uint32_t(dim) + uint32_t((free_bank - int(dim % M) + M) % M);
         for (int l = 0; l < G; ++l)
-          if (!filled[size_t(c) * 32 + g * G + l]) ent[base + size_t(c) * 32 + g * G + l] = zcol;
+          if (!filled[size_t(c) * 32 + g * G + l]) ent[base + at(c, g * G + l)] = zcol;
       }
     }
   }
@@ -978,6 +983,7 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
   B.sell_h = hsgn;
   // FP32 conflict-free schedule (uniform tables whose rows fit the shared-memory up pass)
   B.sched_rt = 0;
+  B.sched_v4 = false;
   B.sched_ent.reset();
   B.sched_off.reset();
   const int rt32 = up_rows_per_cta(dim, sizeof(float));
@@ -986,8 +992,11 @@ int build_sell(edg_sector_s* s, SpinBasis& B) {
     for (int64_t k = 0; k < B.nnz; ++k) sg[k] = (val[k] == hsgn) ? 0u : 1u;
     std::vector<uint32_t> qoff, qent;
     bool ok = false;
-    build_schedule(dim, rt32, off, src, sg, qoff, qent, &ok);
+    // the two-CTA form of the up pass loads its entries four slots at a time
+    const bool v4 = size_t(dim + kUpZeroSlots) * rt32 * sizeof(float) <= kUpSmemTwoPerSM;
+    build_schedule(dim, rt32, off, src, sg, qoff, qent, &ok, kSellBatch, v4);
     if (ok) {
+      B.sched_v4 = v4;
       qent.push_back(uint32_t(dim));
       EDG_CHECK(B.sched_off.alloc(qoff.size(), st, "SELL schedule"));
       EDG_CHECK(B.sched_ent.alloc(qent.size(), st, "SELL schedule"));

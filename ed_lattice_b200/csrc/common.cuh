@@ -154,6 +154,7 @@ struct SpinBasis {
   DevBuf<uint32_t> sched_ent;
   DevBuf<uint32_t> sched_off;
   int sched_rt = 0;             // rows-per-CTA of the FP32 up pass the schedule was built for
+  bool sched_v4 = false;        // slots stored four per lane together (two 16-byte loads per batch)
   // Packed FP32 schedule (uniform tables, 2 * (DimUp + 32) <= 32768 slots): the conflict-free
   // slot schedule for two rows per CTA with slot counts rounded to 2 instead of 8, two 16-bit
   // entries per 32-bit word (entry 2k of a row in the low half of word k, 2k+1 in the high

@@ -129,6 +129,7 @@ struct SellArgs {
   const uint32_t* __restrict__ off;
   const T* __restrict__ val;  // non-uniform tables only
   T h;                        // |value| with the sign of code 0 (uniform tables)
+  bool v4 = false;            // a lane's slots stored four together (SpinBasis::sched_v4)
 };
 
 // acc[0..RT) += h * x[0..RT): packed FP32x2 FMAs where the pair shares h (Blackwell
@@ -182,7 +183,9 @@ __device__ __forceinline__ double flip_sign(double h, uint32_t e) {
 template <typename T, bool LZ, bool ONE>
 constexpr int up_threads() { return LZ && !ONE && !lz_sub_in_dw<T>() ? 768 : 1024; }
 
-template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE>
+// E4: the table stores a lane's slots four together (sched_v4), so a batch of 8 entries is
+// two 16-byte loads per lane instead of eight 4-byte ones (two CTAs per SM, uniform tables).
+template <typename T, int RT, bool FIRST, bool UNIFORM, bool LZ, bool ONE, bool E4 = false>
 __global__ void __launch_bounds__(up_threads<T, LZ, ONE>(), ONE ? 1 : 2) k_up_smem(HxvArgs<T> a, SellArgs<T> sl, int64_t nrowblk) {
   if (!select_column(a)) return;
   using V = typename VecT<T, RT>::type;
@@ -262,6 +265,18 @@ __global__ void __launch_bounds__(up_threads<T, LZ, ONE>(), ONE ? 1 : 2) k_up_sm
           }
 #pragma unroll
           for (int u = 0; u < kUpBatch; ++u) e[u] = en[u];
+        }
+      } else if (E4 && UNIFORM) {
+        static_assert(!E4 || kUpBatch == 8, "two 16-byte entry loads per batch");
+        const uint4* __restrict__ ent4 = reinterpret_cast<const uint4*>(sl.ent);
+        for (uint32_t q = o >> 2; q < (o1 >> 2); q += 8 * kUpBatch) {
+          const uint4 x0 = __ldg(ent4 + q + lane), x1 = __ldg(ent4 + q + 32 + lane);
+          const uint32_t e[kUpBatch] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+          for (int u = 0; u < kUpBatch; ++u) {
+            const V x = S[e[u] & 0x7fffffffu];
+            Fma<T, RT>::run(flip_sign(hs, e[u]), reinterpret_cast<const T*>(&x), acc);
+          }
         }
       } else {
         for (uint32_t p0 = o + lane; p0 < o1; p0 += 32 * kUpBatch) {
@@ -1386,6 +1401,9 @@ int launch_up_smem(const HxvArgs<T>& a, const SellArgs<T>& sl, cudaStream_t st, 
   const size_t smem = size_t(a.dimup + kUpZeroSlots) * RT * sizeof(T);
   const int per_sm = smem <= kUpSmemTwoPerSM ? 2 : 1;
   auto kern = per_sm == 2 ? k_up_smem<T, RT, FIRST, UNIFORM, LZ, false> : k_up_smem<T, RT, FIRST, UNIFORM, LZ, true>;
+  if constexpr (sizeof(T) == 4 && UNIFORM) {
+    if (per_sm == 2 && sl.v4) kern = k_up_smem<T, RT, FIRST, UNIFORM, LZ, false, true>;
+  }
   if (smem > 48 * 1024) EDG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   const int64_t nrb = (a.dimdw + RT - 1) / RT;
   int64_t g = nrb < int64_t(sms) * per_sm ? nrb : int64_t(sms) * per_sm;
@@ -1566,6 +1584,7 @@ int up_pass(const HxvArgs<T>& a, const SpinBasis& B, cudaStream_t st, int sms, i
   if (sizeof(T) == 4 && B.sched_rt == rt && B.sched_ent.p) {  // FP32: bank-conflict-free order
     sl.ent = B.sched_ent.p;
     sl.off = B.sched_off.p;
+    sl.v4 = B.sched_v4;
   }
   sl.val = pick_sell<T>(B);
   sl.h = T(B.sell_h);
